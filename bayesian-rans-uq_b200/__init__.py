@@ -1,0 +1,20 @@
+"""B200-native forward model for Bayesian calibration of k-omega SST closure
+coefficients: the SIMPLE + SST steady solve of the reference's ForwardModel /
+ForwardBatch, run by hand-written sm_100a CUDA kernels behind a C ABI
+(include/rq_b200.h). Import it as ``rans_uq_b200`` (the repository-root shim).
+"""
+from . import _native
+from .core import (EvaluationResult, EvaluationStatus, FlowBoundaryConditions, ForwardBatch,
+                   ForwardBatchResult, ForwardBatchRow, ForwardEvaluationResult, ForwardModel,
+                   InferenceParameterSet, Mesh, ObservationOperator, SST_DEFAULTS, SST_NAMES,
+                   SolverSettings, Vec3, evaluate_multi)
+
+__all__ = ["EvaluationResult", "EvaluationStatus", "FlowBoundaryConditions", "ForwardBatch",
+           "ForwardBatchResult", "ForwardBatchRow", "ForwardEvaluationResult", "ForwardModel",
+           "InferenceParameterSet", "Mesh", "ObservationOperator", "SST_DEFAULTS", "SST_NAMES",
+           "SolverSettings", "Vec3", "evaluate_multi", "lib"]
+
+
+def lib():
+    """The loaded CUDA library (raises if it is not built)."""
+    return _native.lib()

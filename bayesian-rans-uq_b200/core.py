@@ -1,0 +1,563 @@
+"""Host-side mirror of the reference forward-model API (the ``cfdr._core``
+pybind11 module, rans-uq/python/bindings.cpp:452-975) on the B200 path.
+
+Same names, argument meaning and error behaviour as the reference for the calls
+a calibration makes: ``Mesh.make_periodic_channel_2d`` /
+``make_curved_channel_periodic_2d``, ``SolverSettings``,
+``FlowBoundaryConditions.channel_defaults``, ``InferenceParameterSet``,
+``ObservationOperator.add_velocity_profile``, ``ForwardBatch(...).evaluate``
+and ``ForwardModel.evaluate[_with_diagnostics]``. Every solve runs on the GPU
+through the C ABI (include/rq_b200.h); nothing here computes a flow field.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+
+class EvaluationStatus(enum.IntEnum):
+    """EvaluationStatus (core/include/EvaluationTypes.hpp:6); Python names as bindings.cpp:464-469."""
+
+    Converged = 0
+    Unconverged = 1
+    DivergenceDetected = 2
+    InvalidParameters = 3
+    Unknown = 4
+
+
+@dataclass
+class Vec3:
+    x: float = 0.0
+    y: float = 0.0
+    z: float = 0.0
+
+
+@dataclass
+class Mesh:
+    """A streamwise-periodic mesh description (the GPU path's mesh family)."""
+
+    kind: int
+    nx: int
+    ny: int
+    lx: float = 1.0
+    h: float = 1.0
+    re_tau: float = 0.0
+    yplus: float = 1.0
+    x_nodes: np.ndarray | None = None
+    y_bottom: np.ndarray | None = None
+    y_top: float = 0.0
+    re: float = 0.0
+    _wall_distance: bool = False
+
+    @staticmethod
+    def make_periodic_channel_2d(nx, ny, Lx, h, re_tau, yplus_target=1.0) -> "Mesh":
+        """Mesh::makePeriodicChannel2D (core/src/Mesh.cpp:511-521)."""
+        if nx < 3 or ny < 1 or not (Lx > 0 and h > 0 and re_tau > 0 and yplus_target > 0):
+            raise ValueError("periodic channel needs nx >= 3, ny >= 1 and positive sizes")
+        return Mesh(N.MESH_CHANNEL, int(nx), int(ny), float(Lx), float(h), float(re_tau),
+                    float(yplus_target))
+
+    @staticmethod
+    def make_curved_channel_periodic_2d(x_nodes, y_bottom, y_top, ny, re=0.0,
+                                        yplus_target=1.0) -> "Mesh":
+        """Mesh::makeCurvedChannelPeriodic2D (core/src/Mesh.cpp:490-509)."""
+        x = np.ascontiguousarray(np.asarray(x_nodes, dtype=np.float64))
+        y = np.ascontiguousarray(np.asarray(y_bottom, dtype=np.float64))
+        if x.ndim != 1 or x.shape != y.shape or len(x) < 4:
+            raise ValueError("makeCurvedChannelPeriodic2D: need nx+1 x nodes and matching "
+                             "yBottom samples")
+        return Mesh(N.MESH_CURVED, len(x) - 1, int(ny), x_nodes=x, y_bottom=y,
+                    y_top=float(y_top), re=float(re), yplus=float(yplus_target))
+
+    def compute_wall_distance(self) -> None:
+        self._wall_distance = True
+
+    def wall_distance_valid(self) -> bool:
+        return self._wall_distance
+
+    def n_cells(self) -> int:
+        return self.nx * self.ny
+
+    def desc(self) -> N.MeshDesc:
+        d = N.MeshDesc()
+        d.kind, d.nx, d.ny = self.kind, self.nx, self.ny
+        d.lx, d.h, d.re_tau, d.yplus = self.lx, self.h, self.re_tau, self.yplus
+        if self.kind == N.MESH_CURVED:
+            d.x_nodes, d.y_bottom = N.dptr(self.x_nodes), N.dptr(self.y_bottom)
+            d.y_top, d.re = self.y_top, self.re
+        return d
+
+    def cell_geometry(self) -> np.ndarray:
+        """(n_cells, 4): centre x, centre y, volume, wall distance."""
+        d = self.desc()
+        nc = C.c_int32()
+        N.call("rq_mesh_geometry", C.byref(d), C.byref(nc), None)
+        out = np.zeros((nc.value, 4))
+        N.call("rq_mesh_geometry", C.byref(d), C.byref(nc), N.dptr(out))
+        return out
+
+    def cell_centers(self) -> np.ndarray:
+        return self.cell_geometry()[:, :2]
+
+
+@dataclass
+class SolverSettings:
+    """SolverSettings (core/include/FlowFields.hpp:70-241) with the reference defaults."""
+
+    max_iterations: int = 500
+    convergence_tol: float = 1e-5
+    divergence_limit: float = 1e6
+    legacy_convergence: bool = False
+    convergence_window: int = 25
+    monitor_interval: int = 10
+    alpha_u: float = 0.7
+    alpha_p: float = 0.3
+    alpha_k: float = 0.5
+    alpha_omega: float = 0.5
+    inner_iterations: int = 200
+    inner_tolerance: float = 1e-3
+    turb_start_iter: int = 5
+    turb_update_interval: int = 1
+    nut_floor_iters: int = 500
+    legacy_rhie_chow_gate: bool = False
+    legacy_omega_wall_pinning: bool = False
+    momentum_convection: str = "limitedLinearUpwind"
+    turbulence_convection: str = "limitedLinearUpwind"
+    alpha_injection: float = 0.3
+    body_force: Vec3 = field(default_factory=Vec3)
+    k_min: float = 1e-10
+    k_max: float = 1e10
+    omega_min: float = 1e-6
+    report_interval: int = 10
+    verbose: bool = True
+    pressure_solver: str = "AMG"
+    momentum_solver: str = "BiCGSTAB"
+    turbulence_solver: str = "BiCGSTAB"
+    use_wall_functions: bool = False
+    sst_variant: int = 0
+    # B200 path only
+    precision: str = "fp64"
+    block_threads: int = 0
+
+    def native(self) -> N.Settings:
+        unsupported = []
+        if self.legacy_convergence:
+            unsupported.append("legacy_convergence")
+        if self.legacy_rhie_chow_gate:
+            unsupported.append("legacy_rhie_chow_gate")
+        if self.legacy_omega_wall_pinning:
+            unsupported.append("legacy_omega_wall_pinning")
+        if self.momentum_convection != "limitedLinearUpwind" or \
+                self.turbulence_convection != "limitedLinearUpwind":
+            unsupported.append("convection schemes other than limitedLinearUpwind")
+        if self.use_wall_functions:
+            unsupported.append("wall functions")
+        if self.sst_variant != 0:
+            unsupported.append("SST variants other than Full")
+        if self.momentum_solver != "BiCGSTAB" or self.turbulence_solver != "BiCGSTAB":
+            unsupported.append("momentum/turbulence solvers other than BiCGSTAB")
+        if unsupported:
+            raise NotImplementedError("outside the B200 forward-model path: " + ", ".join(unsupported))
+        for name in ("momentum_convection", "turbulence_convection"):
+            if getattr(self, name) not in ("upwind", "linearUpwind", "limitedLinearUpwind"):
+                raise ValueError(f"unknown SIMPLE convection scheme: {getattr(self, name)}")
+        if self.pressure_solver not in N.SOLVERS:
+            raise ValueError(f"unknown linear solver: '{self.pressure_solver}'")
+        if self.precision not in N.PRECISIONS:
+            raise ValueError(f"unknown precision: '{self.precision}'")
+        s = N.Settings()
+        s.max_iterations, s.inner_iterations = self.max_iterations, self.inner_iterations
+        s.convergence_window, s.monitor_interval = self.convergence_window, self.monitor_interval
+        s.turb_start_iter, s.turb_update_interval = self.turb_start_iter, self.turb_update_interval
+        s.nut_floor_iters = self.nut_floor_iters
+        s.pressure_solver = N.SOLVERS[self.pressure_solver]
+        s.precision = N.PRECISIONS[self.precision]
+        s.block_threads = self.block_threads
+        s.convergence_tol, s.inner_tolerance = self.convergence_tol, self.inner_tolerance
+        s.divergence_limit = self.divergence_limit
+        s.alpha_u, s.alpha_p, s.alpha_k, s.alpha_omega = (
+            self.alpha_u, self.alpha_p, self.alpha_k, self.alpha_omega)
+        s.body_force[:] = (self.body_force.x, self.body_force.y, self.body_force.z)
+        s.k_min, s.k_max, s.omega_min = self.k_min, self.k_max, self.omega_min
+        return s
+
+
+@dataclass
+class FlowBoundaryConditions:
+    u_in: float
+    k_in: float
+    omega_in: float
+
+    @staticmethod
+    def channel_defaults(mesh: Mesh, u_in: float, k_in: float, omega_in: float):
+        """FlowBoundaryConditions::channelDefaults (BoundaryCondition.hpp:113-167): every
+        patch of the periodic meshes is a no-slip k-omega wall."""
+        return FlowBoundaryConditions(float(u_in), float(k_in), float(omega_in))
+
+
+# SSTCoefficients defaults (core/include/SSTModel.hpp:12-27), InferenceParameterSet order
+SST_DEFAULTS = (0.85, 0.5, 0.075, 5.0 / 9.0, 1.0, 0.856, 0.0828, 0.44, 0.09, 0.31, 0.41)
+SST_NAMES = ("sigma_k1", "sigma_w1", "beta1", "alpha1", "sigma_k2", "sigma_w2", "beta2",
+             "alpha2", "betaStar", "a1", "kappa")
+_LO = (0.1, 0.1, 0.01, 0.1, 0.1, 0.1, 0.01, 0.1, 0.01, 0.1, 0.35)
+_HI = (2.0, 2.0, 0.2, 1.5, 2.0, 2.0, 0.2, 1.5, 0.2, 0.8, 0.50)
+
+
+@dataclass
+class InferenceParameterSet:
+    """InferenceParameterSet (core/include/InferenceParameters.hpp:18-188)."""
+
+    name: str
+    active_indices: tuple
+    base: tuple = SST_DEFAULTS
+
+    def validate(self) -> None:
+        if not self.active_indices:
+            raise ValueError("inference parameters require at least one active index")
+        if any(i < 0 or i > 10 for i in self.active_indices):
+            raise ValueError("inference parameter index must be in [0,10]")
+        if len(set(self.active_indices)) != len(self.active_indices):
+            raise ValueError("inference parameter indices must be unique")
+
+    def n_active(self) -> int:
+        return len(self.active_indices)
+
+    def active_names(self) -> list:
+        return [SST_NAMES[i] for i in self.active_indices]
+
+    def lower_bounds(self) -> list:
+        return [_LO[i] for i in self.active_indices]
+
+    def upper_bounds(self) -> list:
+        return [_HI[i] for i in self.active_indices]
+
+    def in_bounds(self, theta) -> bool:
+        theta = list(theta)
+        if len(theta) != self.n_active():
+            return False
+        for v, lo, hi in zip(theta, self.lower_bounds(), self.upper_bounds()):
+            if v < lo or v > hi or math.isnan(v) or math.isinf(v):
+                return False
+        return True
+
+    def unpack(self, theta) -> list:
+        if len(theta) != self.n_active():
+            raise RuntimeError(f"theta size mismatch: expected {self.n_active()}, got {len(theta)}")
+        full = list(self.base)
+        for i, v in zip(self.active_indices, theta):
+            full[i] = float(v)
+        return full
+
+    def pack(self, coeffs) -> list:
+        return [coeffs[i] for i in self.active_indices]
+
+    @staticmethod
+    def a1_betaStar():
+        return InferenceParameterSet("a1_betaStar", (9, 8))
+
+    @staticmethod
+    def inlet_turb():
+        return InferenceParameterSet("inletTurb", (2, 1))
+
+    @staticmethod
+    def near_wall4():
+        return InferenceParameterSet("nearWall4", (9, 8, 2, 0))
+
+    @staticmethod
+    def all11():
+        return InferenceParameterSet("all11", tuple(range(11)))
+
+    @staticmethod
+    def live10():
+        return InferenceParameterSet("live10", tuple(range(10)))
+
+    @staticmethod
+    def from_indices(name, idx):
+        p = InferenceParameterSet(name, tuple(int(i) for i in idx))
+        p.validate()
+        return p
+
+
+@dataclass
+class _Probe:
+    location: Vec3
+    component: int
+    observed: float
+    sigma_obs: float
+    sigma_model: float
+
+
+class ObservationOperator:
+    """Velocity-profile observations (ObservationOperator::addVelocityProfile,
+    core/include/ObservationOperator.hpp:222-234) and the Gaussian log-likelihood."""
+
+    def __init__(self) -> None:
+        self._probes: list[_Probe] = []
+
+    def add_velocity_profile(self, location, comp, u_obs, sigma, sigma_model=0.0) -> None:
+        loc = location if isinstance(location, Vec3) else Vec3(*location)
+        if not all(math.isfinite(v) for v in (loc.x, loc.y, loc.z)):
+            raise ValueError("observation location must be finite")
+        if comp < 0 or comp > 2:
+            raise ValueError("velocity observation component must be in [0,2]")
+        var = sigma * sigma + sigma_model * sigma_model
+        if not (math.isfinite(u_obs) and math.isfinite(sigma) and sigma >= 0 and
+                math.isfinite(sigma_model) and sigma_model >= 0 and math.isfinite(var) and var > 0):
+            raise ValueError("Gaussian measurements require finite values, nonnegative "
+                             "uncertainties and finite positive total variance")
+        if self._probes and comp != self._probes[0].component:
+            raise NotImplementedError("one velocity component per problem on the B200 path")
+        self._probes.append(_Probe(loc, int(comp), float(u_obs), float(sigma), float(sigma_model)))
+
+    def n_obs(self) -> int:
+        return len(self._probes)
+
+    def log_likelihood_from_predictions(self, predictions) -> float:
+        """ObservationOperator::logLikelihood (ObservationOperator.hpp:592-609)."""
+        if len(predictions) != len(self._probes):
+            raise ValueError("Likelihood prediction count does not match observations")
+        ll = 0.0
+        for p, v in zip(self._probes, predictions):
+            if not math.isfinite(v):
+                raise ValueError("Likelihood predictions must be finite")
+            var = p.sigma_obs * p.sigma_obs + p.sigma_model * p.sigma_model
+            d = v - p.observed
+            ll += -0.5 * d * d / var
+        return ll
+
+    def arrays(self):
+        n = len(self._probes)
+        cols = np.zeros((5, n))
+        for i, p in enumerate(self._probes):
+            cols[:, i] = (p.location.x, p.location.y, p.observed, p.sigma_obs, p.sigma_model)
+        return [np.ascontiguousarray(c) for c in cols]
+
+
+@dataclass
+class EvaluationResult:
+    status: EvaluationStatus
+    log_lik: float
+    predictions: np.ndarray
+    simple_iters: int
+
+
+@dataclass
+class ForwardBatchRow:
+    result: EvaluationResult
+    final_worst_measure: float
+    contraction_rate_u: float
+    stalled: bool
+    error: str
+
+
+@dataclass
+class ForwardBatchResult:
+    rows: list
+    n_observations: int
+
+    @property
+    def predictions(self) -> np.ndarray:
+        if not self.rows:
+            return np.zeros((0, self.n_observations))
+        return np.stack([r.result.predictions for r in self.rows])
+
+    @property
+    def log_likelihoods(self) -> np.ndarray:
+        return np.array([r.result.log_lik for r in self.rows])
+
+    @property
+    def statuses(self) -> list:
+        return [r.result.status for r in self.rows]
+
+    @property
+    def iteration_counts(self) -> np.ndarray:
+        return np.array([r.result.simple_iters for r in self.rows], dtype=np.int32)
+
+    @property
+    def errors(self) -> list:
+        return [r.error for r in self.rows]
+
+    @property
+    def convergence_mask(self) -> np.ndarray:
+        return np.array([r.result.status == EvaluationStatus.Converged for r in self.rows])
+
+
+class _Problem:
+    """Owns one device-resident mesh class (rq_problem)."""
+
+    def __init__(self, mesh, params, obs, bcs, nu, settings, u_init, p_init, k_init, omega_init):
+        params.validate()
+        if not mesh.wall_distance_valid():
+            raise ValueError("ForwardBatch needs compute_wall_distance before construction")
+        self.params, self.obs = params, obs
+        self.mesh = mesh
+        self._keep = []
+        md = mesh.desc()
+        bc = N.BcDesc(bcs.u_in, bcs.k_in, bcs.omega_in)
+        st = settings.native()
+        od = N.ObsDesc()
+        od.n_obs = obs.n_obs()
+        if od.n_obs:
+            arrs = obs.arrays()
+            self._keep += arrs
+            od.component = obs._probes[0].component
+            od.x, od.y, od.observed, od.sigma_obs, od.sigma_model = (N.dptr(a) for a in arrs)
+        u = u_init if isinstance(u_init, Vec3) else Vec3(*u_init)
+        init = np.array([u.x, u.y, u.z, p_init, k_init, omega_init], dtype=np.float64)
+        active = np.array(params.active_indices, dtype=np.int32)
+        base = np.array(params.base, dtype=np.float64)
+        h = C.c_void_p()
+        N.call("rq_problem_create", C.byref(md), C.byref(bc), C.c_double(nu), C.byref(st),
+               C.byref(od), N.dptr(init), N.iptr(active), C.c_int32(len(active)), N.dptr(base),
+               C.byref(h))
+        self.handle = h
+        self.n_cells = mesh.n_cells()
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                N.lib().rq_problem_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+def _rows_from_native(out, pred, n_obs, params_n) -> list:
+    rows = []
+    for i, o in enumerate(out):
+        status = EvaluationStatus(o.status)
+        err = ""
+        if status == EvaluationStatus.InvalidParameters:
+            err = "coefficient row is nonfinite or out of bounds"
+        p = np.array(pred[i], dtype=np.float64) if n_obs else np.zeros(0)
+        rows.append(ForwardBatchRow(EvaluationResult(status, o.loglik, p, o.iterations),
+                                    o.final_worst, o.contraction_rate, bool(o.stalled), err))
+    return rows
+
+
+class ForwardBatch:
+    """ForwardBatch (rans-uq/include/ForwardBatch.hpp:23-125) on the GPU: every row is a
+    cold solve by one persistent CTA; rows are independent of batch order and size."""
+
+    def __init__(self, mesh, param_set, obs_op, bcs, nu, settings=None, u_init=Vec3(1, 0, 0),
+                 p_init=0.0, k_init=1e-4, omega_init=1.0):
+        settings = settings or SolverSettings()
+        self._problem = _Problem(mesh, param_set, obs_op, bcs, nu, settings, u_init, p_init,
+                                 k_init, omega_init)
+        self.param_set, self.obs_op = param_set, obs_op
+
+    def n_parameters(self) -> int:
+        return self.param_set.n_active()
+
+    def n_observations(self) -> int:
+        return self.obs_op.n_obs()
+
+    def evaluate(self, theta, workers: int = 1) -> ForwardBatchResult:
+        if int(workers) < 1:
+            raise ValueError("workers must be positive")
+        theta = np.ascontiguousarray(np.asarray(theta, dtype=np.float64))
+        if theta.ndim != 2 or theta.shape[1] != self.n_parameters():
+            raise ValueError("theta must have shape (n_rows, n_parameters)")
+        n, no = theta.shape[0], self.n_observations()
+        out = (N.RowOut * max(n, 1))()
+        pred = np.full((max(n, 1), max(no, 1)), np.nan)
+        if n:
+            N.call("rq_evaluate_batch", self._problem.handle, N.dptr(theta), C.c_int64(n), out,
+                   N.dptr(pred), None, None, C.c_int32(0))
+        return ForwardBatchResult(_rows_from_native(list(out)[:n], pred[:, :no], no,
+                                                    self.n_parameters()), no)
+
+    def evaluate_fields(self, theta, hist_cap: int = 0):
+        """Rows plus the final fields (n, 11, n_cells) and residual histories."""
+        theta = np.ascontiguousarray(np.asarray(theta, dtype=np.float64))
+        n, no, nc = theta.shape[0], self.n_observations(), self._problem.n_cells
+        out = (N.RowOut * max(n, 1))()
+        pred = np.full((max(n, 1), max(no, 1)), np.nan)
+        fields = np.zeros((max(n, 1), 11, nc))
+        hist = np.zeros((max(n, 1), max(hist_cap, 1), 11))
+        N.call("rq_evaluate_batch", self._problem.handle, N.dptr(theta), C.c_int64(n), out,
+               N.dptr(pred), N.dptr(fields), N.dptr(hist) if hist_cap else None,
+               C.c_int32(hist_cap))
+        res = ForwardBatchResult(_rows_from_native(list(out)[:n], pred[:, :no], no,
+                                                   self.n_parameters()), no)
+        return res, fields[:n], hist[:n, :hist_cap]
+
+
+def evaluate_multi(batches, problem_of_row, theta) -> ForwardBatchResult:
+    """Rows of several ForwardBatch mesh classes in ONE persistent launch
+    (rq_evaluate_multi): row i is evaluated by batches[problem_of_row[i]]."""
+    nb = len(batches)
+    handles = (C.c_void_p * nb)(*[b._problem.handle.value for b in batches])
+    pr = np.ascontiguousarray(np.asarray(problem_of_row, dtype=np.int32))
+    theta = np.ascontiguousarray(np.asarray(theta, dtype=np.float64))
+    n = theta.shape[0]
+    stride_t = theta.shape[1]
+    no = max(b.n_observations() for b in batches)
+    out = (N.RowOut * max(n, 1))()
+    pred = np.full((max(n, 1), max(no, 1)), np.nan)
+    N.call("rq_evaluate_multi", handles, C.c_int32(nb), N.iptr(pr), N.dptr(theta),
+           C.c_int32(stride_t), C.c_int64(n), out, N.dptr(pred), C.c_int32(max(no, 1)))
+    rows = []
+    for i, o in enumerate(list(out)[:n]):
+        b = batches[pr[i]]
+        k = b.n_observations()
+        rows.extend(_rows_from_native([o], pred[i:i + 1, :k], k, b.n_parameters()))
+    return ForwardBatchResult(rows, no)
+
+
+@dataclass
+class ForwardEvaluationResult:
+    result: EvaluationResult
+    final_worst_measure: float
+    contraction_rate_u: float
+    stalled: bool
+    error: str
+    fields: np.ndarray | None = None
+    history: np.ndarray | None = None
+
+
+class ForwardModel:
+    """ForwardModel (rans-uq/include/ForwardModel.hpp:199-281): one cold GPU solve per call.
+    The warm-start cache is not part of the B200 path (batches disable it too)."""
+
+    def __init__(self, mesh, param_set, obs_op, bcs, nu, settings=None, u_init=Vec3(1, 0, 0),
+                 p_init=0.0, k_init=1e-4, omega_init=1.0):
+        self._batch = ForwardBatch(mesh, param_set, obs_op, bcs, nu, settings, u_init, p_init,
+                                   k_init, omega_init)
+        self._last = None
+
+    def evaluate(self, theta) -> EvaluationResult:
+        return self.evaluate_with_diagnostics(theta).result
+
+    def evaluate_with_diagnostics(self, theta, snapshot: bool = False,
+                                  hist_cap: int = 0) -> ForwardEvaluationResult:
+        res, fields, hist = self._batch.evaluate_fields(np.asarray([theta], dtype=np.float64),
+                                                        hist_cap=hist_cap)
+        row = res.rows[0]
+        keep = row.result.status in (EvaluationStatus.Converged, EvaluationStatus.Unconverged)
+        self._last = fields[0] if keep else None
+        return ForwardEvaluationResult(row.result, row.final_worst_measure, row.contraction_rate_u,
+                                       row.stalled, row.error, fields[0] if keep else None,
+                                       hist[0] if hist_cap else None)
+
+    def penalized_log_likelihood(self, theta) -> float:
+        r = self.evaluate(theta)
+        return r.log_lik if r.status == EvaluationStatus.Converged else -1e30
+
+    def has_last_fields(self) -> bool:
+        return self._last is not None
+
+    def last_fields(self) -> np.ndarray:
+        if self._last is None:
+            raise RuntimeError("No fields retained for the last evaluation")
+        return self._last
+
+    def set_target_anisotropy(self, b_target):
+        raise NotImplementedError("Reynolds-stress injection is outside the B200 forward-model path")

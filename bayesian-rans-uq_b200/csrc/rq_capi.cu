@@ -1,0 +1,738 @@
+// C ABI of the B200 forward model (include/rq_b200.h). Host work here is the
+// per-mesh-class set-up (rq_setup.cpp), admission of inputs with the
+// reference's rules, and the launch of persistent solve CTAs; all per-draw
+// numerics run in rq_solver.cu.
+#include "../../include/rq_b200.h"
+#include "rq_device.cuh"
+#include "rq_kernels.h"
+#include "rq_setup.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+struct RqError : std::runtime_error {
+    int code;
+    RqError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        throw RqError(RQ_E_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        throw RqError(RQ_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F> int guarded(F &&f) {
+    try {
+        f();
+        return RQ_OK;
+    } catch (const RqError &e) {
+        g_error = e.what();
+        return e.code;
+    } catch (const std::invalid_argument &e) {
+        g_error = e.what();
+        return RQ_E_INVALID;
+    } catch (const std::bad_alloc &e) {
+        g_error = "host allocation failed";
+        return RQ_E_OOM;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        return RQ_E_CUDA;
+    }
+}
+
+// device allocation that frees itself
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p)
+            cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t b) {
+        if (b <= bytes)
+            return;
+        release();
+        check(cudaMalloc(&p, b), "cudaMalloc");
+        bytes = b;
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// The reference's parameter bounds (core/include/InferenceParameters.hpp:147-165).
+const double kLower[11] = {0.1, 0.1, 0.01, 0.1, 0.1, 0.1, 0.01, 0.1, 0.01, 0.1, 0.35};
+const double kUpper[11] = {2.0, 2.0, 0.2, 1.5, 2.0, 2.0, 0.2, 1.5, 0.2, 0.8, 0.50};
+
+long pad32(long n) { return (n + 31) / 32 * 32; }
+
+} // namespace
+
+struct rq_problem {
+    rq::StructMesh mesh;
+    rq::AmgHost amg;
+    rq::DevClass cls{};      // host copy with device pointers
+    DevBuf dCls, dDoubles, dInts;
+    std::vector<int32_t> active;
+    double base[11];
+    int32_t nObs = 0;
+    int block = 256;
+    // launch scratch, reused across calls
+    DevBuf dWs, dJobs, dRows, dPred, dFields, dHist, dTheta, dCounter;
+    std::mutex mu;
+};
+
+namespace {
+
+void validateSettings(const rq_settings &s) {
+    if (s.max_iterations < 0 || s.inner_iterations <= 0 || s.convergence_window < 2 ||
+        s.monitor_interval <= 0 || s.turb_update_interval <= 0 || s.turb_start_iter < 0 ||
+        s.nut_floor_iters < 0)
+        throw std::invalid_argument("invalid SIMPLE iteration count or cadence");
+    if (2 * s.convergence_window > rq::kWindowCap)
+        throw RqError(RQ_E_UNSUPPORTED, "convergence_window above 32 is not supported on the GPU path");
+    if (!std::isfinite(s.divergence_limit) || s.divergence_limit < 0)
+        throw std::invalid_argument("SIMPLE divergence limit must be finite and nonnegative");
+    if (!std::isfinite(s.convergence_tol) || s.convergence_tol < 0)
+        throw std::invalid_argument("SIMPLE convergence tolerance must be finite and nonnegative");
+    for (double v : {s.inner_tolerance, s.alpha_u, s.alpha_k, s.alpha_omega})
+        if (!std::isfinite(v) || v <= 0)
+            throw std::invalid_argument("SIMPLE tolerances and relaxation denominators must be finite and positive");
+    if (!std::isfinite(s.alpha_p) || s.alpha_p < 0)
+        throw std::invalid_argument("SIMPLE pressure/source relaxation must be finite and nonnegative");
+    for (double v : s.body_force)
+        if (!std::isfinite(v))
+            throw std::invalid_argument("SIMPLE body force must be finite");
+    if (s.body_force[2] != 0.0)
+        throw RqError(RQ_E_UNSUPPORTED, "the 2-D GPU path takes no spanwise body force");
+    for (double v : {s.k_min, s.k_max, s.omega_min})
+        if (!std::isfinite(v) || v < 0)
+            throw std::invalid_argument("SIMPLE turbulence limits must be finite and nonnegative");
+    if (s.k_max < s.k_min)
+        throw std::invalid_argument("SIMPLE kMax must be at least kMin");
+    if (s.pressure_solver < 0 || s.pressure_solver > 2)
+        throw std::invalid_argument("unknown pressure solver");
+    if (s.precision != RQ_PREC_FP64 && s.precision != RQ_PREC_MIXED)
+        throw std::invalid_argument("unknown precision");
+    if (s.block_threads != 0 &&
+        (s.block_threads < 64 || s.block_threads > 512 || s.block_threads % 32 != 0))
+        throw std::invalid_argument("block_threads must be 0 or a multiple of 32 in [64, 512]");
+}
+
+rq::StructMesh buildMesh(const rq_mesh_desc &d) {
+    if (d.kind == RQ_MESH_PERIODIC_CHANNEL) {
+        if (d.nx < 3 || d.ny < 1)
+            throw std::invalid_argument("periodic channel needs nx >= 3 and ny >= 1");
+        return rq::makePeriodicChannel(d.nx, d.ny, d.lx, d.h, d.re_tau, d.yplus);
+    }
+    if (d.kind == RQ_MESH_CURVED_PERIODIC) {
+        if (!d.x_nodes || !d.y_bottom || d.nx < 3)
+            throw std::invalid_argument("curved mesh needs nx >= 3 and nx+1 node samples");
+        std::vector<double> xn(d.x_nodes, d.x_nodes + d.nx + 1), yb(d.y_bottom, d.y_bottom + d.nx + 1);
+        return rq::makeCurvedPeriodic(xn, yb, d.y_top, d.ny, d.re, d.yplus);
+    }
+    throw std::invalid_argument("unknown mesh kind");
+}
+
+// Upload the class arrays and fill the device descriptor.
+void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings &s,
+            const double init[6]) {
+    const rq::StructMesh &m = P.mesh;
+    const rq::AmgHost &h = P.amg;
+    std::vector<double> D;
+    std::vector<int32_t> I;
+    std::vector<std::pair<const double **, size_t>> dptr;
+    std::vector<std::pair<const int32_t **, size_t>> iptr;
+    rq::DevClass &C = P.cls;
+    auto addD = [&](const double **slot, const std::vector<double> &v) {
+        dptr.push_back({slot, D.size()});
+        D.insert(D.end(), v.begin(), v.end());
+        while (D.size() % 4)
+            D.push_back(0.0);
+    };
+    auto addI = [&](const int32_t **slot, const std::vector<int32_t> &v) {
+        iptr.push_back({slot, I.size()});
+        I.insert(I.end(), v.begin(), v.end());
+        while (I.size() % 8)
+            I.push_back(0);
+    };
+    C.nx = m.nx;
+    C.ny = m.ny;
+    C.n = m.n;
+    C.nfy = m.nfy();
+    C.balance = m.balance ? 1 : 0;
+    C.nu = nu;
+    C.beta1Init = 0.075; // applyAllBCs -> applyOmegaBC default (BoundaryCondition.hpp:361, 416-422)
+    for (int i = 0; i < 6; ++i)
+        C.init[i] = init[i];
+    rq::DevSettings &st = C.st;
+    st.maxIter = s.max_iterations;
+    st.innerIter = s.inner_iterations;
+    st.window = s.convergence_window;
+    st.monitorInterval = s.monitor_interval;
+    st.turbStart = s.turb_start_iter;
+    st.turbInterval = s.turb_update_interval;
+    st.floorIters = s.nut_floor_iters;
+    st.pSolver = s.pressure_solver;
+    st.precision = s.precision;
+    st.tol = s.convergence_tol;
+    st.innerTol = s.inner_tolerance;
+    st.divLimit = s.divergence_limit;
+    st.aU = s.alpha_u;
+    st.aP = s.alpha_p;
+    st.aK = s.alpha_k;
+    st.aW = s.alpha_omega;
+    st.fx = s.body_force[0];
+    st.fy = s.body_force[1];
+    st.kMin = s.k_min;
+    st.kMax = s.k_max;
+    st.wMin = s.omega_min;
+    addD(&C.cx, m.cx);
+    addD(&C.cy, m.cy);
+    addD(&C.vol, m.vol);
+    addD(&C.wd, m.wd);
+    addD(&C.xa, m.xa);
+    addD(&C.xnx, m.xnx);
+    addD(&C.xny, m.xny);
+    addD(&C.xw, m.xw);
+    addD(&C.xdl, m.xdl);
+    addD(&C.xdx, m.xdx);
+    addD(&C.xdy, m.xdy);
+    addD(&C.xsh, m.xsh);
+    addD(&C.ya, m.ya);
+    addD(&C.ynx, m.ynx);
+    addD(&C.yny, m.yny);
+    addD(&C.yw, m.yw);
+    addD(&C.ydl, m.ydl);
+    addD(&C.ydx, m.ydx);
+    addD(&C.ydy, m.ydy);
+    if (m.balance) {
+        addD(&C.sing, m.sing);
+        addD(&C.slap, m.slap);
+        addD(&C.sgx, m.sgx);
+        addD(&C.sgy, m.sgy);
+    }
+    // probes
+    const int nobs = obs ? obs->n_obs : 0;
+    if (nobs < 0 || nobs > rq::kMaxProbes)
+        throw RqError(RQ_E_UNSUPPORTED, "at most 64 observations per problem on the GPU path");
+    C.nobs = nobs;
+    C.obsComp = obs ? obs->component : 0;
+    if (nobs > 0) {
+        if (C.obsComp < 0 || C.obsComp > 2)
+            throw std::invalid_argument("velocity observation component must be in [0,2]");
+        if (C.obsComp == 2)
+            throw RqError(RQ_E_UNSUPPORTED, "the 2-D GPU path observes x or y velocity only");
+        std::vector<int32_t> cell(nobs), nnb(nobs), nb(4 * nobs);
+        std::vector<double> ox(nobs), oy(nobs), axx(nobs), axy(nobs), ayy(nobs), det(nobs),
+            dx(4 * nobs), dy(4 * nobs), wt(4 * nobs), val(nobs), var(nobs), fl(nobs);
+        for (int t = 0; t < nobs; ++t) {
+            const double so = obs->sigma_obs[t], sm = obs->sigma_model ? obs->sigma_model[t] : 0.0;
+            const double variance = so * so + sm * sm; // Measurement::totalVariance
+            if (!std::isfinite(obs->observed[t]) || !std::isfinite(so) || so < 0 ||
+                !std::isfinite(sm) || sm < 0 || !std::isfinite(variance) || variance <= 0)
+                throw std::invalid_argument(
+                    "Gaussian measurements require finite values, nonnegative uncertainties "
+                    "and finite positive total variance");
+            if (!std::isfinite(obs->x[t]) || !std::isfinite(obs->y[t]))
+                throw std::invalid_argument("observation location must be finite");
+            const rq::ProbeHost p = rq::prepareProbe(m, obs->x[t], obs->y[t]);
+            cell[t] = p.cell;
+            nnb[t] = p.nnb;
+            ox[t] = p.ox;
+            oy[t] = p.oy;
+            axx[t] = p.axx;
+            axy[t] = p.axy;
+            ayy[t] = p.ayy;
+            det[t] = p.det;
+            for (int k = 0; k < 4; ++k) {
+                nb[4 * t + k] = p.nb[k];
+                dx[4 * t + k] = p.dx[k];
+                dy[4 * t + k] = p.dy[k];
+                wt[4 * t + k] = p.wt[k];
+            }
+            val[t] = obs->observed[t];
+            var[t] = variance;
+            fl[t] = std::sqrt(variance); // monitor floor sigma_i (ForwardModel.cpp:64-71)
+        }
+        addI(&C.pcell, cell);
+        addI(&C.pnnb, nnb);
+        addI(&C.pnb, nb);
+        addD(&C.pox, ox);
+        addD(&C.poy, oy);
+        addD(&C.paxx, axx);
+        addD(&C.paxy, axy);
+        addD(&C.payy, ayy);
+        addD(&C.pdet, det);
+        addD(&C.pdx, dx);
+        addD(&C.pdy, dy);
+        addD(&C.pwt, wt);
+        addD(&C.obsVal, val);
+        addD(&C.obsVar, var);
+        addD(&C.obsFloor, fl);
+    }
+    // AMG hierarchy
+    const int L = static_cast<int>(h.lev.size());
+    if (L > rq::kMaxLevels)
+        throw RqError(RQ_E_UNSUPPORTED, "AMG hierarchy deeper than 12 levels");
+    if (h.coarseN() > rq::kMaxCoarse)
+        throw RqError(RQ_E_UNSUPPORTED, "coarsest AMG level above 64 rows");
+    C.nlev = L;
+    int valOff = 0, vecOff = 0;
+    for (int l = 0; l < L; ++l) {
+        const auto &Lv = h.lev[l];
+        rq::DevAmgLevel &dl = C.lev[l];
+        dl.n = Lv.n;
+        dl.nnz = l > 0 ? static_cast<int>(Lv.col.size()) : 0;
+        dl.valOff = valOff;
+        dl.vecOff = vecOff;
+        if (l > 0) {
+            valOff += static_cast<int>(pad32(dl.nnz));
+            addI(&dl.ptr, Lv.ptr);
+            addI(&dl.col, Lv.col);
+            addI(&dl.diagPos, Lv.diagPos);
+        }
+        if (l > 0 || L == 1)
+            vecOff += static_cast<int>(pad32(4L * Lv.n));
+        if (l + 1 < L) {
+            addI(&dl.agg, Lv.agg);
+            addI(&dl.childPtr, Lv.childPtr);
+            addI(&dl.childIdx, Lv.childIdx);
+            addI(&dl.gPtr, Lv.gPtr);
+            addI(&dl.gSrc, Lv.gSrc);
+        }
+    }
+    C.amgVals = valOff;
+    C.amgVecs = vecOff;
+    const long n = m.n, nf = m.n + m.nfy(), mc = h.coarseN();
+    C.wsDoubles = 46 * pad32(n) + 4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
+    // upload and patch pointers
+    P.dDoubles.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
+    P.dInts.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));
+    check(cudaMemcpy(P.dDoubles.p, D.data(), D.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(P.dInts.p, I.data(), I.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+    for (auto &e : dptr)
+        *e.first = P.dDoubles.as<double>() + e.second;
+    for (auto &e : iptr)
+        *e.first = P.dInts.as<int32_t>() + e.second;
+    P.dCls.ensure(sizeof(rq::DevClass));
+    check(cudaMemcpy(P.dCls.p, &C, sizeof(rq::DevClass), cudaMemcpyHostToDevice), "upload");
+}
+
+int defaultBlock(int n) {
+    if (n <= 512)
+        return 256;
+    return 512;
+}
+
+// Unpack theta -> 11 coefficients with the reference's admission
+// (InferenceParameterSet::inBounds / unpack, InferenceParameters.hpp:67-77, 127-140).
+bool unpackRow(const rq_problem &P, const double *theta, double out[11]) {
+    for (int i = 0; i < 11; ++i)
+        out[i] = P.base[i];
+    for (size_t a = 0; a < P.active.size(); ++a) {
+        const int idx = P.active[a];
+        const double v = theta[a];
+        if (v < kLower[idx] || v > kUpper[idx] || std::isnan(v) || std::isinf(v))
+            return false;
+        out[idx] = v;
+    }
+    return true;
+}
+
+struct Launch {
+    std::vector<rq::DevJob> jobs;
+    std::vector<int64_t> rowOf; // job -> output row
+};
+
+// Runs jobs (already filled except output pointers) for rows that were admitted.
+void runJobs(rq_problem &owner, std::vector<rq::DevJob> &jobs, const std::vector<const rq_problem *> &probOfJob,
+             rq::RowOut *dRows, double *dPred, int predStride, double *dFields, long fieldStride,
+             double *dHist, int histCap, cudaStream_t stream) {
+    const int nj = static_cast<int>(jobs.size());
+    if (nj == 0)
+        return;
+    int block = 64;
+    long wsStride = 0;
+    for (const auto *p : probOfJob) {
+        block = std::max(block, p->block);
+        wsStride = std::max(wsStride, static_cast<long>(p->cls.wsDoubles));
+    }
+    int dev = 0, sms = 1;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
+    const int perSM = rq::solveBlocksPerSM(block);
+    const int grid = std::max(1, std::min(nj, sms * perSM));
+    for (int j = 0; j < nj; ++j) {
+        jobs[j].row = dRows + j;
+        jobs[j].pred = dPred + static_cast<long>(j) * predStride;
+        jobs[j].fields = dFields ? dFields + static_cast<long>(j) * fieldStride : nullptr;
+        jobs[j].hist = dHist ? dHist + static_cast<long>(j) * histCap * 11 : nullptr;
+        jobs[j].histCap = histCap;
+    }
+    owner.dJobs.ensure(sizeof(rq::DevJob) * nj);
+    owner.dWs.ensure(sizeof(double) * wsStride * grid);
+    owner.dCounter.ensure(sizeof(int));
+    check(cudaMemcpyAsync(owner.dJobs.p, jobs.data(), sizeof(rq::DevJob) * nj, cudaMemcpyHostToDevice, stream), "jobs");
+    check(cudaMemsetAsync(owner.dCounter.p, 0, sizeof(int), stream), "counter");
+    check(rq::launchSolve(owner.dJobs.as<rq::DevJob>(), nj, owner.dCounter.as<int>(),
+                          owner.dWs.as<double>(), wsStride, grid, block, stream),
+          "solve launch");
+}
+
+} // namespace
+
+extern "C" {
+
+const char *rq_last_error(void) { return g_error.c_str(); }
+int rq_version(void) { return 100; }
+
+int rq_default_settings(rq_settings *s) {
+    return guarded([&] {
+        if (!s)
+            throw std::invalid_argument("null settings");
+        std::memset(s, 0, sizeof(*s));
+        s->max_iterations = 500;
+        s->inner_iterations = 200;
+        s->convergence_window = 25;
+        s->monitor_interval = 10;
+        s->turb_start_iter = 5;
+        s->turb_update_interval = 1;
+        s->nut_floor_iters = 500;
+        s->pressure_solver = RQ_SOLVER_AMG;
+        s->precision = RQ_PREC_FP64;
+        s->block_threads = 0;
+        s->convergence_tol = 1e-5;
+        s->inner_tolerance = 1e-3;
+        s->divergence_limit = 1e6;
+        s->alpha_u = 0.7;
+        s->alpha_p = 0.3;
+        s->alpha_k = 0.5;
+        s->alpha_omega = 0.5;
+        s->k_min = 1e-10;
+        s->k_max = 1e10;
+        s->omega_min = 1e-6;
+    });
+}
+
+int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
+                      const rq_settings *settings, const rq_obs_desc *obs, const double init[6],
+                      const int32_t *active, int32_t n_active, const double base[11],
+                      rq_problem **out) {
+    return guarded([&] {
+        if (!mesh || !bc || !settings || !init || !active || !base || !out)
+            throw std::invalid_argument("null argument");
+        *out = nullptr;
+        // simple_admission::problem / initial (rans-uq/include/SIMPLEValidation.hpp:10-60)
+        if (!std::isfinite(nu) || nu <= 0)
+            throw std::invalid_argument("SIMPLE kinematic viscosity must be finite and positive");
+        validateSettings(*settings);
+        if (!std::isfinite(bc->u_in) || !std::isfinite(bc->k_in) || !std::isfinite(bc->omega_in))
+            throw std::invalid_argument("active boundary values must be finite");
+        for (int i = 0; i < 4; ++i)
+            if (!std::isfinite(init[i]))
+                throw std::invalid_argument("SIMPLE initial velocity and pressure must be finite");
+        if (!std::isfinite(init[4]) || init[4] < 0)
+            throw std::invalid_argument("SIMPLE initial k must be finite and nonnegative");
+        if (!std::isfinite(init[5]) || init[5] <= 0)
+            throw std::invalid_argument("SIMPLE initial omega must be finite and positive");
+        if (init[2] != 0.0)
+            throw RqError(RQ_E_UNSUPPORTED, "the 2-D GPU path starts from zero spanwise velocity");
+        if (n_active < 1 || n_active > 11)
+            throw std::invalid_argument("inference parameters require at least one active index");
+        bool seen[11] = {};
+        for (int a = 0; a < n_active; ++a) {
+            if (active[a] < 0 || active[a] > 10)
+                throw std::invalid_argument("inference parameter index must be in [0,10]");
+            if (seen[active[a]])
+                throw std::invalid_argument("inference parameter indices must be unique");
+            seen[active[a]] = true;
+        }
+        for (int i = 0; i < 11; ++i)
+            if (!std::isfinite(base[i]) || base[i] < 0)
+                throw std::invalid_argument("SST coefficients must be finite and nonnegative");
+        if (base[2] == 0 || base[8] == 0)
+            throw std::invalid_argument("SST beta1 and betaStar must be positive");
+        auto P = std::make_unique<rq_problem>();
+        P->mesh = buildMesh(*mesh);
+        P->amg = rq::buildAmg(P->mesh);
+        P->active.assign(active, active + n_active);
+        std::memcpy(P->base, base, sizeof(P->base));
+        P->nObs = obs ? obs->n_obs : 0;
+        P->block = settings->block_threads ? settings->block_threads : defaultBlock(P->mesh.n);
+        upload(*P, obs, nu, *settings, init);
+        *out = P.release();
+    });
+}
+
+int rq_problem_destroy(rq_problem *p) {
+    return guarded([&] { delete p; });
+}
+
+int rq_problem_info(const rq_problem *p, int32_t *n_cells, int32_t *n_obs, int32_t *n_active,
+                    int32_t *amg_levels) {
+    return guarded([&] {
+        if (!p)
+            throw std::invalid_argument("null problem");
+        if (n_cells)
+            *n_cells = p->mesh.n;
+        if (n_obs)
+            *n_obs = p->nObs;
+        if (n_active)
+            *n_active = static_cast<int32_t>(p->active.size());
+        if (amg_levels)
+            *amg_levels = static_cast<int32_t>(p->amg.lev.size());
+    });
+}
+
+int rq_evaluate_multi(rq_problem *const *problems, int32_t n_problems,
+                      const int32_t *problem_of_row, const double *theta, int32_t theta_stride,
+                      int64_t n, rq_row_out *rows, double *predictions, int32_t pred_stride) {
+    return guarded([&] {
+        if (!problems || n_problems < 1 || (n > 0 && (!problem_of_row || !theta || !rows || !predictions)))
+            throw std::invalid_argument("null argument");
+        if (n < 0)
+            throw std::invalid_argument("negative row count");
+        if (n == 0)
+            return;
+        int maxActive = 0, maxObs = 0;
+        for (int i = 0; i < n_problems; ++i) {
+            if (!problems[i])
+                throw std::invalid_argument("null problem");
+            maxActive = std::max<int>(maxActive, static_cast<int>(problems[i]->active.size()));
+            maxObs = std::max(maxObs, problems[i]->nObs);
+        }
+        if (theta_stride < maxActive || pred_stride < std::max(maxObs, 1))
+            throw std::invalid_argument("theta/prediction stride below the problems' widths");
+        rq_problem &owner = *problems[0];
+        std::lock_guard<std::mutex> lock(owner.mu);
+        std::vector<rq::DevJob> jobs;
+        std::vector<const rq_problem *> probOfJob;
+        std::vector<int64_t> rowOfJob;
+        const double nan = std::nan("");
+        for (int64_t r = 0; r < n; ++r) {
+            const int pi = problem_of_row[r];
+            if (pi < 0 || pi >= n_problems)
+                throw std::invalid_argument("problem index out of range");
+            const rq_problem &P = *problems[pi];
+            double coeffs[11];
+            for (int t = 0; t < pred_stride; ++t)
+                predictions[r * pred_stride + t] = nan;
+            if (!unpackRow(P, theta + r * theta_stride, coeffs)) {
+                rows[r] = rq_row_out{RQ_INVALID_PARAMETERS, 0, 0, 0, -1e30, nan, nan};
+                continue;
+            }
+            rq::DevJob j{};
+            j.cls = P.dCls.as<rq::DevClass>();
+            std::memcpy(j.coeffs, coeffs, sizeof(coeffs));
+            jobs.push_back(j);
+            probOfJob.push_back(&P);
+            rowOfJob.push_back(r);
+        }
+        // longest solves first (cells as the cost proxy); results do not depend on order
+        std::vector<int> order(jobs.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return probOfJob[a]->mesh.n > probOfJob[b]->mesh.n;
+        });
+        std::vector<rq::DevJob> sj;
+        std::vector<const rq_problem *> sp;
+        std::vector<int64_t> sr;
+        for (int k : order) {
+            sj.push_back(jobs[k]);
+            sp.push_back(probOfJob[k]);
+            sr.push_back(rowOfJob[k]);
+        }
+        const int nj = static_cast<int>(sj.size());
+        if (nj == 0)
+            return;
+        owner.dRows.ensure(sizeof(rq::RowOut) * nj);
+        owner.dPred.ensure(sizeof(double) * nj * pred_stride);
+        runJobs(owner, sj, sp, owner.dRows.as<rq::RowOut>(), owner.dPred.as<double>(), pred_stride,
+                nullptr, 0, nullptr, 0, nullptr);
+        std::vector<rq::RowOut> hr(nj);
+        std::vector<double> hp(static_cast<size_t>(nj) * pred_stride);
+        check(cudaMemcpy(hr.data(), owner.dRows.p, sizeof(rq::RowOut) * nj, cudaMemcpyDeviceToHost), "rows");
+        check(cudaMemcpy(hp.data(), owner.dPred.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost), "predictions");
+        for (int k = 0; k < nj; ++k) {
+            const int64_t r = sr[k];
+            const rq::RowOut &o = hr[k];
+            rows[r] = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik,
+                                 o.finalWorst, o.contractionRate};
+            const int no = sp[k]->nObs;
+            for (int t = 0; t < no; ++t)
+                predictions[r * pred_stride + t] = hp[static_cast<size_t>(k) * pred_stride + t];
+        }
+    });
+}
+
+int rq_evaluate_batch(rq_problem *p, const double *theta, int64_t n, rq_row_out *rows,
+                      double *predictions, double *fields, double *history, int32_t hist_cap) {
+    if (!fields && !history) {
+        std::vector<int32_t> pr(static_cast<size_t>(std::max<int64_t>(n, 0)), 0);
+        rq_problem *ps[1] = {p};
+        const int na = p ? static_cast<int>(p->active.size()) : 0;
+        const int no = p ? std::max(p->nObs, 1) : 1;
+        if (p && p->nObs == 0) { // predictions buffer has zero width: use scratch
+            std::vector<double> scratch(static_cast<size_t>(std::max<int64_t>(n, 0)));
+            return rq_evaluate_multi(ps, 1, pr.data(), theta, na, n, rows, scratch.data(), 1);
+        }
+        return rq_evaluate_multi(ps, 1, pr.data(), theta, na, n, rows, predictions, no);
+    }
+    return guarded([&] {
+        if (!p || (n > 0 && (!theta || !rows)))
+            throw std::invalid_argument("null argument");
+        if (n < 0 || hist_cap < 0)
+            throw std::invalid_argument("negative size");
+        std::lock_guard<std::mutex> lock(p->mu);
+        const double nan = std::nan("");
+        const int no = std::max(p->nObs, 1), nc = p->mesh.n;
+        std::vector<rq::DevJob> jobs;
+        std::vector<const rq_problem *> probs;
+        std::vector<int64_t> rowOf;
+        for (int64_t r = 0; r < n; ++r) {
+            double coeffs[11];
+            if (!unpackRow(*p, theta + r * p->active.size(), coeffs)) {
+                rows[r] = rq_row_out{RQ_INVALID_PARAMETERS, 0, 0, 0, -1e30, nan, nan};
+                if (predictions)
+                    for (int t = 0; t < p->nObs; ++t)
+                        predictions[r * p->nObs + t] = nan;
+                if (fields)
+                    for (long e = 0; e < 11L * nc; ++e)
+                        fields[r * 11L * nc + e] = nan;
+                continue;
+            }
+            rq::DevJob j{};
+            j.cls = p->dCls.as<rq::DevClass>();
+            std::memcpy(j.coeffs, coeffs, sizeof(coeffs));
+            jobs.push_back(j);
+            probs.push_back(p);
+            rowOf.push_back(r);
+        }
+        const int nj = static_cast<int>(jobs.size());
+        if (nj == 0)
+            return;
+        p->dRows.ensure(sizeof(rq::RowOut) * nj);
+        p->dPred.ensure(sizeof(double) * nj * no);
+        if (fields)
+            p->dFields.ensure(sizeof(double) * nj * 11L * nc);
+        if (history && hist_cap > 0)
+            p->dHist.ensure(sizeof(double) * nj * 11L * hist_cap);
+        runJobs(*p, jobs, probs, p->dRows.as<rq::RowOut>(), p->dPred.as<double>(), no,
+                fields ? p->dFields.as<double>() : nullptr, 11L * nc,
+                (history && hist_cap > 0) ? p->dHist.as<double>() : nullptr, hist_cap, nullptr);
+        std::vector<rq::RowOut> hr(nj);
+        std::vector<double> hp(static_cast<size_t>(nj) * no);
+        check(cudaMemcpy(hr.data(), p->dRows.p, sizeof(rq::RowOut) * nj, cudaMemcpyDeviceToHost), "rows");
+        check(cudaMemcpy(hp.data(), p->dPred.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost), "predictions");
+        std::vector<double> hf, hh;
+        if (fields) {
+            hf.resize(static_cast<size_t>(nj) * 11 * nc);
+            check(cudaMemcpy(hf.data(), p->dFields.p, sizeof(double) * hf.size(), cudaMemcpyDeviceToHost), "fields");
+        }
+        if (history && hist_cap > 0) {
+            hh.resize(static_cast<size_t>(nj) * 11 * hist_cap);
+            check(cudaMemcpy(hh.data(), p->dHist.p, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost), "history");
+        }
+        for (int k = 0; k < nj; ++k) {
+            const int64_t r = rowOf[k];
+            const rq::RowOut &o = hr[k];
+            rows[r] = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik,
+                                 o.finalWorst, o.contractionRate};
+            if (predictions)
+                for (int t = 0; t < p->nObs; ++t)
+                    predictions[r * p->nObs + t] = hp[static_cast<size_t>(k) * no + t];
+            if (fields)
+                std::memcpy(fields + r * 11L * nc, hf.data() + static_cast<size_t>(k) * 11 * nc,
+                            sizeof(double) * 11 * nc);
+            if (history && hist_cap > 0)
+                std::memcpy(history + r * 11L * hist_cap, hh.data() + static_cast<size_t>(k) * 11 * hist_cap,
+                            sizeof(double) * 11 * hist_cap);
+        }
+    });
+}
+
+int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *predictions,
+             double *fields, double *history, int32_t hist_cap) {
+    return guarded([&] {
+        if (!p || !coeffs || !row)
+            throw std::invalid_argument("null argument");
+        for (int i = 0; i < 11; ++i)
+            if (!std::isfinite(coeffs[i]) || coeffs[i] < 0)
+                throw std::invalid_argument("SST coefficients must be finite and nonnegative");
+        if (coeffs[2] == 0 || coeffs[8] == 0)
+            throw std::invalid_argument("SST beta1 and betaStar must be positive");
+        std::lock_guard<std::mutex> lock(p->mu);
+        const int no = std::max(p->nObs, 1), nc = p->mesh.n;
+        std::vector<rq::DevJob> jobs(1);
+        jobs[0].cls = p->dCls.as<rq::DevClass>();
+        std::memcpy(jobs[0].coeffs, coeffs, sizeof(double) * 11);
+        std::vector<const rq_problem *> probs{p};
+        p->dRows.ensure(sizeof(rq::RowOut));
+        p->dPred.ensure(sizeof(double) * no);
+        if (fields)
+            p->dFields.ensure(sizeof(double) * 11L * nc);
+        if (history && hist_cap > 0)
+            p->dHist.ensure(sizeof(double) * 11L * hist_cap);
+        runJobs(*p, jobs, probs, p->dRows.as<rq::RowOut>(), p->dPred.as<double>(), no,
+                fields ? p->dFields.as<double>() : nullptr, 11L * nc,
+                (history && hist_cap > 0) ? p->dHist.as<double>() : nullptr, hist_cap, nullptr);
+        rq::RowOut o;
+        check(cudaMemcpy(&o, p->dRows.p, sizeof(o), cudaMemcpyDeviceToHost), "row");
+        *row = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik, o.finalWorst,
+                          o.contractionRate};
+        if (predictions && p->nObs > 0)
+            check(cudaMemcpy(predictions, p->dPred.p, sizeof(double) * p->nObs, cudaMemcpyDeviceToHost), "predictions");
+        if (fields)
+            check(cudaMemcpy(fields, p->dFields.p, sizeof(double) * 11 * nc, cudaMemcpyDeviceToHost), "fields");
+        if (history && hist_cap > 0)
+            check(cudaMemcpy(history, p->dHist.p, sizeof(double) * 11 * hist_cap, cudaMemcpyDeviceToHost), "history");
+    });
+}
+
+int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells) {
+    return guarded([&] {
+        if (!mesh || !n_cells)
+            throw std::invalid_argument("null argument");
+        const rq::StructMesh m = buildMesh(*mesh);
+        *n_cells = m.n;
+        if (cells)
+            for (int c = 0; c < m.n; ++c) {
+                cells[4 * c] = m.cx[c];
+                cells[4 * c + 1] = m.cy[c];
+                cells[4 * c + 2] = m.vol[c];
+                cells[4 * c + 3] = m.wd[c];
+            }
+    });
+}
+
+int rq_evaluate_multi_device(rq_problem *const *, int32_t, const int32_t *, const double *, int32_t,
+                             int64_t, rq_row_out *, double *, int32_t, void *) {
+    g_error = "rq_evaluate_multi_device is not available in this build";
+    return RQ_E_UNSUPPORTED;
+}
+
+int rq_linear_solve(const rq_ldu *, double *, int32_t, double, int32_t, rq_solver_result *) {
+    g_error = "rq_linear_solve is not available in this build";
+    return RQ_E_UNSUPPORTED;
+}
+
+} // extern "C"

@@ -1,0 +1,80 @@
+// Device-side data layout of the B200 forward model. One mesh class (mesh,
+// boundary conditions, viscosity, settings, probes, AMG pattern) lives in HBM
+// once; every coefficient draw is a job that one CTA runs from cold start to
+// its verdict without leaving the GPU (see rq_solver.cu).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace rq {
+
+constexpr int kMaxLevels = 12;    // AMG levels (the reference allows 20; meshes here need <= 8)
+constexpr int kMaxCoarse = 64;    // rows of the dense coarsest AMG level
+constexpr int kMaxProbes = 64;    // observations per problem
+constexpr int kWindowCap = 64;    // 2 * convergenceWindow samples kept per estimator
+
+enum Precision : int32_t { kFP64 = 0, kMixed = 1 };
+enum PSolver : int32_t { kPAmg = 0, kPPcg = 1, kPBicgstab = 2 };
+
+// SolverSettings subset of the hot path (rans-uq FlowFields.hpp:70-241).
+struct DevSettings {
+    int32_t maxIter, innerIter, window, monitorInterval;
+    int32_t turbStart, turbInterval, floorIters, pSolver;
+    int32_t precision, pad;
+    double tol, innerTol, divLimit;
+    double aU, aP, aK, aW;
+    double fx, fy;
+    double kMin, kMax, wMin;
+};
+
+struct DevAmgLevel {
+    int32_t n, nnz;             // rows; CSR nnz (levels >= 1)
+    int32_t valOff, vecOff;     // per-solve value / vector offsets (levels >= 1)
+    const int32_t *ptr, *col, *diagPos;
+    const int32_t *agg;                  // row -> next-level row
+    const int32_t *childPtr, *childIdx;  // next-level row -> rows of this level
+    const int32_t *gPtr, *gSrc;          // next-level nnz -> entries of this level
+};
+
+struct DevClass {
+    int32_t nx, ny, n, nfy;
+    int32_t balance, nobs, nlev, obsComp;
+    double nu, beta1Init;      // beta1 of the initial wall-omega face value (applyAllBCs default)
+    double init[6];            // U xyz, p, k, omega
+    DevSettings st;
+    // cells
+    const double *cx, *cy, *vol, *wd;
+    // east faces (n)
+    const double *xa, *xnx, *xny, *xw, *xdl, *xdx, *xdy, *xsh;
+    // y faces (n + nx)
+    const double *ya, *ynx, *yny, *yw, *ydl, *ydx, *ydy;
+    // planar singular omega balance
+    const double *sing, *slap, *sgx, *sgy;
+    // probes: 4 neighbour slots each
+    const int32_t *pcell, *pnnb, *pnb;
+    const double *pox, *poy, *paxx, *paxy, *payy, *pdet, *pdx, *pdy, *pwt;
+    const double *obsVal, *obsVar, *obsFloor;
+    DevAmgLevel lev[kMaxLevels];
+    int32_t amgVals, amgVecs;  // per-solve doubles for coarse values / vectors
+    int64_t wsDoubles;         // per-solve workspace
+};
+
+// Outcome of one draw; the status values and order follow EvaluationStatus
+// (core/include/EvaluationTypes.hpp:6).
+struct RowOut {
+    int32_t status, iterations, stalled, converged;
+    double loglik, finalWorst, contractionRate;
+};
+
+struct DevJob {
+    const DevClass *cls;
+    double coeffs[11];
+    RowOut *row;
+    double *pred;      // nobs
+    double *fields;    // optional 11 x n
+    double *hist;      // optional hist_cap x 11
+    int32_t histCap;
+    int32_t pad;
+};
+
+} // namespace rq

@@ -1,0 +1,17 @@
+// Launch entry points of the device code (rq_solver.cu), used by rq_capi.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "rq_device.cuh"
+
+namespace rq {
+
+size_t solveSharedBytes();
+// Persistent CTAs: each pulls job indices from *nextJob (zeroed by the caller)
+// until njobs are taken; ws is grid x wsStride doubles of per-CTA workspace.
+cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
+                        int grid, int block, cudaStream_t stream);
+// CTAs of `block` threads that fit on one SM at once.
+int solveBlocksPerSM(int block);
+
+} // namespace rq

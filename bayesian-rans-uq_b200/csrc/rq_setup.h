@@ -1,0 +1,77 @@
+// Host-side set-up of one mesh class for the device solver: the periodic
+// terrain-following mesh in structured (i, j) form, its wall distance, the
+// planar singular-omega balance, the fixed AMG hierarchy of the pressure
+// correction and the velocity-probe stencils. Everything here runs once per
+// mesh class; the per-draw work is on the GPU.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rq {
+
+// Structured periodic mesh. Cell c = j*nx + i. "x-face" c is the east face of
+// cell c (owner c, neighbour (i+1) mod nx, the last column's being the
+// periodic wrap face). "y-face" jf*nx + i lies below cell row jf: jf = 0 is the
+// bottom wall (owner row 0), jf = ny the top wall (owner row ny-1) and the rest
+// are internal with owner row jf-1 and neighbour row jf.
+struct StructMesh {
+    int nx = 0, ny = 0, n = 0;
+    double lx = 0;
+    std::vector<double> cx, cy, vol, wd;
+    std::vector<double> xa, xnx, xny, xw, xdl, xdx, xdy, xsh, xfx, xfy; // n
+    std::vector<double> ya, ynx, yny, yw, ydl, ydx, ydy, yfx, yfy;      // n + nx
+    // planar singular omega balance (empty unless the mesh qualifies)
+    bool balance = false;
+    std::vector<double> sing, slap, sgx, sgy; // sgx per x-face, sgy per y-face
+    int nfy() const { return n + nx; }
+};
+
+// Mesh generators (restating core/src/Mesh.cpp:490-741 and :431-463).
+StructMesh buildPeriodic(const std::vector<double> &xNodes, const std::vector<double> &yBottom,
+                         double yTop, int ny, double y1t);
+StructMesh makePeriodicChannel(int nx, int ny, double lx, double h, double reTau, double yPlus);
+StructMesh makeCurvedPeriodic(const std::vector<double> &xNodes,
+                              const std::vector<double> &yBottom, double yTop, int ny, double re,
+                              double yPlus);
+
+// Planar singular-omega qualification and arrays (rans-uq/src/SIMPLESolver.cpp:92-153).
+void preparePlanarBalance(StructMesh &m);
+
+// Fixed AMG hierarchy of the pressure-correction pattern. Level 0 is the
+// structured 5-point matrix (entry slot*n + cell, slots: 0 diag, 1 W, 2 E,
+// 3 S, 4 N); coarser levels are CSR. Aggregation is the reference's greedy
+// strength-0.25 rule (core/include/LinearSolver.hpp:535-575) applied to the
+// geometric Laplacian area/delta with the cell-0 pin; coarse values are
+// Galerkin sums (:578-618) gathered in fine CSR order.
+struct AmgHost {
+    struct Level {
+        int n = 0;
+        std::vector<int> ptr, col;            // CSR (levels >= 1)
+        std::vector<int> diagPos;             // CSR position of (i,i)
+        std::vector<int> agg;                 // row -> coarse row (all but the last level)
+        std::vector<int> childPtr, childIdx;  // coarse row -> fine rows, ascending
+        std::vector<int> gPtr, gSrc;          // coarse nnz -> fine entries summed into it
+    };
+    std::vector<Level> lev;
+    int coarseN() const { return lev.back().n; }
+    size_t coarseNnz() const { return lev.size() > 1 ? lev.back().col.size() : 0; }
+};
+AmgHost buildAmg(const StructMesh &m, int minCoarse = 50, int maxLevels = 20);
+
+// Velocity/pressure probe (PreparedObservation, core/include/ObservationOperator.hpp:630-670).
+struct ProbeHost {
+    int cell = -1;
+    double ox = 0, oy = 0, axx = 0, axy = 0, ayy = 0, det = 0;
+    int nnb = 0;
+    int nb[4] = {-1, -1, -1, -1}; // neighbour cell, or -1 for a wall face
+    double dx[4] = {0, 0, 0, 0}, dy[4] = {0, 0, 0, 0}, wt[4] = {0, 0, 0, 0};
+};
+ProbeHost prepareProbe(const StructMesh &m, double x, double y);
+
+// The faces of cell c in the reference's face-index order (creation order of
+// buildPeriodic2D): returned as codes 0 W, 1 E, 2 S, 3 N. Used where the
+// order of a sum or of a search must follow the reference.
+int cellFaceOrder(const StructMesh &m, int c, int out[4]);
+
+} // namespace rq

@@ -1,0 +1,1768 @@
+// The B200 forward model: one CTA runs one SIMPLE + k-omega SST solve, every
+// outer iteration of it, from cold start to its verdict, with all state in
+// HBM/L2 and the CTA's shared memory. Persistent CTAs pull draws from a job
+// queue (atomic counter), so a batch of mixed mesh classes keeps every SM busy
+// until the longest solve ends; a serving loop launches the same kernel per
+// admitted request on its own stream.
+//
+// The loop restates SIMPLESolver::solve (rans-uq/src/SIMPLESolver.cpp:1193-1716)
+// on the structured periodic layout of rq_setup.h. Every face sum is gathered
+// per cell in the reference's face order; dot products are block reductions
+// (warp shuffles, then a fixed-order sum of the warp partials that every
+// thread evaluates identically, so control flow stays uniform in the CTA).
+//
+// Inner solvers (core/include/LinearSolver.hpp): right-Jacobi BiCGSTAB
+// (:251-345) for momentum, k and omega; for the pressure correction PCG
+// (:184-246) with Jacobi or with the AMG V-cycle of this project (fixed
+// aggregation from rq_setup.cpp, damped-Jacobi smoothing, Galerkin values
+// refreshed per solve, dense coarsest inverse), or BiCGSTAB.
+#include "rq_device.cuh"
+#include "rq_kernels.h"
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace rq {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int kRedSlots = 8;             // values per block reduction
+constexpr double kJacobiW = 0.6;         // AMG smoother damping
+
+struct Work {
+    double *Ux, *Uy, *p, *k, *w, *nuT, *F1, *F2, *Pk, *CD, *S;
+    double *gUxx, *gUxy, *gUyx, *gUyy, *gKx, *gKy, *gWx, *gWy, *gPx, *gPy;
+    double *phi, *phiOld, *phiPred, *pCoeff; // x faces [0,n) then y faces [n, n+nfy)
+    double *d, *aW, *aE, *aS, *aN, *b, *aP, *aPraw;
+    double *Uxp, *Uyp, *kOld, *wOld, *pp;
+    double *r, *rh, *pv, *v, *s, *t, *ph, *sh;
+    double *z, *xa, *xb, *rr;                // PCG / level-0 V-cycle
+    double *amgVal, *amgVec, *dense0, *dense1;
+};
+
+struct Shared {
+    DevClass C;
+    Work W;
+    double coeff[11];
+    double red[2][kRedSlots][32];
+    double ring[4][kWindowCap];  // U, k, omega, Q change samples
+    int cnt[4];
+    double q[kMaxProbes], qPrev[kMaxProbes];
+    int haveQPrev;
+    int job;
+};
+
+// ---------------------------------------------------------------- reductions
+template <int K> struct Red {
+    double v[K];
+};
+
+template <int K>
+__device__ __forceinline__ void blockSum(double (&v)[K], Shared &S, int &rp) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1)
+            v[k] += __shfl_xor_sync(FULL, v[k], o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            S.red[rp][k][warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w)
+            s += S.red[rp][k][w];
+        v[k] = s;
+    }
+    rp ^= 1;
+}
+
+template <int K>
+__device__ __forceinline__ void blockMax(double (&v)[K], Shared &S, int &rp) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1)
+            v[k] = fmax(v[k], __shfl_xor_sync(FULL, v[k], o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            S.red[rp][k][warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = S.red[rp][k][0];
+        for (int w = 1; w < nw; ++w)
+            s = fmax(s, S.red[rp][k][w]);
+        v[k] = s;
+    }
+    rp ^= 1;
+}
+
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+
+// ---------------------------------------------------------------- geometry helpers
+struct Cell {
+    int c, i, j, W, E;
+    bool south, north; // internal south / north faces
+    bool xEfirst;      // east before west in face order (first column)
+    bool yNfirst;      // north before south (bottom row of a multi-row mesh)
+};
+
+__device__ __forceinline__ Cell cellOf(const DevClass &C, int c) {
+    Cell q;
+    q.c = c;
+    q.i = c % C.nx;
+    q.j = c / C.nx;
+    q.W = q.i == 0 ? c + C.nx - 1 : c - 1;
+    q.E = q.i == C.nx - 1 ? c - C.nx + 1 : c + 1;
+    q.south = q.j > 0;
+    q.north = q.j < C.ny - 1;
+    q.xEfirst = q.i == 0;
+    q.yNfirst = q.j == 0 && C.ny > 1;
+    return q;
+}
+
+// sum four face terms in the reference's face-index order
+__device__ __forceinline__ double order4(const Cell &q, double tW, double tE, double tS, double tN) {
+    const double x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+    const double y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
+    return ((x1 + x2) + y1) + y2;
+}
+// accumulate onto a running value in face order
+__device__ __forceinline__ double accum4(const Cell &q, double acc, double tW, double tE, double tS,
+                                         double tN) {
+    const double x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+    const double y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
+    return (((acc + x1) + x2) + y1) + y2;
+}
+
+// the wall face of a wall cell; a cell touching both walls keeps the last (top) one
+__device__ __forceinline__ int wallFaceOf(const DevClass &C, int c) {
+    const int j = c / C.nx;
+    return (j == C.ny - 1 ? C.ny : 0) * C.nx + c % C.nx;
+}
+__device__ __forceinline__ bool isWallCell(const DevClass &C, int c) {
+    const int j = c / C.nx;
+    return j == 0 || j == C.ny - 1;
+}
+
+__device__ __forceinline__ double wallOmega(const DevClass &C, double b1, double y) {
+    const double coefficient = C.balance ? 6.0 : 60.0; // resolvedWallOmega, SIMPLESolver.cpp:155-161
+    return coefficient * C.nu / (b1 * y * y);
+}
+// wall face value of omega (applyOmegaBC, BoundaryCondition.hpp:361-384)
+__device__ __forceinline__ double wallFaceOmega(const DevClass &C, double b1, int f) {
+    const double y1 = dmax(C.ydl[f], 1e-20);
+    return 60.0 * C.nu / (b1 * y1 * y1);
+}
+
+// Green-Gauss gradient of one cell (Field.hpp:178-212); bS / bN are the wall
+// face values used where the cell touches the bottom / top wall.
+__device__ __forceinline__ void ggCell(const DevClass &C, const Cell &q, const double *phi,
+                                       double bS, double bN, double &gx, double &gy) {
+    const int c = q.c;
+    const double pc = phi[c];
+    // east (owner c)
+    const double wE = C.xw[c];
+    const double fE = pc * wE + phi[q.E] * (1.0 - wE);
+    const double sxE = C.xnx[c] * C.xa[c], syE = C.xny[c] * C.xa[c];
+    // west (owner W, neighbour c)
+    const double wWf = C.xw[q.W];
+    const double fW = phi[q.W] * wWf + pc * (1.0 - wWf);
+    const double sxW = C.xnx[q.W] * C.xa[q.W], syW = C.xny[q.W] * C.xa[q.W];
+    // north: internal (owner c) or top wall (owner c)
+    const int fn = c + C.nx;
+    double fN;
+    if (q.north) {
+        const double w = C.yw[fn];
+        fN = pc * w + phi[c + C.nx] * (1.0 - w);
+    } else {
+        fN = bN;
+    }
+    const double sxN = C.ynx[fn] * C.ya[fn], syN = C.yny[fn] * C.ya[fn];
+    // south: internal (owner c - nx, neighbour c) or bottom wall (owner c)
+    const int fs = c;
+    double fS;
+    if (q.south) {
+        const double w = C.yw[fs];
+        fS = phi[c - C.nx] * w + pc * (1.0 - w);
+    } else {
+        fS = bS;
+    }
+    const double sxS = C.ynx[fs] * C.ya[fs], syS = C.yny[fs] * C.ya[fs];
+    const double sgnS = q.south ? -1.0 : 1.0;
+    gx = order4(q, -(sxW * fW), sxE * fE, sgnS * (sxS * fS), sxN * fN);
+    gy = order4(q, -(syW * fW), syE * fE, sgnS * (syS * fS), syN * fN);
+    const double V = C.vol[c];
+    if (V > 1e-30) {
+        gx = gx / V;
+        gy = gy / V;
+    }
+}
+
+// matrix row times x in the reference's matvec order (diagonal first, then faces)
+__device__ __forceinline__ double rowDot(const Cell &q, const double *d, const double *aW,
+                                         const double *aE, const double *aS, const double *aN,
+                                         const double *x, int nx) {
+    const int c = q.c;
+    const double tW = aW[c] * x[q.W], tE = aE[c] * x[q.E];
+    const double tS = q.south ? aS[c] * x[c - nx] : 0.0;
+    const double tN = q.north ? aN[c] * x[c + nx] : 0.0;
+    return accum4(q, d[c] * x[c], tW, tE, tS, tN);
+}
+
+__device__ __forceinline__ double jac(double r, double d) {
+    return (fabs(d) > 1e-30) ? r / d : r; // jacobiPrecond, LinearSolver.hpp:173-177
+}
+
+struct LinRes {
+    int iterations;
+    double finalRes, initialRes;
+    bool converged;
+};
+
+#define FOR_CELLS(c) for (int c = threadIdx.x; c < n; c += blockDim.x)
+
+// Right-Jacobi BiCGSTAB (LinearSolver.hpp:251-345). r holds b - A x0 on entry
+// and r0n its norm (both computed by the caller's assembly phase).
+__device__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW,
+                           const double *aE, const double *aS, const double *aN, double *x,
+                           double r0n, int maxIter, double tol) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const int n = C.n, nx = C.nx;
+    LinRes res{0, 0.0, r0n, false};
+    if (r0n < 1e-30) {
+        res.converged = true;
+        return res;
+    }
+    double *r = W.r, *rh = W.rh, *p = W.pv, *v = W.v, *s = W.s, *t = W.t, *ph = W.ph, *sh = W.sh;
+    FOR_CELLS(c) {
+        rh[c] = r[c];
+        p[c] = 0.0;
+        v[c] = 0.0;
+    }
+    double rho = 1, alpha = 1, omega = 1;
+    // rhoN of the first iteration
+    double acc[1] = {0.0};
+    FOR_CELLS(c) acc[0] += r[c] * r[c];
+    blockSum<1>(acc, S, rp);
+    double rhoN = acc[0];
+    for (int it = 0; it < maxIter; ++it) {
+        if (fabs(rhoN) < 1e-30)
+            break;
+        const double beta = (rhoN / (rho + 1e-30)) * (alpha / (omega + 1e-30));
+        FOR_CELLS(c) {
+            p[c] = r[c] + beta * (p[c] - omega * v[c]);
+            ph[c] = jac(p[c], d[c]);
+        }
+        __syncthreads();
+        double a1[1] = {0.0};
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            const double vc = rowDot(q, d, aW, aE, aS, aN, ph, nx);
+            v[c] = vc;
+            a1[0] += rh[c] * vc;
+        }
+        blockSum<1>(a1, S, rp);
+        const double rv = a1[0];
+        if (fabs(rv) < 1e-30)
+            break;
+        alpha = rhoN / rv;
+        double a2[1] = {0.0};
+        FOR_CELLS(c) {
+            const double sc = r[c] - alpha * v[c];
+            s[c] = sc;
+            sh[c] = jac(sc, d[c]);
+            a2[0] += sc * sc;
+        }
+        blockSum<1>(a2, S, rp);
+        const double sn = sqrt(a2[0]);
+        if (sn / r0n < tol) {
+            FOR_CELLS(c) x[c] += alpha * ph[c];
+            __syncthreads();
+            res.iterations = it + 1;
+            res.finalRes = sn / r0n;
+            res.converged = true;
+            return res;
+        }
+        double a3[2] = {0.0, 0.0};
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            const double tc = rowDot(q, d, aW, aE, aS, aN, sh, nx);
+            t[c] = tc;
+            a3[0] += tc * tc;
+            a3[1] += tc * s[c];
+        }
+        blockSum<2>(a3, S, rp);
+        const double tt = a3[0];
+        omega = (tt > 1e-30) ? a3[1] / tt : 0.0;
+        double a4[2] = {0.0, 0.0};
+        FOR_CELLS(c) {
+            x[c] += alpha * ph[c] + omega * sh[c];
+            const double rc = s[c] - omega * t[c];
+            r[c] = rc;
+            a4[0] += rc * rc;
+            a4[1] += rh[c] * rc;
+        }
+        blockSum<2>(a4, S, rp);
+        const double rn = sqrt(a4[0]);
+        res.iterations = it + 1;
+        res.finalRes = rn / r0n;
+        if (res.finalRes < tol) {
+            res.converged = true;
+            return res;
+        }
+        if (fabs(omega) < 1e-30)
+            break;
+        rho = rhoN;
+        rhoN = a4[1];
+    }
+    return res;
+}
+
+// ---------------------------------------------------------------- AMG V-cycle
+__device__ __forceinline__ double level0Entry(const Work &W, int n, int e) {
+    const int slot = e / n, c = e - slot * n;
+    const double *a = slot == 0 ? W.d : slot == 1 ? W.aW : slot == 2 ? W.aE : slot == 3 ? W.aS : W.aN;
+    return a[c];
+}
+
+// Galerkin values of every coarse level from the current pressure system,
+// then the dense inverse of the coarsest level by Gauss-Jordan elimination
+// (ping-pong buffers, one barrier per pivot).
+__device__ void amgRefresh(Shared &S) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const int L = C.nlev;
+    for (int l = 0; l + 1 < L; ++l) {
+        const DevAmgLevel &F = C.lev[l];
+        const DevAmgLevel &Q = C.lev[l + 1];
+        double *cv = W.amgVal + Q.valOff;
+        const double *fv = W.amgVal + F.valOff;
+        for (int e = threadIdx.x; e < Q.nnz; e += blockDim.x) {
+            double s = 0.0;
+            for (int k = F.gPtr[e]; k < F.gPtr[e + 1]; ++k)
+                s += (l == 0) ? level0Entry(W, C.n, F.gSrc[k]) : fv[F.gSrc[k]];
+            cv[e] = s;
+        }
+        __syncthreads();
+    }
+    const DevAmgLevel &Q = C.lev[L - 1];
+    const int m = Q.n, m2 = 2 * m;
+    const double *qv = W.amgVal + Q.valOff;
+    double *A0 = W.dense0, *A1 = W.dense1;
+    for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
+        A0[e] = ((e % m2) == m + e / m2) ? 1.0 : 0.0;
+    __syncthreads();
+    if (L == 1) { // the whole (small) pressure system is the coarsest level
+        for (int r = threadIdx.x; r < m; r += blockDim.x) {
+            const Cell q = cellOf(C, r);
+            A0[r * m2 + r] += W.d[r];
+            A0[r * m2 + q.W] += W.aW[r];
+            A0[r * m2 + q.E] += W.aE[r];
+            if (q.south)
+                A0[r * m2 + r - C.nx] += W.aS[r];
+            if (q.north)
+                A0[r * m2 + r + C.nx] += W.aN[r];
+        }
+    } else {
+        for (int r = threadIdx.x; r < m; r += blockDim.x)
+            for (int k = Q.ptr[r]; k < Q.ptr[r + 1]; ++k)
+                A0[r * m2 + Q.col[k]] = qv[k];
+    }
+    __syncthreads();
+    for (int piv = 0; piv < m; ++piv) {
+        const double inv = 1.0 / A0[piv * m2 + piv];
+        for (int e = threadIdx.x; e < m * m2; e += blockDim.x) {
+            const int r = e / m2, col = e - r * m2;
+            const double pr = A0[piv * m2 + col] * inv;
+            A1[e] = (r == piv) ? pr : A0[e] - A0[r * m2 + piv] * pr;
+        }
+        __syncthreads();
+        double *tmp = A0;
+        A0 = A1;
+        A1 = tmp;
+    }
+    if (A0 != W.dense0) { // keep the inverse in dense0
+        for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
+            W.dense0[e] = A0[e];
+        __syncthreads();
+    }
+}
+
+// CSR row of level l >= 1 times x
+__device__ __forceinline__ double csrRow(const DevAmgLevel &L, const double *val, const double *x,
+                                         int i) {
+    double s = 0.0;
+    for (int k = L.ptr[i]; k < L.ptr[i + 1]; ++k)
+        s += val[k] * x[L.col[k]];
+    return s;
+}
+
+// z = M^-1 b at level 0 (b = W.r). Returns (r, z) reduced in the last phase.
+__device__ double vcycle(Shared &S, int &rp) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const int L = C.nlev, n0 = C.n, nx = C.nx;
+    const double om = kJacobiW;
+    // vectors of coarse level l: b, xa, xb, r at amgVec + vecOff + {0,1,2,3}*n
+    auto vb = [&](int l) { return W.amgVec + C.lev[l].vecOff; };
+    // ---- down
+    for (int l = 0; l + 1 < L; ++l) {
+        const DevAmgLevel &Lv = C.lev[l];
+        const int n = Lv.n;
+        double *b, *xa, *xb, *rr;
+        if (l == 0) {
+            b = W.r;
+            xa = W.xa;
+            xb = W.xb;
+            rr = W.rr;
+        } else {
+            b = vb(l);
+            xa = b + n;
+            xb = b + 2 * n;
+            rr = b + 3 * n;
+        }
+        const double *val = W.amgVal + Lv.valOff;
+        // P1: restriction (l >= 1) and the first sweep from zero
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double bi;
+            if (l == 0) {
+                bi = b[i];
+            } else {
+                const DevAmgLevel &F = C.lev[l - 1];
+                const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
+                bi = 0.0;
+                for (int k = F.childPtr[i]; k < F.childPtr[i + 1]; ++k)
+                    bi += fr[F.childIdx[k]];
+                b[i] = bi;
+            }
+            const double di = (l == 0) ? W.d[i] : val[Lv.diagPos[i]];
+            xa[i] = om * bi / di;
+        }
+        __syncthreads();
+        // P2: second sweep
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double ax, di;
+            if (l == 0) {
+                const Cell q = cellOf(C, i);
+                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
+                di = W.d[i];
+            } else {
+                ax = csrRow(Lv, val, xa, i);
+                di = val[Lv.diagPos[i]];
+            }
+            xb[i] = xa[i] + om * (b[i] - ax) / di;
+        }
+        __syncthreads();
+        // P3: residual
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double ax;
+            if (l == 0) {
+                const Cell q = cellOf(C, i);
+                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xb, nx);
+            } else {
+                ax = csrRow(Lv, val, xb, i);
+            }
+            rr[i] = b[i] - ax;
+        }
+        __syncthreads();
+    }
+    // ---- coarsest: restriction, dense solve into xb
+    {
+        const int l = L - 1;
+        const DevAmgLevel &Lv = C.lev[l];
+        const int m = Lv.n, m2 = 2 * m;
+        double *b = vb(l), *xb = b + 2 * m;
+        if (L == 1) { // a single level: direct solve of the whole system
+            for (int i = threadIdx.x; i < m; i += blockDim.x)
+                b[i] = W.r[i];
+        } else {
+            const DevAmgLevel &F = C.lev[l - 1];
+            const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
+            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+                double bi = 0.0;
+                for (int k = F.childPtr[i]; k < F.childPtr[i + 1]; ++k)
+                    bi += fr[F.childIdx[k]];
+                b[i] = bi;
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            double s = 0.0;
+            const double *row = W.dense0 + i * m2 + m;
+            for (int j = 0; j < m; ++j)
+                s += row[j] * b[j];
+            xb[i] = s;
+        }
+        __syncthreads();
+    }
+    // ---- up: prolongation fused into the first post sweep
+    double rz = 0.0;
+    for (int l = L - 2; l >= 0; --l) {
+        const DevAmgLevel &Lv = C.lev[l];
+        const int n = Lv.n;
+        const double *xc = vb(l + 1) + 2 * C.lev[l + 1].n; // coarse xb
+        double *b, *xa, *xb;
+        if (l == 0) {
+            b = W.r;
+            xa = W.xa;
+            xb = W.z;
+        } else {
+            b = vb(l);
+            xa = b + n;
+            xb = b + 2 * n;
+        }
+        const double *xprev = (l == 0) ? W.xb : xb; // down-pass result
+        const double *val = W.amgVal + Lv.valOff;
+        const int *agg = Lv.agg;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const double xi = xprev[i] + xc[agg[i]];
+            double ax, di;
+            if (l == 0) {
+                const Cell q = cellOf(C, i);
+                const int c = i;
+                auto X = [&](int jj) { return xprev[jj] + xc[agg[jj]]; };
+                const double tW = W.aW[c] * X(q.W), tE = W.aE[c] * X(q.E);
+                const double tS = q.south ? W.aS[c] * X(c - nx) : 0.0;
+                const double tN = q.north ? W.aN[c] * X(c + nx) : 0.0;
+                ax = accum4(q, W.d[c] * xi, tW, tE, tS, tN);
+                di = W.d[c];
+            } else {
+                ax = 0.0;
+                for (int k = Lv.ptr[i]; k < Lv.ptr[i + 1]; ++k) {
+                    const int jj = Lv.col[k];
+                    ax += val[k] * (xprev[jj] + xc[agg[jj]]);
+                }
+                di = val[Lv.diagPos[i]];
+            }
+            xa[i] = xi + om * (b[i] - ax) / di;
+        }
+        __syncthreads();
+        double part = 0.0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            double ax, di;
+            if (l == 0) {
+                const Cell q = cellOf(C, i);
+                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
+                di = W.d[i];
+            } else {
+                ax = csrRow(Lv, val, xa, i);
+                di = val[Lv.diagPos[i]];
+            }
+            const double zi = xa[i] + om * (b[i] - ax) / di;
+            xb[i] = zi;
+            if (l == 0)
+                part += b[i] * zi;
+        }
+        if (l == 0) {
+            double a[1] = {part};
+            blockSum<1>(a, S, rp);
+            rz = a[0];
+        } else {
+            __syncthreads();
+        }
+    }
+    if (L == 1) { // the coarsest solve is the whole preconditioner
+        const double *xb = vb(0) + 2 * C.lev[0].n;
+        double part = 0.0;
+        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+            W.z[i] = xb[i];
+            part += W.r[i] * xb[i];
+        }
+        double a[1] = {part};
+        blockSum<1>(a, S, rp);
+        rz = a[0];
+    }
+    return rz;
+}
+
+// PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0; r holds b and r0n its norm.
+__device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, double tol,
+                      bool amg) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const int n = C.n, nx = C.nx;
+    LinRes res{0, 0.0, r0n, false};
+    if (r0n < 1e-30) {
+        res.converged = true;
+        return res;
+    }
+    if (amg)
+        amgRefresh(S);
+    double *r = W.r, *z = W.z, *p = W.pv, *Ap = W.v;
+    double rz;
+    if (amg) {
+        rz = vcycle(S, rp);
+    } else {
+        double a[1] = {0.0};
+        FOR_CELLS(c) {
+            z[c] = jac(r[c], W.d[c]);
+            a[0] += r[c] * z[c];
+        }
+        blockSum<1>(a, S, rp);
+        rz = a[0];
+    }
+    FOR_CELLS(c) p[c] = z[c];
+    __syncthreads();
+    for (int it = 0; it < maxIter; ++it) {
+        double a1[1] = {0.0};
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            const double v = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, p, nx);
+            Ap[c] = v;
+            a1[0] += p[c] * v;
+        }
+        blockSum<1>(a1, S, rp);
+        const double pAp = a1[0];
+        if (fabs(pAp) < 1e-30)
+            break;
+        const double alpha = rz / pAp;
+        double a2[1] = {0.0};
+        FOR_CELLS(c) {
+            x[c] += alpha * p[c];
+            const double rc = r[c] - alpha * Ap[c];
+            r[c] = rc;
+            a2[0] += rc * rc;
+        }
+        blockSum<1>(a2, S, rp);
+        const double rn = sqrt(a2[0]);
+        res.iterations = it + 1;
+        res.finalRes = rn / r0n;
+        if (res.finalRes < tol) {
+            res.converged = true;
+            return res;
+        }
+        double rzNew;
+        if (amg) {
+            rzNew = vcycle(S, rp);
+        } else {
+            double a3[1] = {0.0};
+            FOR_CELLS(c) {
+                z[c] = jac(r[c], W.d[c]);
+                a3[0] += r[c] * z[c];
+            }
+            blockSum<1>(a3, S, rp);
+            rzNew = a3[0];
+        }
+        const double beta = rzNew / (rz + 1e-30);
+        FOR_CELLS(c) p[c] = z[c] + beta * p[c];
+        __syncthreads();
+        rz = rzNew;
+    }
+    return res;
+}
+
+// ---------------------------------------------------------------- contraction estimate
+// ContractionEstimate (SIMPLESolver.cpp:32-74) over a shared ring of samples;
+// every warp evaluates the window maxima with shuffles (max is exact).
+struct Est {
+    double rate, remaining;
+};
+__device__ Est estimate(const Shared &S, int e, int window, double negligible) {
+    const int m = window < 2 ? 2 : window;
+    const int cnt = S.cnt[e];
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    if (cnt < 2 * m)
+        return {__longlong_as_double(0x7ff8000000000000LL), inf};
+    const int lane = threadIdx.x & 31;
+    double dNew = 0.0, dOld = 0.0;
+    for (int l = lane; l < m; l += 32) {
+        dNew = dmax(dNew, S.ring[e][(cnt - m + l) % kWindowCap]);
+        dOld = dmax(dOld, S.ring[e][(cnt - 2 * m + l) % kWindowCap]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dNew = dmax(dNew, __shfl_xor_sync(FULL, dNew, o));
+        dOld = dmax(dOld, __shfl_xor_sync(FULL, dOld, o));
+    }
+    double rate;
+    if (dOld <= 0.0)
+        rate = dNew > 0.0 ? inf : 0.0;
+    else
+        rate = pow(dNew / dOld, 1.0 / m);
+    double remaining;
+    if (dNew <= negligible)
+        remaining = dNew;
+    else if (!(rate < 1.0))
+        remaining = inf;
+    else
+        remaining = dNew * rate / (1.0 - rate);
+    return {rate, remaining};
+}
+
+__device__ __forceinline__ void pushSample(Shared &S, int e, double v) {
+    __syncthreads(); // everyone finished reading the ring
+    if (threadIdx.x == 0) {
+        S.ring[e][S.cnt[e] % kWindowCap] = v;
+        S.cnt[e] += 1;
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------- the solve
+__device__ void carve(Shared &S, double *ws) {
+    const DevClass &C = S.C;
+    const int n = C.n, nf = C.n + C.nfy;
+    Work &W = S.W;
+    double *p = ws;
+    auto take = [&](long cnt) {
+        double *r = p;
+        p += (cnt + 31) / 32 * 32;
+        return r;
+    };
+    W.Ux = take(n);
+    W.Uy = take(n);
+    W.p = take(n);
+    W.k = take(n);
+    W.w = take(n);
+    W.nuT = take(n);
+    W.F1 = take(n);
+    W.F2 = take(n);
+    W.Pk = take(n);
+    W.CD = take(n);
+    W.S = take(n);
+    W.gUxx = take(n);
+    W.gUxy = take(n);
+    W.gUyx = take(n);
+    W.gUyy = take(n);
+    W.gKx = take(n);
+    W.gKy = take(n);
+    W.gWx = take(n);
+    W.gWy = take(n);
+    W.gPx = take(n);
+    W.gPy = take(n);
+    W.phi = take(nf);
+    W.phiOld = take(nf);
+    W.phiPred = take(nf);
+    W.pCoeff = take(nf);
+    W.d = take(n);
+    W.aW = take(n);
+    W.aE = take(n);
+    W.aS = take(n);
+    W.aN = take(n);
+    W.b = take(n);
+    W.aP = take(n);
+    W.aPraw = take(n);
+    W.Uxp = take(n);
+    W.Uyp = take(n);
+    W.kOld = take(n);
+    W.wOld = take(n);
+    W.pp = take(n);
+    W.r = take(n);
+    W.rh = take(n);
+    W.pv = take(n);
+    W.v = take(n);
+    W.s = take(n);
+    W.t = take(n);
+    W.ph = take(n);
+    W.sh = take(n);
+    W.z = take(n);
+    W.xa = take(n);
+    W.xb = take(n);
+    W.rr = take(n);
+    W.amgVal = take(C.amgVals);
+    W.amgVec = take(C.amgVecs);
+    const int m = C.lev[C.nlev - 1].n;
+    W.dense0 = take(2L * m * m);
+    W.dense1 = take(2L * m * m);
+}
+
+__device__ void runSolve(Shared &S, const DevJob &job) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const DevSettings &st = C.st;
+    const int n = C.n, nx = C.nx, ny = C.ny, nfy = C.nfy;
+    const double nu = C.nu;
+    int rp = 0;
+    // coefficients (InferenceParameterSet order) and their blends (SSTModel.hpp:12-61)
+    const double sk1 = S.coeff[0], sw1 = S.coeff[1], b1 = S.coeff[2], al1 = S.coeff[3];
+    const double sk2 = S.coeff[4], sw2 = S.coeff[5], b2 = S.coeff[6], al2 = S.coeff[7];
+    const double bs = S.coeff[8], a1 = S.coeff[9];
+    auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+
+    // ---- initUniform (SIMPLESolver.cpp:267-298) and applyAllBCs
+    const double U0 = C.init[0], U1 = C.init[1], P0 = C.init[3], K0 = C.init[4], W0 = C.init[5];
+    FOR_CELLS(c) {
+        W.Ux[c] = U0;
+        W.Uy[c] = U1;
+        W.p[c] = P0;
+        W.k[c] = K0;
+        const double om = dmax(wallOmega(C, b1, dmax(C.wd[c], 1e-20)), W0);
+        W.w[c] = om;
+        W.F1[c] = 1.0;
+        W.F2[c] = 1.0;
+        W.Pk[c] = 0.0;
+        W.CD[c] = 0.0;
+        W.nuT[c] = a1 * K0 / dmax(a1 * om, 1e-20);
+        W.S[c] = 0.0;
+    }
+    if (threadIdx.x < 4)
+        S.cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0)
+        S.haveQPrev = 0;
+    __syncthreads();
+    // phi = interpolated fluxes of the initial state (wall faces carry U_b = 0)
+    for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+        double v = 0.0;
+        if (f < n) {
+            const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+            const double w = C.xw[f];
+            const double ux = W.Ux[f] * w + W.Ux[q] * (1.0 - w), uy = W.Uy[f] * w + W.Uy[q] * (1.0 - w);
+            v = (ux * C.xnx[f] + uy * C.xny[f]) * C.xa[f];
+        } else {
+            const int g = f - n, jf = g / nx;
+            if (jf > 0 && jf < ny) {
+                const int o = g - nx;
+                const double w = C.yw[g];
+                const double ux = W.Ux[o] * w + W.Ux[g] * (1.0 - w), uy = W.Uy[o] * w + W.Uy[g] * (1.0 - w);
+                v = (ux * C.ynx[g] + uy * C.yny[g]) * C.ya[g];
+            } else {
+                v = (0.0 * C.ynx[g] + 0.0 * C.yny[g]) * C.ya[g];
+            }
+        }
+        W.phi[f] = v;
+    }
+    __syncthreads();
+
+    bool established = false;
+    bool wallBetaInit = true; // the face omega still carries applyAllBCs' beta1
+    double lastK = 1.0, lastW = 1.0;
+    const double tol = st.tol, negligible = 0.01 * tol;
+    double worst = inf, fluxRef = 0.0, n0x = 1, n0y = 1, n0p = 1;
+    int status = 1, finalIter = st.maxIter;
+    bool converged = false, diverged = false;
+    double rateU = __longlong_as_double(0x7ff8000000000000LL);
+
+    auto bwOf = [&](int f) { return wallFaceOmega(C, wallBetaInit ? C.beta1Init : b1, f); };
+
+    for (int iter = 0; iter < st.maxIter; ++iter) {
+        const bool turbActive = iter >= st.turbStart;
+        const bool turbUpdate = turbActive && ((iter - st.turbStart) % st.turbInterval == 0);
+        // ---- phase: save U, interpolated old flux, gradients of U and p
+        for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+            double v = 0.0;
+            if (f < n) {
+                const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                const double w = C.xw[f];
+                const double ux = W.Ux[f] * w + W.Ux[q] * (1.0 - w), uy = W.Uy[f] * w + W.Uy[q] * (1.0 - w);
+                v = (ux * C.xnx[f] + uy * C.xny[f]) * C.xa[f];
+            } else {
+                const int g = f - n, jf = g / nx;
+                if (jf > 0 && jf < ny) {
+                    const int o = g - nx;
+                    const double w = C.yw[g];
+                    const double ux = W.Ux[o] * w + W.Ux[g] * (1.0 - w), uy = W.Uy[o] * w + W.Uy[g] * (1.0 - w);
+                    v = (ux * C.ynx[g] + uy * C.yny[g]) * C.ya[g];
+                } else {
+                    v = (0.0 * C.ynx[g] + 0.0 * C.yny[g]) * C.ya[g];
+                }
+            }
+            W.phiOld[f] = v;
+        }
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            W.Uxp[c] = W.Ux[c];
+            W.Uyp[c] = W.Uy[c];
+            double gx, gy;
+            ggCell(C, q, W.Ux, 0.0, 0.0, gx, gy);
+            W.gUxx[c] = gx;
+            W.gUxy[c] = gy;
+            ggCell(C, q, W.Uy, 0.0, 0.0, gx, gy);
+            W.gUyx[c] = gx;
+            W.gUyy[c] = gy;
+            // pressure faces carry the owner value (Neumann walls)
+            ggCell(C, q, W.p, W.p[c], W.p[c], gx, gy);
+            W.gPx[c] = gx;
+            W.gPy[c] = gy;
+            if (turbUpdate) {
+                ggCell(C, q, W.k, 0.0, 0.0, gx, gy);
+                W.gKx[c] = gx;
+                W.gKy[c] = gy;
+                ggCell(C, q, W.w, bwOf(q.i), bwOf(C.ny * nx + q.i), gx, gy);
+                W.gWx[c] = gx;
+                W.gWy[c] = gy;
+            }
+        }
+        __syncthreads();
+
+        // ---- SST closure (SSTModel.cpp:157-241) and the startup nuT floor (:1322-1337)
+        if (turbUpdate) {
+            if (!established && iter >= st.turbStart + st.floorIters)
+                established = true;
+            const double floorV = established ? 0.0 : 0.1 * nu;
+            FOR_CELLS(c) {
+                const double s11 = W.gUxx[c], s22 = W.gUyy[c];
+                const double s12 = 0.5 * (W.gUxy[c] + W.gUyx[c]);
+                const double Sc = sqrt(2.0 * (s11 * s11 + s22 * s22 + 0.0 + 2.0 * (s12 * s12 + 0.0 + 0.0)));
+                W.S[c] = Sc;
+                const double kc = dmax(W.k[c], 0.0), wc = dmax(W.w[c], 1e-20);
+                const double y = dmax(C.wd[c], 1e-20);
+                const double cd = 2.0 * sw2 / dmax(wc, 1e-20) * (W.gKx[c] * W.gWx[c] + W.gKy[c] * W.gWy[c]);
+                W.CD[c] = cd;
+                const double sqk = sqrt(dmax(kc, 0.0)), ws = dmax(wc, 1e-20);
+                const double ys = dmax(y, 1e-20), y2 = ys * ys;
+                const double t1 = sqk / (bs * ws * ys);
+                const double t2 = 500.0 * nu / (y2 * ws);
+                const double t3 = 4.0 * sw2 * dmax(kc, 0.0) / (dmax(cd, 1e-10) * y2);
+                const double arg1 = dmin(dmax(t1, t2), t3);
+                const double F1 = tanh(arg1 * arg1 * arg1 * arg1);
+                W.F1[c] = F1;
+                const double u1 = 2.0 * sqk / (bs * ws * ys);
+                const double arg2 = dmax(u1, t2);
+                const double F2 = tanh(arg2 * arg2);
+                W.F2[c] = F2;
+                double den = dmax(a1 * wc, Sc * F2);
+                den = dmax(den, 1e-20);
+                const double nut = a1 * dmax(kc, 0.0) / den;
+                const double raw = nut * Sc * Sc;
+                const double lim = 10.0 * bs * dmax(kc, 0.0) * dmax(wc, 1e-20);
+                W.Pk[c] = dmin(raw, lim);
+                W.nuT[c] = dmax(nut, floorV);
+            }
+            __syncthreads();
+        }
+
+        // ---- momentum x then y (assembleMomentum :303-482)
+        LinRes resU[2];
+        double momRes = 0.0, momScale = 0.0;
+        for (int comp = 0; comp < 2; ++comp) {
+            if (comp == 1) { // gradients of the updated Ux for the y assembly
+                FOR_CELLS(c) {
+                    const Cell q = cellOf(C, c);
+                    double gx, gy;
+                    ggCell(C, q, W.Ux, 0.0, 0.0, gx, gy);
+                    W.gUxx[c] = gx;
+                    W.gUxy[c] = gy;
+                    ggCell(C, q, W.Uy, 0.0, 0.0, gx, gy);
+                    W.gUyx[c] = gx;
+                    W.gUyy[c] = gy;
+                }
+                __syncthreads();
+            }
+            double *U = comp == 0 ? W.Ux : W.Uy;
+            const double *gUc_x = comp == 0 ? W.gUxx : W.gUyx; // grad of this component
+            const double *gUc_y = comp == 0 ? W.gUxy : W.gUyy;
+            const double *colX = comp == 0 ? W.gUxx : W.gUxy;  // dUx/dx_comp
+            const double *colY = comp == 0 ? W.gUyx : W.gUyy;  // dUy/dx_comp
+            const double fb = comp == 0 ? st.fx : st.fy;
+            double acc[3] = {0.0, 0.0, 0.0};
+            FOR_CELLS(c) {
+                const Cell q = cellOf(C, c);
+                const int i = q.i, j = q.j;
+                // faces: 0 W 1 E 2 S 3 N. owner flags, neighbour cells, face arrays
+                double dT[4], aT[4], tsT[4], ccT[4];
+                const bool isWall[4] = {false, false, !q.south, !q.north};
+                const int nb[4] = {q.W, q.E, c - nx, c + nx};
+                for (int k = 0; k < 4; ++k) {
+                    dT[k] = 0.0;
+                    aT[k] = 0.0;
+                    tsT[k] = 0.0;
+                    ccT[k] = 0.0;
+                }
+                for (int k = 0; k < 4; ++k) {
+                    bool own;
+                    int f, o, qn;
+                    const double *A, *NX, *NY, *WT, *DL;
+                    double sh = 0.0;
+                    int fi;
+                    if (k < 2) {
+                        fi = (k == 0) ? q.W : c;
+                        own = (k == 1);
+                        o = fi;
+                        qn = (k == 0) ? c : q.E;
+                        A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl;
+                        sh = C.xsh[fi];
+                        f = fi;
+                    } else {
+                        fi = (k == 2) ? c : c + nx;
+                        own = (k == 3) || isWall[k];
+                        o = (k == 2) ? c - nx : c;
+                        qn = (k == 2) ? c : c + nx;
+                        A = C.ya; NX = C.ynx; NY = C.yny; WT = C.yw; DL = C.ydl;
+                        f = n + fi;
+                    }
+                    const double delta = dmax(DL[fi], 1e-20);
+                    const double F = W.phi[f];
+                    if (isWall[k]) { // resolved wall: molecular viscosity, U_b = 0
+                        const double Db = nu * A[fi] / delta;
+                        const double Ub = 0.0;
+                        if (F >= 0) {
+                            dT[k] = F + Db;
+                            tsT[k] = Db * Ub; // boundary source
+                        } else {
+                            dT[k] = Db;
+                            tsT[k] = (Db - F) * Ub;
+                        }
+                        continue;
+                    }
+                    const double w = WT[fi];
+                    const double nuO = nu + W.nuT[o], nuN = nu + W.nuT[qn];
+                    const double nuF = w * nuO + (1.0 - w) * nuN;
+                    const double D = nuF * A[fi] / delta;
+                    const double cp = dmax(F, 0.0), cn = dmax(-F, 0.0);
+                    dT[k] = own ? D + cp : D + cn;
+                    aT[k] = own ? -(D + cn) : -(D + cp);
+                    // transpose stress flux through this face (StressOperators.hpp:31-81)
+                    const double cf = w * W.nuT[o] + (1.0 - w) * W.nuT[qn];
+                    const double gxf = colX[o] * w + colX[qn] * (1.0 - w);
+                    const double gyf = colY[o] * w + colY[qn] * (1.0 - w);
+                    const double fl = cf * (gxf * NX[fi] + gyf * NY[fi]) * A[fi];
+                    tsT[k] = own ? fl : -fl;
+                    // limitedLinearUpwind deferred correction (:495-532)
+                    if (F != 0.0) {
+                        const bool ownerUp = F > 0.0;
+                        const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
+                        const double xUx = C.cx[up], xUy = C.cy[up];
+                        const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
+                        const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
+                        const double dphi = U[dn] - U[up];
+                        double psi = 0.0;
+                        if (fabs(dphi) > 1e-300) {
+                            const double rr = 2.0 * (gUc_x[up] * (xDx - xUx) + gUc_y[up] * (xDy - xUy)) / dphi - 1.0;
+                            psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
+                        }
+                        const double pf = U[up] + 0.5 * psi * dphi;
+                        const double corr = F * (pf - U[up]);
+                        ccT[k] = own ? -corr : corr;
+                    }
+                }
+                (void)i;
+                (void)j;
+                // internal faces first in face order, then the wall (boundary faces come last)
+                double dsum = 0.0, bsrc = 0.0, ts = 0.0, bcc;
+                {
+                    const double x1 = q.xEfirst ? dT[1] : dT[0], x2 = q.xEfirst ? dT[0] : dT[1];
+                    dsum = dsum + x1;
+                    dsum = dsum + x2;
+                    const int y1 = q.yNfirst ? 3 : 2, y2 = q.yNfirst ? 2 : 3;
+                    // walls come after internal faces: j == 0 puts S (wall) last via yNfirst
+                    if (!isWall[y1])
+                        dsum = dsum + dT[y1];
+                    if (!isWall[y2])
+                        dsum = dsum + dT[y2];
+                    if (isWall[y1]) {
+                        dsum = dsum + dT[y1];
+                        bsrc = bsrc + tsT[y1];
+                    }
+                    if (isWall[y2]) {
+                        dsum = dsum + dT[y2];
+                        bsrc = bsrc + tsT[y2];
+                    }
+                    // transpose stress: internal faces in order, then the zero-coefficient wall
+                    const double t1 = q.xEfirst ? tsT[1] : tsT[0], t2 = q.xEfirst ? tsT[0] : tsT[1];
+                    ts = ts + t1;
+                    ts = ts + t2;
+                    if (!isWall[y1])
+                        ts = ts + tsT[y1];
+                    if (!isWall[y2])
+                        ts = ts + tsT[y2];
+                    for (int k = 2; k < 4; ++k)
+                        if (isWall[k]) {
+                            const double gcx = colX[c], gcy = colY[c];
+                            const int fi = (k == 2) ? c : c + nx;
+                            ts = ts + 0.0 * (gcx * C.ynx[fi] + gcy * C.yny[fi]) * C.ya[fi];
+                        }
+                    // deferred correction in face order (internal faces only)
+                    bcc = 0.0;
+                    (void)bcc;
+                }
+                double bsum = bsrc;
+                bsum -= (comp == 0 ? W.gPx[c] : W.gPy[c]) * C.vol[c];
+                if (fb != 0.0)
+                    bsum += fb * C.vol[c];
+                bsum += ts;
+                {
+                    const double x1 = q.xEfirst ? ccT[1] : ccT[0], x2 = q.xEfirst ? ccT[0] : ccT[1];
+                    bsum += x1;
+                    bsum += x2;
+                    const int y1 = q.yNfirst ? 3 : 2, y2 = q.yNfirst ? 2 : 3;
+                    if (!isWall[y1])
+                        bsum += ccT[y1];
+                    if (!isWall[y2])
+                        bsum += ccT[y2];
+                }
+                const double aU = st.aU;
+                const double draw = dsum;
+                bsum += (1.0 - aU) / aU * draw * U[c];
+                const double dd = draw / aU;
+                W.aPraw[c] = draw;
+                if (comp == 0)
+                    W.aP[c] = dd;
+                W.d[c] = dd;
+                W.aW[c] = aT[0];
+                W.aE[c] = aT[1];
+                W.aS[c] = aT[2];
+                W.aN[c] = aT[3];
+                W.b[c] = bsum;
+                // residual b - A U of this row (relaxation cancels at U)
+                const double tW = aT[0] * U[q.W], tE = aT[1] * U[q.E];
+                const double tS = q.south ? aT[2] * U[c - nx] : 0.0;
+                const double tN = q.north ? aT[3] * U[c + nx] : 0.0;
+                const double rc = bsum - accum4(q, dd * U[c], tW, tE, tS, tN);
+                W.r[c] = rc;
+                acc[0] += fabs(rc);
+                acc[1] += rc * rc;
+                if (comp == 0) {
+                    const double un = sqrt(W.Ux[c] * W.Ux[c] + W.Uy[c] * W.Uy[c] + 0.0);
+                    const double contribution = draw * un;
+                    acc[2] += contribution;
+                }
+            }
+            blockSum<3>(acc, S, rp);
+            momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
+            if (comp == 0)
+                momScale = acc[2];
+            resU[comp] = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, U, sqrt(acc[1]),
+                                  st.innerIter, st.innerTol);
+            __syncthreads();
+        }
+
+        // ---- predicted flux (stored Rhie-Chow, :1401-1419) and p' assembly (:717-830)
+        const double relaxCorr = 1.0 - st.aU;
+        double fs[1] = {0.0};
+        for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+            int o, q;
+            const double *A, *NX, *NY, *WT, *DL, *DX, *DY;
+            int fi;
+            bool wall = false;
+            if (f < n) {
+                fi = f;
+                o = f;
+                q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl; DX = C.xdx; DY = C.xdy;
+            } else {
+                fi = f - n;
+                const int jf = fi / nx;
+                wall = (jf == 0 || jf == ny);
+                o = fi - nx;
+                q = fi;
+                A = C.ya; NX = C.ynx; NY = C.yny; WT = C.yw; DL = C.ydl; DX = C.ydx; DY = C.ydy;
+            }
+            double ph, pc = 0.0;
+            if (wall) {
+                ph = (0.0 * NX[fi] + 0.0 * NY[fi]) * A[fi];
+            } else {
+                const double w = WT[fi];
+                const double ux = W.Ux[o] * w + W.Ux[q] * (1.0 - w), uy = W.Uy[o] * w + W.Uy[q] * (1.0 - w);
+                ph = (ux * NX[fi] + uy * NY[fi]) * A[fi];
+                const double delta = dmax(DL[fi], 1e-20);
+                const double dO = (fabs(W.aP[o]) > 1e-30) ? C.vol[o] / W.aP[o] : 0.0;
+                const double dN = (fabs(W.aP[q]) > 1e-30) ? C.vol[q] / W.aP[q] : 0.0;
+                const double dF = w * dO + (1.0 - w) * dN;
+                const double dl = dmax(DL[fi], 1e-30);
+                const double ex = DX[fi] / dl, ey = DY[fi] / dl;
+                const double gbx = W.gPx[o] * w + W.gPx[q] * (1.0 - w);
+                const double gby = W.gPy[o] * w + W.gPy[q] * (1.0 - w);
+                ph += -dF * A[fi] * ((W.p[q] - W.p[o]) / delta - (gbx * ex + gby * ey));
+                ph += relaxCorr * (W.phi[f] - W.phiOld[f]);
+                pc = dF * A[fi] / delta;
+            }
+            W.phiPred[f] = ph;
+            W.pCoeff[f] = pc;
+            fs[0] += fabs(ph);
+        }
+        __syncthreads();
+        double pacc[3] = {0.0, 0.0, fs[0]};
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            const int fE = c, fW = q.W, fN = n + c + nx, fS = n + c;
+            // diagonal: coefficients of internal faces in order
+            const double cW = W.pCoeff[fW], cE = W.pCoeff[fE];
+            const double cS = q.south ? W.pCoeff[fS] : 0.0, cN = q.north ? W.pCoeff[fN] : 0.0;
+            double dsum = 0.0;
+            {
+                const double x1 = q.xEfirst ? cE : cW, x2 = q.xEfirst ? cW : cE;
+                dsum = dsum + x1;
+                dsum = dsum + x2;
+                if (q.yNfirst) {
+                    if (q.north)
+                        dsum = dsum + cN;
+                } else {
+                    if (q.south)
+                        dsum = dsum + cS;
+                    if (q.north)
+                        dsum = dsum + cN;
+                }
+            }
+            // source: -(owner fluxes) + (neighbour fluxes), walls last
+            const double tW = W.phiPred[fW], tE = -W.phiPred[fE];
+            double bsum = 0.0;
+            {
+                const double x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+                bsum += x1;
+                bsum += x2;
+                if (q.yNfirst) {
+                    bsum += -W.phiPred[fN];
+                    bsum += -W.phiPred[fS]; // bottom wall
+                } else {
+                    bsum += q.south ? W.phiPred[fS] : -W.phiPred[fS];
+                    bsum += -W.phiPred[fN];
+                }
+            }
+            if (c == 0)
+                dsum += fabs(dsum) > 1e-30 ? dsum : 1.0; // pin of the outlet-free system
+            W.d[c] = dsum;
+            W.aW[c] = -cW;
+            W.aE[c] = -cE;
+            W.aS[c] = -cS;
+            W.aN[c] = -cN;
+            W.b[c] = bsum;
+            W.r[c] = bsum;
+            W.pp[c] = 0.0;
+            pacc[0] += fabs(bsum);
+            pacc[1] += bsum * bsum;
+        }
+        blockSum<3>(pacc, S, rp);
+        const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
+        const double fluxScale = pacc[2];
+        LinRes resP;
+        if (st.pSolver == kPBicgstab)
+            resP = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, W.pp, sqrt(pacc[1]), st.innerIter,
+                            st.innerTol);
+        else
+            resP = pcg(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver == kPAmg);
+        __syncthreads();
+
+        // ---- corrections (:916-940, :1443-1467): grad p' with owner-valued wall faces
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            double gx, gy;
+            ggCell(C, q, W.pp, W.pp[c], W.pp[c], gx, gy);
+            W.gKx[c] = gx; // scratch for grad p' (k gradients are recomputed below)
+            W.gKy[c] = gy;
+        }
+        __syncthreads();
+        FOR_CELLS(c) {
+            const double rA = (fabs(W.aP[c]) > 1e-30) ? 1.0 / W.aP[c] : 0.0;
+            W.Ux[c] -= rA * W.gKx[c] * C.vol[c];
+            W.Uy[c] -= rA * W.gKy[c] * C.vol[c];
+            W.p[c] += st.aP * W.pp[c];
+        }
+        for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+            double v;
+            if (f < n) {
+                const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                v = W.phiPred[f] - W.pCoeff[f] * (W.pp[q] - W.pp[f]);
+            } else {
+                const int g = f - n, jf = g / nx;
+                if (jf > 0 && jf < ny)
+                    v = W.phiPred[f] - W.pCoeff[f] * (W.pp[g] - W.pp[g - nx]);
+                else
+                    v = W.phiPred[f] + W.pCoeff[f] * W.pp[jf == 0 ? g : g - nx];
+            }
+            W.phi[f] = v;
+        }
+        __syncthreads();
+
+        // ---- turbulence (:1476-1538)
+        LinRes resK{0, 0, 0, true}, resW{0, 0, 0, true};
+        if (turbUpdate) {
+            FOR_CELLS(c) {
+                const Cell q = cellOf(C, c);
+                W.kOld[c] = W.k[c];
+                W.wOld[c] = W.w[c];
+                double gx, gy;
+                ggCell(C, q, W.k, 0.0, 0.0, gx, gy);
+                W.gKx[c] = gx;
+                W.gKy[c] = gy;
+            }
+            __syncthreads();
+            for (int eq = 0; eq < 2; ++eq) { // 0: k, 1: omega
+                double *X = eq == 0 ? W.k : W.w;
+                const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
+                if (eq == 1) {
+                    FOR_CELLS(c) {
+                        const Cell q = cellOf(C, c);
+                        double gx, gy;
+                        ggCell(C, q, W.w, bwOf(q.i), bwOf(ny * nx + q.i), gx, gy);
+                        W.gWx[c] = gx;
+                        W.gWy[c] = gy;
+                    }
+                    __syncthreads();
+                }
+                double acc[1] = {0.0};
+                FOR_CELLS(c) {
+                    const Cell q = cellOf(C, c);
+                    const bool isWall[4] = {false, false, !q.south, !q.north};
+                    double dT[4] = {0, 0, 0, 0}, aT[4] = {0, 0, 0, 0}, ccT[4] = {0, 0, 0, 0};
+                    double bT[4] = {0, 0, 0, 0}, balT[4] = {0, 0, 0, 0};
+                    for (int k = 0; k < 4; ++k) {
+                        bool own;
+                        int o, qn, fi, f;
+                        const double *A, *WT, *DL;
+                        double sh = 0.0;
+                        if (k < 2) {
+                            fi = (k == 0) ? q.W : c;
+                            own = (k == 1);
+                            o = fi;
+                            qn = (k == 0) ? c : q.E;
+                            A = C.xa; WT = C.xw; DL = C.xdl;
+                            sh = C.xsh[fi];
+                            f = fi;
+                        } else {
+                            fi = (k == 2) ? c : c + nx;
+                            own = (k == 3) || isWall[k];
+                            o = (k == 2) ? c - nx : c;
+                            qn = (k == 2) ? c : c + nx;
+                            A = C.ya; WT = C.yw; DL = C.ydl;
+                            f = n + fi;
+                        }
+                        const double delta = dmax(DL[fi], 1e-20);
+                        const double F = W.phi[f];
+                        if (isWall[k]) {
+                            const double sg = eq == 0 ? blend(sk1, sk2, W.F1[c]) : blend(sw1, sw2, W.F1[c]);
+                            const double Db = (nu + sg * W.nuT[c]) * A[fi] / delta;
+                            const double xb = eq == 0 ? 0.0 : bwOf(fi);
+                            if (F >= 0) {
+                                dT[k] = F + Db;
+                                bT[k] = Db * xb;
+                            } else {
+                                dT[k] = Db;
+                                bT[k] = (Db - F) * xb;
+                            }
+                            continue;
+                        }
+                        const double w = WT[fi];
+                        const double F1f = w * W.F1[o] + (1.0 - w) * W.F1[qn];
+                        const double sg = eq == 0 ? blend(sk1, sk2, F1f) : blend(sw1, sw2, F1f);
+                        const double eO = nu + sg * W.nuT[o], eN = nu + sg * W.nuT[qn];
+                        const double ef = w * eO + (1.0 - w) * eN;
+                        const double D = ef * A[fi] / delta;
+                        const double cp = dmax(F, 0.0), cn = dmax(-F, 0.0);
+                        dT[k] = own ? D + cp : D + cn;
+                        aT[k] = own ? -(D + cn) : -(D + cp);
+                        if (eq == 1 && C.balance) { // singular near-wall balance (:1073-1087)
+                            const double amp = 6 * nu / b1;
+                            const double diff = (C.sing[qn] - C.sing[o]) / delta;
+                            const double sgd = (k < 2) ? C.sgx[fi] : C.sgy[fi];
+                            const double corr = amp * A[fi] * ((ef - nu) * sgd - ef * diff);
+                            balT[k] = own ? corr : -corr;
+                        }
+                        if (F != 0.0) {
+                            const bool ownerUp = F > 0.0;
+                            const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
+                            const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
+                            const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
+                            const double dphi = X[dn] - X[up];
+                            double psi = 0.0;
+                            if (fabs(dphi) > 1e-300) {
+                                const double rr = 2.0 * (gX[up] * (xDx - C.cx[up]) + gY[up] * (xDy - C.cy[up])) / dphi - 1.0;
+                                psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
+                            }
+                            const double pf = X[up] + 0.5 * psi * dphi;
+                            const double corr = F * (pf - X[up]);
+                            ccT[k] = own ? -corr : corr;
+                        }
+                    }
+                    // face-order sums: internal faces, then the wall face
+                    const int y1 = q.yNfirst ? 3 : 2, y2 = q.yNfirst ? 2 : 3;
+                    const int x1 = q.xEfirst ? 1 : 0, x2 = q.xEfirst ? 0 : 1;
+                    const int ord[4] = {x1, x2, y1, y2};
+                    double dsum = 0.0, bsum = 0.0, bal = 0.0;
+                    for (int t = 0; t < 4; ++t)
+                        if (!isWall[ord[t]]) {
+                            dsum = dsum + dT[ord[t]];
+                            bal = bal + balT[ord[t]];
+                        }
+                    for (int t = 0; t < 4; ++t)
+                        if (isWall[ord[t]]) {
+                            dsum = dsum + dT[ord[t]];
+                            bsum = bsum + bT[ord[t]];
+                        }
+                    const double V = C.vol[c], F1 = W.F1[c];
+                    if (eq == 0) {
+                        bsum += W.Pk[c] * V;
+                        dsum += bs * dmax(W.w[c], 1e-20) * V;
+                    } else {
+                        const double wc = dmax(W.w[c], 1e-20);
+                        const double Sv = W.S[c];
+                        const double S2 = Sv * Sv;
+                        const double lim = 10.0 * bs * dmax(W.k[c], 0.0) * dmax(W.w[c], 1e-20) / dmax(W.nuT[c], 1e-30);
+                        const double prod = dmin(S2, lim);
+                        bsum += blend(al1, al2, F1) * prod * V;
+                        dsum += blend(b1, b2, F1) * wc * V;
+                        bsum += (1.0 - F1) * W.CD[c] * V;
+                        if (C.balance) {
+                            const double corr = bal + nu * (6 * nu / b1) * C.slap[c] * V;
+                            if (corr < 0)
+                                dsum -= corr / wc;
+                            else
+                                bsum += corr;
+                        }
+                    }
+                    for (int t = 0; t < 4; ++t)
+                        if (!isWall[ord[t]])
+                            bsum += ccT[ord[t]];
+                    const double al = eq == 0 ? st.aK : st.aW;
+                    bsum += (1.0 - al) / al * dsum * X[c];
+                    dsum /= al;
+                    // omega: eliminate constrained wall cells (constrainOmega :687-704)
+                    double x0 = X[c];
+                    if (eq == 1) {
+                        const int nbc[4] = {q.W, q.E, c - nx, c + nx};
+                        const bool selfW = !q.south || !q.north;
+                        for (int t = 0; t < 4; ++t) {
+                            const int k = ord[t];
+                            if (isWall[k])
+                                continue;
+                            const int qq = nbc[k];
+                            const int jq = qq / nx;
+                            const bool nbW = (jq == 0 || jq == ny - 1);
+                            const bool own = (k == 1 || k == 3);
+                            if (own) {
+                                if (selfW) {
+                                    aT[k] = 0.0;
+                                } else if (nbW) {
+                                    bsum -= aT[k] * wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, qq)], 1e-20));
+                                    aT[k] = 0.0;
+                                }
+                            } else {
+                                if (nbW) {
+                                    bsum -= aT[k] * wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, qq)], 1e-20));
+                                    aT[k] = 0.0;
+                                } else if (selfW) {
+                                    aT[k] = 0.0;
+                                }
+                            }
+                        }
+                        if (selfW) {
+                            const double val = wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, c)], 1e-20));
+                            bsum = dsum * val;
+                            x0 = val;
+                        }
+                    }
+                    W.d[c] = dsum;
+                    W.aW[c] = aT[0];
+                    W.aE[c] = aT[1];
+                    W.aS[c] = aT[2];
+                    W.aN[c] = aT[3];
+                    W.b[c] = bsum;
+                    (void)x0;
+                }
+                __syncthreads();
+                // initial residual with the (constrained) initial guess: wall cells of
+                // omega start from their wall value (read through x0, never from X,
+                // so the in-place update below cannot race with a neighbour's read)
+                FOR_CELLS(c) {
+                    const Cell q = cellOf(C, c);
+                    auto x0 = [&](int cc) {
+                        return (eq == 1 && isWallCell(C, cc))
+                                   ? wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, cc)], 1e-20))
+                                   : X[cc];
+                    };
+                    const double tW = W.aW[c] * x0(q.W), tE = W.aE[c] * x0(q.E);
+                    const double tS = q.south ? W.aS[c] * x0(c - nx) : 0.0;
+                    const double tN = q.north ? W.aN[c] * x0(c + nx) : 0.0;
+                    const double xc = x0(c);
+                    const double rc = W.b[c] - accum4(q, W.d[c] * xc, tW, tE, tS, tN);
+                    W.r[c] = rc;
+                    acc[0] += rc * rc;
+                    if (eq == 1)
+                        X[c] = xc;
+                }
+                blockSum<1>(acc, S, rp);
+                LinRes rr = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, X, sqrt(acc[0]),
+                                     st.innerIter, st.innerTol);
+                if (eq == 0)
+                    resK = rr;
+                else
+                    resW = rr;
+                __syncthreads();
+                if (eq == 0) {
+                    FOR_CELLS(c) W.k[c] = dmax(st.kMin, dmin(st.kMax, W.k[c]));
+                } else {
+                    FOR_CELLS(c) {
+                        const Cell q = cellOf(C, c);
+                        double v = dmax(st.wMin, dmin(1e15, W.w[c]));
+                        if (!q.south || !q.north)
+                            v = wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, c)], 1e-20));
+                        W.w[c] = v;
+                    }
+                    wallBetaInit = false;
+                }
+                __syncthreads();
+            }
+        }
+
+        // ---- change norms and bookkeeping (:1520-1715)
+        double mx[6] = {1e-30, 1e-30, 0.0, 0.0, 1e-300, 0.0};
+        FOR_CELLS(c) {
+            if (turbUpdate) {
+                mx[0] = dmax(mx[0], fabs(W.k[c]));
+                mx[1] = dmax(mx[1], fabs(W.w[c]));
+                mx[2] = dmax(mx[2], fabs(W.k[c] - W.kOld[c]));
+                mx[3] = dmax(mx[3], fabs(W.w[c] - W.wOld[c]));
+            }
+            mx[4] = dmax(mx[4], sqrt(W.Ux[c] * W.Ux[c] + W.Uy[c] * W.Uy[c] + 0.0));
+            const double ax = W.Ux[c] - W.Uxp[c], ay = W.Uy[c] - W.Uyp[c];
+            mx[5] = dmax(mx[5], sqrt(ax * ax + ay * ay + 0.0));
+        }
+        blockMax<6>(mx, S, rp);
+        if (turbUpdate) {
+            lastK = mx[2] / mx[0];
+            lastW = mx[3] / mx[1];
+            pushSample(S, 1, lastK);
+            pushSample(S, 2, lastW);
+        }
+        double e[11];
+        e[0] = iter;
+        e[1] = resU[0].initialRes;
+        e[2] = resU[1].initialRes;
+        e[3] = 0.0;
+        e[4] = resP.initialRes;
+        e[5] = turbActive ? lastK : 0.0;
+        e[6] = turbActive ? lastW : 0.0;
+        e[7] = momRes / dmax(momScale, 1e-300);
+        e[8] = contScaled;
+        e[9] = mx[5] / mx[4];
+        pushSample(S, 0, e[9]);
+        const Est eU = estimate(S, 0, st.window, negligible);
+        e[10] = eU.remaining;
+        const bool haveMonitor = C.nobs > 0;
+        if (haveMonitor && iter % (st.monitorInterval > 1 ? st.monitorInterval : 1) == 0) {
+            if (threadIdx.x < C.nobs) { // PreparedObservation::evaluate (:678-772)
+                const int t = threadIdx.x;
+                const int cell = C.pcell[t];
+                const double *X = C.obsComp == 0 ? W.Ux : W.Uy;
+                const double center = X[cell];
+                double bx = 0, by = 0;
+                for (int k = 0; k < C.pnnb[t]; ++k) {
+                    const int nb = C.pnb[4 * t + k];
+                    const double diff = (nb < 0 ? 0.0 : X[nb]) - center;
+                    bx += C.pwt[4 * t + k] * C.pdx[4 * t + k] * diff;
+                    by += C.pwt[4 * t + k] * C.pdy[4 * t + k] * diff;
+                }
+                double gx = 0.0, gy = 0.0;
+                if (fabs(C.pdet[t]) > 1e-14 * (C.paxx[t] * C.payy[t] + 1e-300)) {
+                    gx = (C.payy[t] * bx - C.paxy[t] * by) / C.pdet[t];
+                    gy = (C.paxx[t] * by - C.paxy[t] * bx) / C.pdet[t];
+                }
+                S.q[t] = center + gx * C.pox[t] + gy * C.poy[t];
+            }
+            __syncthreads();
+            bool finite = true;
+            for (int t = 0; t < C.nobs; ++t)
+                finite = finite && isfinite(S.q[t]);
+            if (!finite) { // the reference throws here: the row becomes Unknown
+                status = 4;
+                finalIter = iter;
+                break;
+            }
+            if (S.haveQPrev) {
+                double qMax = 0.0, dq = 0.0;
+                for (int t = 0; t < C.nobs; ++t)
+                    qMax = dmax(qMax, fabs(S.q[t]));
+                for (int t = 0; t < C.nobs; ++t) {
+                    const double fl = C.obsFloor[t];
+                    dq = dmax(dq, fabs(S.q[t] - S.qPrev[t]) / dmax(dmax(fabs(S.q[t]), fl), 1e-300));
+                }
+                pushSample(S, 3, dq);
+            }
+            __syncthreads();
+            if (threadIdx.x < C.nobs)
+                S.qPrev[threadIdx.x] = S.q[threadIdx.x];
+            if (threadIdx.x == 0)
+                S.haveQPrev = 1;
+            __syncthreads();
+        }
+        {
+            double wv = e[7];
+            wv = dmax(wv, e[8]);
+            wv = dmax(wv, e[9]);
+            wv = dmax(wv, e[10]);
+            worst = wv;
+        }
+        if (turbActive) {
+            const Est eK = estimate(S, 1, st.window, negligible);
+            const Est eW = estimate(S, 2, st.window, negligible);
+            double wv = worst;
+            wv = dmax(wv, lastK);
+            wv = dmax(wv, eK.remaining);
+            wv = dmax(wv, lastW);
+            wv = dmax(wv, eW.remaining);
+            worst = wv;
+        }
+        if (haveMonitor) {
+            const Est eQ = estimate(S, 3, st.window, negligible);
+            const double last = S.cnt[3] > 0 ? S.ring[3][(S.cnt[3] - 1) % kWindowCap] : inf;
+            double wv = worst;
+            wv = dmax(wv, last);
+            wv = dmax(wv, eQ.remaining);
+            worst = wv;
+        }
+        if (!isfinite(worst))
+            worst = inf;
+        if (iter == 0) {
+            n0x = dmax(e[1], 1e-30);
+            n0y = dmax(e[2], 1e-30);
+            n0p = dmax(e[4], 1e-30);
+            fluxRef = fluxScale;
+        } else if (iter < 50) {
+            n0p = dmax(n0p, e[4]);
+            fluxRef = dmax(fluxRef, fluxScale);
+        }
+        auto safe = [](double v, double ref) { return ref < 1e-20 ? 0.0 : v / ref; };
+        const double nm = dmax(n0x, n0y);
+        const double nUx = safe(e[1], nm), nUy = safe(e[2], nm);
+        const double nP = safe(e[4], dmax(n0p, fluxRef));
+        if (job.hist && iter < job.histCap && threadIdx.x == 0)
+            for (int t = 0; t < 11; ++t)
+                job.hist[11L * iter + t] = e[t];
+        double maxRes = dmax(dmax(nUx, nUy), nP);
+        if (turbActive)
+            maxRes = dmax(dmax(maxRes, lastK), lastW);
+        bool bad = !isfinite(lastK) || !isfinite(lastW);
+        for (int t = 1; t <= 9; ++t)
+            bad = bad || !isfinite(e[t]);
+        if (bad) {
+            maxRes = inf;
+            worst = inf;
+        }
+        rateU = eU.rate;
+        const bool turbScheduled = st.turbStart < st.maxIter;
+        if (worst < tol && iter > 0 && (!turbScheduled || (turbActive && established))) {
+            converged = true;
+            finalIter = iter;
+            status = 0;
+            break;
+        }
+        if (isnan(maxRes) || isinf(maxRes) || maxRes > st.divLimit) {
+            diverged = true;
+            finalIter = iter;
+            status = 2;
+            break;
+        }
+    }
+    __syncthreads();
+    const bool stalled = !converged && !diverged && status == 1 && isfinite(rateU) && rateU >= 1.0;
+
+    // ---- outputs: verdict, probe predictions, log-likelihood (ObservationOperator.hpp:592-609)
+    if (status == 0 || status == 1) {
+        if (threadIdx.x < C.nobs) {
+            const int t = threadIdx.x;
+            const int cell = C.pcell[t];
+            const double *X = C.obsComp == 0 ? W.Ux : W.Uy;
+            const double center = X[cell];
+            double bx = 0, by = 0;
+            for (int k = 0; k < C.pnnb[t]; ++k) {
+                const int nb = C.pnb[4 * t + k];
+                const double diff = (nb < 0 ? 0.0 : X[nb]) - center;
+                bx += C.pwt[4 * t + k] * C.pdx[4 * t + k] * diff;
+                by += C.pwt[4 * t + k] * C.pdy[4 * t + k] * diff;
+            }
+            double gx = 0.0, gy = 0.0;
+            if (fabs(C.pdet[t]) > 1e-14 * (C.paxx[t] * C.payy[t] + 1e-300)) {
+                gx = (C.payy[t] * bx - C.paxy[t] * by) / C.pdet[t];
+                gy = (C.paxx[t] * by - C.paxy[t] * bx) / C.pdet[t];
+            }
+            S.q[t] = center + gx * C.pox[t] + gy * C.poy[t];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        RowOut o;
+        o.iterations = finalIter;
+        o.stalled = stalled;
+        o.converged = converged;
+        o.finalWorst = worst;
+        o.contractionRate = rateU;
+        o.status = status;
+        o.loglik = status == 2 ? -1e6 : (status == 4 ? -1e6 : 0.0);
+        if (status == 0 || status == 1) {
+            double ll = 0.0;
+            bool ok = true;
+            for (int t = 0; t < C.nobs; ++t) {
+                const double v = S.q[t];
+                job.pred[t] = v;
+                ok = ok && isfinite(v);
+                const double diff = v - C.obsVal[t];
+                ll += -0.5 * diff * diff / C.obsVar[t];
+            }
+            if (!ok || !isfinite(ll)) {
+                o.status = 4;
+                o.loglik = -1e6;
+            } else {
+                o.loglik = ll;
+            }
+        }
+        if (o.status != 0 && o.status != 1)
+            for (int t = 0; t < C.nobs; ++t)
+                job.pred[t] = __longlong_as_double(0x7ff8000000000000LL);
+        *job.row = o;
+    }
+    if (job.fields && status != 2) {
+        const double *src[11] = {W.Ux, W.Uy, nullptr, W.p, W.k, W.w, W.nuT, W.F1, W.F2, W.Pk, W.CD};
+        for (int b = 0; b < 11; ++b)
+            FOR_CELLS(c) job.fields[(long)b * n + c] = src[b] ? src[b][c] : 0.0;
+    }
+    __syncthreads();
+}
+
+} // namespace
+
+__global__ void __launch_bounds__(512) solveKernel(const DevJob *jobs, int njobs, int *nextJob,
+                                                   double *wsBase, long wsStride) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    Shared &S = *reinterpret_cast<Shared *>(smemRaw);
+    double *ws = wsBase + wsStride * blockIdx.x;
+    for (;;) {
+        if (threadIdx.x == 0)
+            S.job = atomicAdd(nextJob, 1);
+        __syncthreads();
+        const int j = S.job;
+        if (j >= njobs)
+            break;
+        const DevJob &job = jobs[j];
+        // class descriptor and coefficients into shared memory
+        {
+            const int words = sizeof(DevClass) / 4;
+            const int *src = reinterpret_cast<const int *>(job.cls);
+            int *dst = reinterpret_cast<int *>(&S.C);
+            for (int t = threadIdx.x; t < words; t += blockDim.x)
+                dst[t] = src[t];
+            if (threadIdx.x < 11)
+                S.coeff[threadIdx.x] = job.coeffs[threadIdx.x];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            carve(S, ws);
+        __syncthreads();
+        runSolve(S, job);
+        __syncthreads();
+    }
+}
+
+size_t solveSharedBytes() { return sizeof(Shared); }
+
+cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
+                        int grid, int block, cudaStream_t stream) {
+    const size_t smem = sizeof(Shared);
+    cudaError_t e = cudaFuncSetAttribute(solveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    solveKernel<<<grid, block, smem, stream>>>(jobs, njobs, nextJob, ws, wsStride);
+    return cudaGetLastError();
+}
+
+} // namespace rq
+
+namespace rq {
+int solveBlocksPerSM(int block) {
+    int blocks = 0;
+    const size_t smem = sizeof(Shared);
+    cudaFuncSetAttribute(solveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, solveKernel, block, smem) !=
+        cudaSuccess)
+        return 1;
+    return blocks > 0 ? blocks : 1;
+}
+} // namespace rq

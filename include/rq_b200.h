@@ -1,0 +1,184 @@
+/*
+ * rq_b200.h -- C ABI of the B200-native forward model for Bayesian calibration
+ * of RANS (k-omega SST) closure coefficients.
+ *
+ * Plain C types only: host pointers and sizes in, host buffers out (the
+ * *_device variants take device pointers and a CUDA stream as void*). Every
+ * entry point returns RQ_OK or a negative RQ_E_* code; rq_last_error() gives
+ * the message of the calling thread's last failure. No C++ exception crosses
+ * this boundary.
+ *
+ * Reference interfaces replaced (paths in the reference project):
+ *   rq_problem_create / rq_problem_destroy
+ *       ForwardBatch(mesh, parameters, observations, boundaries, nu, settings, U, p, k, omega)
+ *       rans-uq/include/ForwardBatch.hpp:34-49, ForwardModel ctor rans-uq/src/ForwardModel.cpp:8-18
+ *   rq_evaluate_batch
+ *       ForwardBatch::evaluate(theta rows, workers)              rans-uq/include/ForwardBatch.hpp:52-124
+ *       (per row: ForwardModel::evaluateWithDiagnostics        rans-uq/src/ForwardModel.cpp:35-137)
+ *   rq_evaluate_multi
+ *       several ForwardBatch::evaluate calls (one per mesh class) fused into one launch
+ *   rq_solve
+ *       SIMPLESolver::initUniform + solve(FlowFields&, Workspace&) rans-uq/src/SIMPLESolver.cpp:267-298, 1193-1716
+ *   rq_linear_solve
+ *       makeSolver(name)->solve(LinearSystem, x, maxIter, tol)  core/include/LinearSolver.hpp:137-153, 988-998
+ *   rq_mesh_geometry
+ *       Mesh::makePeriodicChannel2D / makeCurvedChannelPeriodic2D + computeWallDistance
+ *       core/src/Mesh.cpp:490-741, 431-463
+ */
+#ifndef RQ_B200_H
+#define RQ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes */
+#define RQ_OK 0
+#define RQ_E_INVALID -1      /* invalid argument (the reference throws std::invalid_argument) */
+#define RQ_E_CUDA -2         /* CUDA runtime failure (no device, launch error, ...)          */
+#define RQ_E_OOM -3          /* device memory exhausted (the reference's bad_alloc)            */
+#define RQ_E_UNSUPPORTED -4  /* outside the GPU path's scope (see the message)                */
+
+/* ---- EvaluationStatus, same values and order (core/include/EvaluationTypes.hpp:6) */
+#define RQ_CONVERGED 0
+#define RQ_UNCONVERGED 1
+#define RQ_DIVERGED 2
+#define RQ_INVALID_PARAMETERS 3
+#define RQ_UNKNOWN 4
+
+/* ---- linear solver kinds: the reference factory names "AMG", "PCG", "BiCGSTAB" */
+#define RQ_SOLVER_AMG 0
+#define RQ_SOLVER_PCG 1
+#define RQ_SOLVER_BICGSTAB 2
+
+/* ---- inner-solve precision */
+#define RQ_PREC_FP64 0   /* plain form: every inner solve in FP64 */
+#define RQ_PREC_MIXED 1  /* FP32 Krylov/AMG sweeps with FP64 residual refinement */
+
+/* mesh kinds */
+#define RQ_MESH_PERIODIC_CHANNEL 0 /* Mesh::makePeriodicChannel2D(nx, ny, lx, h, re_tau, yplus) */
+#define RQ_MESH_CURVED_PERIODIC 1  /* Mesh::makeCurvedChannelPeriodic2D(x_nodes, y_bottom, y_top, ny, re, yplus) */
+
+typedef struct rq_mesh_desc {
+    int32_t kind, nx, ny, pad;
+    double lx, h, re_tau, yplus;        /* channel */
+    const double *x_nodes;              /* curved: nx+1 x nodes */
+    const double *y_bottom;             /* curved: nx+1 bottom samples (periodic) */
+    double y_top, re;                   /* curved */
+} rq_mesh_desc;
+
+/* FlowBoundaryConditions::channelDefaults(mesh, u_in, k_in, omega_in): on the
+   streamwise-periodic meshes every boundary is a no-slip k-omega wall. */
+typedef struct rq_bc_desc {
+    double u_in, k_in, omega_in;
+} rq_bc_desc;
+
+/* SolverSettings (core/include/FlowFields.hpp:70-241), hot-path subset. */
+typedef struct rq_settings {
+    int32_t max_iterations;      /* 500     */
+    int32_t inner_iterations;    /* 200     */
+    int32_t convergence_window;  /* 25      */
+    int32_t monitor_interval;    /* 10      */
+    int32_t turb_start_iter;     /* 5       */
+    int32_t turb_update_interval;/* 1       */
+    int32_t nut_floor_iters;     /* 500     */
+    int32_t pressure_solver;     /* RQ_SOLVER_AMG */
+    int32_t precision;           /* RQ_PREC_FP64 */
+    int32_t block_threads;       /* 0 = autotuned CTA size */
+    double convergence_tol;      /* 1e-5    */
+    double inner_tolerance;      /* 1e-3    */
+    double divergence_limit;     /* 1e6     */
+    double alpha_u, alpha_p, alpha_k, alpha_omega; /* 0.7 0.3 0.5 0.5 */
+    double body_force[3];        /* 0 0 0   */
+    double k_min, k_max, omega_min; /* 1e-10 1e10 1e-6 */
+} rq_settings;
+
+/* Velocity-profile probes (ObservationOperator::addVelocityProfile). */
+typedef struct rq_obs_desc {
+    int32_t n_obs, component;      /* component 0 = x, 1 = y */
+    const double *x, *y;           /* probe locations */
+    const double *observed;        /* y_obs */
+    const double *sigma_obs;       /* observation std */
+    const double *sigma_model;     /* model discrepancy std (may be NULL) */
+} rq_obs_desc;
+
+/* One batch row (ForwardBatchRow, rans-uq/include/ForwardBatch.hpp:8-14). */
+typedef struct rq_row_out {
+    int32_t status;        /* RQ_CONVERGED ... RQ_UNKNOWN */
+    int32_t iterations;    /* EvaluationResult::simpleIters */
+    int32_t stalled;
+    int32_t converged;
+    double loglik;         /* -1e30 invalid, -1e6 diverged/unknown */
+    double final_worst;    /* ConvergenceHistory::finalWorstMeasure */
+    double contraction_rate;
+} rq_row_out;
+
+/* Solver result (SolverResult, core/include/LinearSolver.hpp:137-143). */
+typedef struct rq_solver_result {
+    int32_t iterations, converged;
+    double final_res, initial_res;
+} rq_solver_result;
+
+/* LDU system (LinearSystem, core/include/LinearSolver.hpp:20-116). */
+typedef struct rq_ldu {
+    int32_t n_cells, n_faces;
+    const double *diag, *upper, *lower, *source;
+    const int32_t *owner, *neighbour;
+} rq_ldu;
+
+typedef struct rq_problem rq_problem;
+
+const char *rq_last_error(void);
+int rq_version(void);
+
+/* Fills s with the reference's SolverSettings defaults. */
+int rq_default_settings(rq_settings *s);
+
+/* Builds a mesh class on the device. init = {Ux, Uy, Uz, p, k, omega} (cold start);
+   active = InferenceParameterSet active indices (0..10), base = the 11 coefficients
+   that fill the inactive ones (SSTCoefficients order). */
+int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
+                      const rq_settings *settings, const rq_obs_desc *obs, const double init[6],
+                      const int32_t *active, int32_t n_active, const double base[11],
+                      rq_problem **out);
+int rq_problem_destroy(rq_problem *p);
+int rq_problem_info(const rq_problem *p, int32_t *n_cells, int32_t *n_obs, int32_t *n_active,
+                    int32_t *amg_levels);
+
+/* theta: n rows x n_active (host). rows: n (host). predictions: n x n_obs (host,
+   NaN where the reference returns none). fields (optional, host): n x 11 x n_cells,
+   blocks Ux Uy Uz p k omega nuT F1 F2 Pk CDkw. history (optional): n x hist_cap x 11. */
+int rq_evaluate_batch(rq_problem *p, const double *theta, int64_t n, rq_row_out *rows,
+                      double *predictions, double *fields, double *history, int32_t hist_cap);
+
+/* Several mesh classes in one persistent launch: row i uses problems[problem_of_row[i]];
+   theta rows are padded to max n_active (row stride = theta_stride doubles),
+   predictions to max n_obs (stride = pred_stride). */
+int rq_evaluate_multi(rq_problem *const *problems, int32_t n_problems,
+                      const int32_t *problem_of_row, const double *theta, int32_t theta_stride,
+                      int64_t n, rq_row_out *rows, double *predictions, int32_t pred_stride);
+
+/* Same on device buffers (device theta, rows, predictions) on a CUDA stream (cudaStream_t as void*). */
+int rq_evaluate_multi_device(rq_problem *const *problems, int32_t n_problems,
+                             const int32_t *problem_of_row_host, const double *theta_dev,
+                             int32_t theta_stride, int64_t n, rq_row_out *rows_dev,
+                             double *predictions_dev, int32_t pred_stride, void *stream);
+
+/* One solve from a cold start with all eleven coefficients. */
+int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *predictions,
+             double *fields, double *history, int32_t hist_cap);
+
+/* Mesh geometry as built for the device (nCells x 4: cx, cy, volume, wall distance). */
+int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells);
+
+/* The linear solvers of the forward model on one LDU system (kind RQ_SOLVER_*);
+   x: initial guess in, solution out (host). */
+int rq_linear_solve(const rq_ldu *A, double *x, int32_t max_iter, double tol, int32_t kind,
+                    rq_solver_result *result);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,60 @@
+"""Regenerates the golden fixtures of tests/golden/ from the reference itself.
+
+Run in a container where the reference sources are mounted and oracle/_ref is
+built (``make -C oracle ref``):  python tests/golden/make_golden.py
+Every number written here was computed by the compiled reference
+(oracle/_ref/libcfdr_ref.so, the reference's own ForwardModel), or read from
+the reference's committed golden JSON.
+"""
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "tests"))
+from oracle import checker as ck  # noqa: E402
+import cases  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+REF = Path("/root/reference")
+
+
+def solve_npz(name, case, hist=0):
+    o = ck.solve(case, "ref", hist_cap=hist)
+    np.savez_compressed(OUT / f"{name}.npz", status=o.status, iterations=o.iterations,
+                        loglik=o.loglik, final_worst=o.final_worst, predictions=o.predictions,
+                        Ux=o.field("Ux"), k=o.field("k"), omega=o.field("omega"),
+                        nuT=o.field("nuT"), p=o.field("p"))
+    print(name, o.status, o.iterations, flush=True)
+
+
+def main():
+    which = set(sys.argv[1:]) or {"small", "config1", "goldens"}
+    if "small" in which:
+        solve_npz("small_channel_ref", cases.small_channel())
+        solve_npz("small_channel_pcg_ref", cases.small_channel(pressure_solver=ck.P_PCG))
+    if "config1" in which:
+        solve_npz("config1_ref", ck.config1_case())
+    if "goldens" in which:
+        g = json.loads((REF / "tests/golden/constrained_omega/periodic_channel_re180.json").read_text())
+        keep = {"nu": g["nu"], "mesh": g["mesh"], "settings": g["settings"],
+                "result": {k: g["result"][k] for k in ("status", "final_iter", "final_worst_measure",
+                                                        "contraction_rate_u")},
+                "field_norms": g["result"]["field_norms"],
+                "probe_y_over_delta": g["qoi"]["probe_y_over_delta"],
+                "u_plus_probes": g["qoi"]["u_plus_probes"]}
+        src = (REF / "rans-uq/tests/test_sst_channel_grid_convergence.cpp").read_text()
+        keep["grid_convergence_note"] = "stations and U+ of test_sst_channel_grid_convergence.cpp:14-17"
+        keep["grid_convergence_stations"] = [0.01, 0.03, 0.1, 0.2, 0.4, 0.7, 0.95]
+        import re
+        block = src[src.index("reference{"):src.index("};", src.index("reference{"))]
+        keep["grid_convergence_uplus"] = [float(v) for v in re.findall(r"[0-9]+\.[0-9]+", block)]
+        (OUT / "reference_goldens.json").write_text(json.dumps(keep, indent=1))
+        print("goldens", len(keep["grid_convergence_uplus"]))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,106 @@
+"""GPU parity of the B200 forward model against the CPU checkers.
+
+* Trajectory parity: the fields after N outer iterations equal the C++
+  restatement (oracle/rq_oracle.cpp) run with the same linear solvers, to
+  round-off (rtol 1e-9 on the max-norm; the differences are reduction order).
+* Converged parity: converged profiles equal the compiled reference's own
+  ForwardModel (golden fixtures made by tests/golden/make_golden.py) to 1e-10
+  relative, with identical convergence verdicts.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import checker as ck
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = cases.__file__.replace("cases.py", "golden/")
+RTOL_TRAJ = 1e-9
+RTOL_CONV = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("solver,ps", [("AMG", ck.P_AMG), ("PCG", ck.P_PCG)])
+@pytest.mark.parametrize("n_iter", [1, 7, 40])
+def test_fields_after_n_iterations(rq, checker, solver, ps, n_iter):
+    case = cases.small_channel(max_iter=n_iter, pressure_solver=ps)
+    want = checker.solve(case, "oracle", hist_cap=n_iter)
+    batch = cases.product_batch(rq, case, pressure_solver=solver)
+    res, fields, hist = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]], hist_cap=n_iter)
+    row = res.rows[0]
+    assert row.result.status.name == "Unconverged" and row.result.simple_iters == n_iter
+    for name in ("Ux", "k", "omega", "nuT", "F1", "Pk"):
+        i = ck.FIELD_NAMES.index(name)
+        scale = max(np.max(np.abs(want.fields[i])), 1e-300)
+        err = np.max(np.abs(fields[0, i] - want.fields[i])) / scale
+        assert err < RTOL_TRAJ, (name, err)
+    # Uy and p are round-off noise (~1e-13, ~1e-12) in a fully developed channel:
+    # compare them on the velocity scale and on an absolute pressure scale
+    uscale = np.max(np.abs(want.field("Ux")))
+    assert np.max(np.abs(fields[0, 1] - want.field("Uy"))) / uscale < RTOL_TRAJ
+    assert np.max(np.abs(fields[0, 3] - want.field("p"))) < 1e-9
+    # residual history: initial residuals of the x-momentum and pressure solves and the
+    # scaled momentum residual / relative change of U judged by the convergence test
+    h, g = hist[0], want.history
+    for col in (1, 4, 7, 9):
+        assert rel(h[:, col], g[:, col]) < 1e-8, col
+
+
+@pytest.mark.parametrize("fixture,solver", [("small_channel_ref", "AMG"),
+                                            ("small_channel_pcg_ref", "PCG")])
+def test_converged_small_channel_matches_reference(rq, fixture, solver):
+    g = np.load(GOLDEN + fixture + ".npz")
+    case = cases.small_channel()
+    batch = cases.product_batch(rq, case, pressure_solver=solver)
+    res, fields, _ = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]])
+    row = res.rows[0]
+    assert row.result.status.name == str(g["status"])
+    assert rel(row.result.predictions, g["predictions"]) < RTOL_CONV
+    assert rel(fields[0, 0], g["Ux"]) < RTOL_CONV
+    assert rel(fields[0, 4], g["k"]) < 1e-8
+    assert abs(row.result.simple_iters - int(g["iterations"])) <= 0.02 * int(g["iterations"])
+
+
+def test_config1_matches_reference(rq):
+    """Plain small case: 3x128 channel, tol 1e-10 -- profiles within 1e-10 of the reference."""
+    g = np.load(GOLDEN + "config1_ref.npz")
+    case = ck.config1_case()
+    batch = cases.product_batch(rq, case)
+    res, fields, _ = batch.evaluate_fields([[0.31, 0.09]])
+    row = res.rows[0]
+    assert row.result.status.name == "Converged" == str(g["status"])
+    assert rel(row.result.predictions, g["predictions"]) < RTOL_CONV
+    assert rel(fields[0, 0], g["Ux"]) < RTOL_CONV
+
+
+def test_batch_rows_independent_of_composition(rq):
+    case = cases.small_channel()
+    batch = cases.product_batch(rq, case)
+    thetas = np.array([[0.31, 0.09], [0.29, 0.085], [0.33, 0.095], [0.9, 0.09], [0.31, 0.09]])
+    full = batch.evaluate(thetas)
+    alone = batch.evaluate(thetas[1:2])
+    rev = batch.evaluate(thetas[::-1])
+    assert full.rows[3].result.status.name == "InvalidParameters"
+    assert np.all(np.isnan(full.rows[3].result.predictions))
+    assert full.rows[3].result.log_lik == -1e30
+    np.testing.assert_array_equal(full.rows[1].result.predictions, alone.rows[0].result.predictions)
+    np.testing.assert_array_equal(full.rows[0].result.predictions, full.rows[4].result.predictions)
+    np.testing.assert_array_equal(full.rows[2].result.predictions, rev.rows[2].result.predictions)
+    assert full.rows[1].result.simple_iters == alone.rows[0].result.simple_iters
+
+
+def test_multi_class_launch_equals_separate(rq):
+    a = cases.product_batch(rq, cases.small_channel())
+    b = cases.product_batch(rq, cases.small_channel(ny=32, re_tau=250.0, nu=1 / 250.0))
+    theta = np.array([[0.31, 0.09], [0.30, 0.088], [0.31, 0.09]])
+    multi = rq.evaluate_multi([a, b], [0, 1, 1], theta)
+    sa = a.evaluate(theta[:1])
+    sb = b.evaluate(theta[1:])
+    np.testing.assert_array_equal(multi.rows[0].result.predictions, sa.rows[0].result.predictions)
+    np.testing.assert_array_equal(multi.rows[1].result.predictions, sb.rows[0].result.predictions)
+    np.testing.assert_array_equal(multi.rows[2].result.predictions, sb.rows[1].result.predictions)
