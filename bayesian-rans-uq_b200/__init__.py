@@ -7,12 +7,14 @@ from . import _native
 from .core import (EvaluationResult, EvaluationStatus, FlowBoundaryConditions, ForwardBatch,
                    ForwardBatchResult, ForwardBatchRow, ForwardEvaluationResult, ForwardModel,
                    InferenceParameterSet, Mesh, ObservationOperator, SST_DEFAULTS, SST_NAMES,
-                   SolverSettings, Vec3, evaluate_multi)
+                   SolverSettings, Vec3, evaluate_multi, evaluate_multi_device,
+                   rows_from_device_bytes)
 
 __all__ = ["EvaluationResult", "EvaluationStatus", "FlowBoundaryConditions", "ForwardBatch",
            "ForwardBatchResult", "ForwardBatchRow", "ForwardEvaluationResult", "ForwardModel",
            "InferenceParameterSet", "Mesh", "ObservationOperator", "SST_DEFAULTS", "SST_NAMES",
-           "SolverSettings", "Vec3", "evaluate_multi", "lib"]
+           "SolverSettings", "Vec3", "evaluate_multi", "evaluate_multi_device",
+           "rows_from_device_bytes", "lib"]
 
 
 def lib():

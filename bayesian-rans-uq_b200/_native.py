@@ -80,8 +80,8 @@ SIGNATURES = {
     "rq_evaluate_multi": ([C.POINTER(C.c_void_p), C.c_int32, IP, DP, C.c_int32, C.c_int64,
                            C.POINTER(RowOut), DP, C.c_int32], C.c_int),
     "rq_evaluate_multi_device": ([C.POINTER(C.c_void_p), C.c_int32, IP, C.c_void_p, C.c_int32,
-                                  C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p],
-                                 C.c_int),
+                                  C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                  C.c_void_p], C.c_int),
     "rq_solve": ([C.c_void_p, DP, C.POINTER(RowOut), DP, DP, DP, C.c_int32], C.c_int),
     "rq_mesh_geometry": ([C.POINTER(MeshDesc), IP, DP], C.c_int),
     "rq_linear_solve": ([C.POINTER(Ldu), DP, C.c_int32, C.c_double, C.c_int32,

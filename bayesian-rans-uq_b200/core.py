@@ -512,6 +512,32 @@ def evaluate_multi(batches, problem_of_row, theta) -> ForwardBatchResult:
     return ForwardBatchResult(rows, no)
 
 
+def evaluate_multi_device(batches, problem_of_row, theta_dev, rows_dev, pred_dev, stream=0,
+                          clock_dev=None) -> None:
+    """Device-resident form of evaluate_multi (rq_evaluate_multi_device): theta_dev
+    (n x max n_active doubles), rows_dev (n x 48-byte rq_row_out), pred_dev
+    (n x max n_obs doubles) and clock_dev (n x 2 int64 ns, optional) are device
+    pointers (ints); the launch is queued on `stream` and not waited for."""
+    nb = len(batches)
+    handles = (C.c_void_p * nb)(*[b._problem.handle.value for b in batches])
+    pr = np.ascontiguousarray(np.asarray(problem_of_row, dtype=np.int32))
+    n = len(pr)
+    stride_t = max(b.n_parameters() for b in batches)
+    no = max(max(b.n_observations() for b in batches), 1)
+    N.call("rq_evaluate_multi_device", handles, C.c_int32(nb), N.iptr(pr), C.c_void_p(theta_dev),
+           C.c_int32(stride_t), C.c_int64(n), C.c_void_p(rows_dev), C.c_void_p(pred_dev),
+           C.c_int32(no), C.c_void_p(stream), C.c_void_p(clock_dev or 0))
+
+
+def rows_from_device_bytes(raw: np.ndarray) -> list:
+    """Decode n x rq_row_out records copied back from the device."""
+    rec = np.frombuffer(raw.tobytes(), dtype=np.dtype([("status", "<i4"), ("iterations", "<i4"),
+                                                       ("stalled", "<i4"), ("converged", "<i4"),
+                                                       ("loglik", "<f8"), ("final_worst", "<f8"),
+                                                       ("contraction_rate", "<f8")]))
+    return rec
+
+
 @dataclass
 class ForwardEvaluationResult:
     result: EvaluationResult

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -95,8 +96,9 @@ struct rq_problem {
     double base[11];
     int32_t nObs = 0;
     int block = 256;
+    int arenaKb = 0; // shared-memory arena per CTA, 0 = automatic
     // launch scratch, reused across calls
-    DevBuf dWs, dJobs, dRows, dPred, dFields, dHist, dTheta, dCounter;
+    DevBuf dWs, dJobs, dRows, dPred, dFields, dHist, dTheta, dCounter, dClock;
     std::mutex mu;
 };
 
@@ -322,6 +324,13 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     }
     C.amgVals = valOff;
     C.amgVecs = vecOff;
+    C.nActive = static_cast<int32_t>(P.active.size());
+    for (int a = 0; a < 11; ++a) {
+        C.active[a] = a < C.nActive ? P.active[a] : 0;
+        C.base[a] = P.base[a];
+        C.lo[a] = kLower[a];
+        C.hi[a] = kUpper[a];
+    }
     const long n = m.n, nf = m.n + m.nfy(), mc = h.coarseN();
     C.wsDoubles = 46 * pad32(n) + 4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
     // upload and patch pointers
@@ -343,59 +352,95 @@ int defaultBlock(int n) {
     return 512;
 }
 
-// Unpack theta -> 11 coefficients with the reference's admission
-// (InferenceParameterSet::inBounds / unpack, InferenceParameters.hpp:67-77, 127-140).
-bool unpackRow(const rq_problem &P, const double *theta, double out[11]) {
-    for (int i = 0; i < 11; ++i)
-        out[i] = P.base[i];
-    for (size_t a = 0; a < P.active.size(); ++a) {
-        const int idx = P.active[a];
-        const double v = theta[a];
-        if (v < kLower[idx] || v > kUpper[idx] || std::isnan(v) || std::isinf(v))
-            return false;
-        out[idx] = v;
-    }
-    return true;
+int maxSmemOptin() {
+    int dev = 0, v = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attribute");
+    return v;
 }
 
-struct Launch {
-    std::vector<rq::DevJob> jobs;
-    std::vector<int64_t> rowOf; // job -> output row
-};
-
-// Runs jobs (already filled except output pointers) for rows that were admitted.
-void runJobs(rq_problem &owner, std::vector<rq::DevJob> &jobs, const std::vector<const rq_problem *> &probOfJob,
-             rq::RowOut *dRows, double *dPred, int predStride, double *dFields, long fieldStride,
-             double *dHist, int histCap, cudaStream_t stream) {
-    const int nj = static_cast<int>(jobs.size());
-    if (nj == 0)
-        return;
-    int block = 64;
-    long wsStride = 0;
-    for (const auto *p : probOfJob) {
-        block = std::max(block, p->block);
-        wsStride = std::max(wsStride, static_cast<long>(p->cls.wsDoubles));
+// Shared-memory arena for a launch: the whole per-solve workspace when it
+// fits beside another CTA on the SM (two CTAs per SM for the small classes),
+// else as much as one CTA per SM can hold; the hottest arrays are placed first.
+int chooseArena(const std::vector<const rq_problem *> &probs) {
+    long ws = 0;
+    int knob = 0;
+    int nmax = 0;
+    for (const auto *p : probs) {
+        ws = std::max(ws, static_cast<long>(p->cls.wsDoubles));
+        knob = std::max(knob, p->arenaKb);
+        nmax = std::max(nmax, p->mesh.n);
     }
+    const long shared = static_cast<long>(rq::solveSharedBytes());
+    const long optin = maxSmemOptin();
+    long bytes;
+    if (knob > 0)
+        bytes = std::min<long>(knob * 1024L, optin - shared);
+    else if (nmax <= 768)
+        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
+    else
+        bytes = optin - shared;
+    bytes = std::max<long>(0, std::min(bytes, ws * 8));
+    return static_cast<int>(bytes / 8 / 32 * 32);
+}
+
+// Launches one persistent solve over rows whose problems are probOfRow[r];
+// theta rows live on the device at thetaDev + r * thetaStride. Output buffers
+// are device pointers indexed by row.
+void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOfRow,
+                const double *thetaDev, int thetaStride, rq::RowOut *rowsDev, double *predDev,
+                int predStride, double *fieldsDev, long fieldStride, double *histDev, int histCap,
+                long long *clockDev, cudaStream_t stream) {
+    const int n = static_cast<int>(probOfRow.size());
+    if (n == 0)
+        return;
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    // longest solves first (cells as the cost proxy); results do not depend on order
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return probOfRow[a]->mesh.n > probOfRow[b]->mesh.n;
+    });
+    std::vector<rq::DevJob> jobs(n);
+    int block = 32;
+    long wsStride = 0;
+    for (int k = 0; k < n; ++k) {
+        const int r = order[k];
+        const rq_problem &P = *probOfRow[r];
+        rq::DevJob &j = jobs[k];
+        j.cls = P.dCls.as<rq::DevClass>();
+        j.theta = thetaDev + static_cast<long>(r) * thetaStride;
+        j.row = rowsDev + r;
+        j.pred = predDev + static_cast<long>(r) * predStride;
+        j.fields = fieldsDev ? fieldsDev + static_cast<long>(r) * fieldStride : nullptr;
+        j.hist = histDev ? histDev + static_cast<long>(r) * histCap * 11 : nullptr;
+        j.histCap = histCap;
+        j.clock = clockDev ? clockDev + 12L * r : nullptr;
+        block = std::max(block, P.block);
+        wsStride = std::max(wsStride, static_cast<long>(P.cls.wsDoubles));
+    }
+    block = rq::normalizeBlock(block);
+    const int arena = chooseArena(probOfRow);
     int dev = 0, sms = 1;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    const int perSM = rq::solveBlocksPerSM(block);
-    const int grid = std::max(1, std::min(nj, sms * perSM));
-    for (int j = 0; j < nj; ++j) {
-        jobs[j].row = dRows + j;
-        jobs[j].pred = dPred + static_cast<long>(j) * predStride;
-        jobs[j].fields = dFields ? dFields + static_cast<long>(j) * fieldStride : nullptr;
-        jobs[j].hist = dHist ? dHist + static_cast<long>(j) * histCap * 11 : nullptr;
-        jobs[j].histCap = histCap;
-    }
-    owner.dJobs.ensure(sizeof(rq::DevJob) * nj);
+    const int perSM = rq::solveBlocksPerSM(block, arena);
+    if (perSM < 1)
+        throw RqError(RQ_E_CUDA, "solve kernel does not fit on an SM with this arena");
+    const int grid = std::max(1, std::min(n, sms * perSM));
+    owner.dJobs.ensure(sizeof(rq::DevJob) * n);
     owner.dWs.ensure(sizeof(double) * wsStride * grid);
     owner.dCounter.ensure(sizeof(int));
-    check(cudaMemcpyAsync(owner.dJobs.p, jobs.data(), sizeof(rq::DevJob) * nj, cudaMemcpyHostToDevice, stream), "jobs");
+    check(cudaMemcpyAsync(owner.dJobs.p, jobs.data(), sizeof(rq::DevJob) * n,
+                          cudaMemcpyHostToDevice, stream), "jobs");
     check(cudaMemsetAsync(owner.dCounter.p, 0, sizeof(int), stream), "counter");
-    check(rq::launchSolve(owner.dJobs.as<rq::DevJob>(), nj, owner.dCounter.as<int>(),
-                          owner.dWs.as<double>(), wsStride, grid, block, stream),
+    check(rq::launchSolve(owner.dJobs.as<rq::DevJob>(), n, owner.dCounter.as<int>(),
+                          owner.dWs.as<double>(), wsStride, grid, block, arena, stream),
           "solve launch");
+}
+
+rq_row_out toRow(const rq::RowOut &o) {
+    return rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik, o.finalWorst,
+                      o.contractionRate};
 }
 
 } // namespace
@@ -522,150 +567,109 @@ int rq_evaluate_multi(rq_problem *const *problems, int32_t n_problems,
         }
         if (theta_stride < maxActive || pred_stride < std::max(maxObs, 1))
             throw std::invalid_argument("theta/prediction stride below the problems' widths");
+        std::vector<const rq_problem *> probOfRow(n);
+        for (int64_t r = 0; r < n; ++r) {
+            if (problem_of_row[r] < 0 || problem_of_row[r] >= n_problems)
+                throw std::invalid_argument("problem index out of range");
+            probOfRow[r] = problems[problem_of_row[r]];
+        }
         rq_problem &owner = *problems[0];
         std::lock_guard<std::mutex> lock(owner.mu);
-        std::vector<rq::DevJob> jobs;
-        std::vector<const rq_problem *> probOfJob;
-        std::vector<int64_t> rowOfJob;
+        owner.dTheta.ensure(sizeof(double) * n * theta_stride);
+        owner.dRows.ensure(sizeof(rq::RowOut) * n);
+        owner.dPred.ensure(sizeof(double) * n * pred_stride);
+        check(cudaMemcpy(owner.dTheta.p, theta, sizeof(double) * n * theta_stride,
+                         cudaMemcpyHostToDevice), "theta");
+        launchRows(owner, probOfRow, owner.dTheta.as<double>(), theta_stride,
+                   owner.dRows.as<rq::RowOut>(), owner.dPred.as<double>(), pred_stride, nullptr, 0,
+                   nullptr, 0, nullptr, nullptr);
+        std::vector<rq::RowOut> hr(n);
+        std::vector<double> hp(static_cast<size_t>(n) * pred_stride);
+        check(cudaMemcpy(hr.data(), owner.dRows.p, sizeof(rq::RowOut) * n, cudaMemcpyDeviceToHost), "rows");
+        check(cudaMemcpy(hp.data(), owner.dPred.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost), "predictions");
         const double nan = std::nan("");
         for (int64_t r = 0; r < n; ++r) {
-            const int pi = problem_of_row[r];
-            if (pi < 0 || pi >= n_problems)
-                throw std::invalid_argument("problem index out of range");
-            const rq_problem &P = *problems[pi];
-            double coeffs[11];
+            rows[r] = toRow(hr[r]);
+            const int no = probOfRow[r]->nObs;
             for (int t = 0; t < pred_stride; ++t)
-                predictions[r * pred_stride + t] = nan;
-            if (!unpackRow(P, theta + r * theta_stride, coeffs)) {
-                rows[r] = rq_row_out{RQ_INVALID_PARAMETERS, 0, 0, 0, -1e30, nan, nan};
-                continue;
-            }
-            rq::DevJob j{};
-            j.cls = P.dCls.as<rq::DevClass>();
-            std::memcpy(j.coeffs, coeffs, sizeof(coeffs));
-            jobs.push_back(j);
-            probOfJob.push_back(&P);
-            rowOfJob.push_back(r);
+                predictions[r * pred_stride + t] = t < no ? hp[r * pred_stride + t] : nan;
         }
-        // longest solves first (cells as the cost proxy); results do not depend on order
-        std::vector<int> order(jobs.size());
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-            return probOfJob[a]->mesh.n > probOfJob[b]->mesh.n;
-        });
-        std::vector<rq::DevJob> sj;
-        std::vector<const rq_problem *> sp;
-        std::vector<int64_t> sr;
-        for (int k : order) {
-            sj.push_back(jobs[k]);
-            sp.push_back(probOfJob[k]);
-            sr.push_back(rowOfJob[k]);
+    });
+}
+
+int rq_evaluate_multi_device(rq_problem *const *problems, int32_t n_problems,
+                             const int32_t *problem_of_row_host, const double *theta_dev,
+                             int32_t theta_stride, int64_t n, rq_row_out *rows_dev,
+                             double *predictions_dev, int32_t pred_stride, void *stream,
+                             int64_t *clock_ns_dev) {
+    return guarded([&] {
+        if (!problems || n_problems < 1 || (n > 0 && (!problem_of_row_host || !theta_dev || !rows_dev || !predictions_dev)))
+            throw std::invalid_argument("null argument");
+        if (n < 0)
+            throw std::invalid_argument("negative row count");
+        int maxActive = 0, maxObs = 0;
+        for (int i = 0; i < n_problems; ++i) {
+            if (!problems[i])
+                throw std::invalid_argument("null problem");
+            maxActive = std::max<int>(maxActive, static_cast<int>(problems[i]->active.size()));
+            maxObs = std::max(maxObs, problems[i]->nObs);
         }
-        const int nj = static_cast<int>(sj.size());
-        if (nj == 0)
-            return;
-        owner.dRows.ensure(sizeof(rq::RowOut) * nj);
-        owner.dPred.ensure(sizeof(double) * nj * pred_stride);
-        runJobs(owner, sj, sp, owner.dRows.as<rq::RowOut>(), owner.dPred.as<double>(), pred_stride,
-                nullptr, 0, nullptr, 0, nullptr);
-        std::vector<rq::RowOut> hr(nj);
-        std::vector<double> hp(static_cast<size_t>(nj) * pred_stride);
-        check(cudaMemcpy(hr.data(), owner.dRows.p, sizeof(rq::RowOut) * nj, cudaMemcpyDeviceToHost), "rows");
-        check(cudaMemcpy(hp.data(), owner.dPred.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost), "predictions");
-        for (int k = 0; k < nj; ++k) {
-            const int64_t r = sr[k];
-            const rq::RowOut &o = hr[k];
-            rows[r] = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik,
-                                 o.finalWorst, o.contractionRate};
-            const int no = sp[k]->nObs;
-            for (int t = 0; t < no; ++t)
-                predictions[r * pred_stride + t] = hp[static_cast<size_t>(k) * pred_stride + t];
+        if (theta_stride < maxActive || pred_stride < std::max(maxObs, 1))
+            throw std::invalid_argument("theta/prediction stride below the problems' widths");
+        static_assert(sizeof(rq::RowOut) == sizeof(rq_row_out), "row layout");
+        std::vector<const rq_problem *> probOfRow(n);
+        for (int64_t r = 0; r < n; ++r) {
+            if (problem_of_row_host[r] < 0 || problem_of_row_host[r] >= n_problems)
+                throw std::invalid_argument("problem index out of range");
+            probOfRow[r] = problems[problem_of_row_host[r]];
         }
+        rq_problem &owner = *problems[0];
+        std::lock_guard<std::mutex> lock(owner.mu);
+        launchRows(owner, probOfRow, theta_dev, theta_stride,
+                   reinterpret_cast<rq::RowOut *>(rows_dev), predictions_dev, pred_stride, nullptr,
+                   0, nullptr, 0, reinterpret_cast<long long *>(clock_ns_dev),
+                   static_cast<cudaStream_t>(stream));
     });
 }
 
 int rq_evaluate_batch(rq_problem *p, const double *theta, int64_t n, rq_row_out *rows,
                       double *predictions, double *fields, double *history, int32_t hist_cap) {
-    if (!fields && !history) {
-        std::vector<int32_t> pr(static_cast<size_t>(std::max<int64_t>(n, 0)), 0);
-        rq_problem *ps[1] = {p};
-        const int na = p ? static_cast<int>(p->active.size()) : 0;
-        const int no = p ? std::max(p->nObs, 1) : 1;
-        if (p && p->nObs == 0) { // predictions buffer has zero width: use scratch
-            std::vector<double> scratch(static_cast<size_t>(std::max<int64_t>(n, 0)));
-            return rq_evaluate_multi(ps, 1, pr.data(), theta, na, n, rows, scratch.data(), 1);
-        }
-        return rq_evaluate_multi(ps, 1, pr.data(), theta, na, n, rows, predictions, no);
-    }
     return guarded([&] {
         if (!p || (n > 0 && (!theta || !rows)))
             throw std::invalid_argument("null argument");
         if (n < 0 || hist_cap < 0)
             throw std::invalid_argument("negative size");
-        std::lock_guard<std::mutex> lock(p->mu);
-        const double nan = std::nan("");
-        const int no = std::max(p->nObs, 1), nc = p->mesh.n;
-        std::vector<rq::DevJob> jobs;
-        std::vector<const rq_problem *> probs;
-        std::vector<int64_t> rowOf;
-        for (int64_t r = 0; r < n; ++r) {
-            double coeffs[11];
-            if (!unpackRow(*p, theta + r * p->active.size(), coeffs)) {
-                rows[r] = rq_row_out{RQ_INVALID_PARAMETERS, 0, 0, 0, -1e30, nan, nan};
-                if (predictions)
-                    for (int t = 0; t < p->nObs; ++t)
-                        predictions[r * p->nObs + t] = nan;
-                if (fields)
-                    for (long e = 0; e < 11L * nc; ++e)
-                        fields[r * 11L * nc + e] = nan;
-                continue;
-            }
-            rq::DevJob j{};
-            j.cls = p->dCls.as<rq::DevClass>();
-            std::memcpy(j.coeffs, coeffs, sizeof(coeffs));
-            jobs.push_back(j);
-            probs.push_back(p);
-            rowOf.push_back(r);
-        }
-        const int nj = static_cast<int>(jobs.size());
-        if (nj == 0)
+        if (n == 0)
             return;
-        p->dRows.ensure(sizeof(rq::RowOut) * nj);
-        p->dPred.ensure(sizeof(double) * nj * no);
+        std::lock_guard<std::mutex> lock(p->mu);
+        const int na = static_cast<int>(p->active.size());
+        const int no = std::max(p->nObs, 1), nc = p->mesh.n;
+        std::vector<const rq_problem *> probOfRow(n, p);
+        p->dTheta.ensure(sizeof(double) * n * na);
+        p->dRows.ensure(sizeof(rq::RowOut) * n);
+        p->dPred.ensure(sizeof(double) * n * no);
         if (fields)
-            p->dFields.ensure(sizeof(double) * nj * 11L * nc);
-        if (history && hist_cap > 0)
-            p->dHist.ensure(sizeof(double) * nj * 11L * hist_cap);
-        runJobs(*p, jobs, probs, p->dRows.as<rq::RowOut>(), p->dPred.as<double>(), no,
-                fields ? p->dFields.as<double>() : nullptr, 11L * nc,
-                (history && hist_cap > 0) ? p->dHist.as<double>() : nullptr, hist_cap, nullptr);
-        std::vector<rq::RowOut> hr(nj);
-        std::vector<double> hp(static_cast<size_t>(nj) * no);
-        check(cudaMemcpy(hr.data(), p->dRows.p, sizeof(rq::RowOut) * nj, cudaMemcpyDeviceToHost), "rows");
+            p->dFields.ensure(sizeof(double) * n * 11L * nc);
+        const bool wantHist = history && hist_cap > 0;
+        if (wantHist)
+            p->dHist.ensure(sizeof(double) * n * 11L * hist_cap);
+        check(cudaMemcpy(p->dTheta.p, theta, sizeof(double) * n * na, cudaMemcpyHostToDevice), "theta");
+        launchRows(*p, probOfRow, p->dTheta.as<double>(), na, p->dRows.as<rq::RowOut>(),
+                   p->dPred.as<double>(), no, fields ? p->dFields.as<double>() : nullptr, 11L * nc,
+                   wantHist ? p->dHist.as<double>() : nullptr, hist_cap, nullptr, nullptr);
+        std::vector<rq::RowOut> hr(n);
+        std::vector<double> hp(static_cast<size_t>(n) * no);
+        check(cudaMemcpy(hr.data(), p->dRows.p, sizeof(rq::RowOut) * n, cudaMemcpyDeviceToHost), "rows");
         check(cudaMemcpy(hp.data(), p->dPred.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost), "predictions");
-        std::vector<double> hf, hh;
-        if (fields) {
-            hf.resize(static_cast<size_t>(nj) * 11 * nc);
-            check(cudaMemcpy(hf.data(), p->dFields.p, sizeof(double) * hf.size(), cudaMemcpyDeviceToHost), "fields");
-        }
-        if (history && hist_cap > 0) {
-            hh.resize(static_cast<size_t>(nj) * 11 * hist_cap);
-            check(cudaMemcpy(hh.data(), p->dHist.p, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost), "history");
-        }
-        for (int k = 0; k < nj; ++k) {
-            const int64_t r = rowOf[k];
-            const rq::RowOut &o = hr[k];
-            rows[r] = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik,
-                                 o.finalWorst, o.contractionRate};
+        if (fields)
+            check(cudaMemcpy(fields, p->dFields.p, sizeof(double) * n * 11L * nc, cudaMemcpyDeviceToHost), "fields");
+        if (wantHist)
+            check(cudaMemcpy(history, p->dHist.p, sizeof(double) * n * 11L * hist_cap, cudaMemcpyDeviceToHost), "history");
+        for (int64_t r = 0; r < n; ++r) {
+            rows[r] = toRow(hr[r]);
             if (predictions)
                 for (int t = 0; t < p->nObs; ++t)
-                    predictions[r * p->nObs + t] = hp[static_cast<size_t>(k) * no + t];
-            if (fields)
-                std::memcpy(fields + r * 11L * nc, hf.data() + static_cast<size_t>(k) * 11 * nc,
-                            sizeof(double) * 11 * nc);
-            if (history && hist_cap > 0)
-                std::memcpy(history + r * 11L * hist_cap, hh.data() + static_cast<size_t>(k) * 11 * hist_cap,
-                            sizeof(double) * 11 * hist_cap);
+                    predictions[r * p->nObs + t] = hp[r * no + t];
         }
     });
 }
@@ -680,30 +684,62 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
                 throw std::invalid_argument("SST coefficients must be finite and nonnegative");
         if (coeffs[2] == 0 || coeffs[8] == 0)
             throw std::invalid_argument("SST beta1 and betaStar must be positive");
+        // a one-off problem view whose parameter set activates all eleven coefficients
         std::lock_guard<std::mutex> lock(p->mu);
+        rq::DevClass all = p->cls;
+        all.nActive = 11;
+        for (int a = 0; a < 11; ++a) {
+            all.active[a] = a;
+            all.lo[a] = -std::numeric_limits<double>::infinity();
+            all.hi[a] = std::numeric_limits<double>::infinity();
+        }
+        DevBuf dAll;
+        dAll.ensure(sizeof(rq::DevClass));
+        check(cudaMemcpy(dAll.p, &all, sizeof(all), cudaMemcpyHostToDevice), "class");
         const int no = std::max(p->nObs, 1), nc = p->mesh.n;
-        std::vector<rq::DevJob> jobs(1);
-        jobs[0].cls = p->dCls.as<rq::DevClass>();
-        std::memcpy(jobs[0].coeffs, coeffs, sizeof(double) * 11);
-        std::vector<const rq_problem *> probs{p};
+        p->dTheta.ensure(sizeof(double) * 11);
         p->dRows.ensure(sizeof(rq::RowOut));
         p->dPred.ensure(sizeof(double) * no);
         if (fields)
             p->dFields.ensure(sizeof(double) * 11L * nc);
-        if (history && hist_cap > 0)
+        const bool wantHist = history && hist_cap > 0;
+        if (wantHist)
             p->dHist.ensure(sizeof(double) * 11L * hist_cap);
-        runJobs(*p, jobs, probs, p->dRows.as<rq::RowOut>(), p->dPred.as<double>(), no,
-                fields ? p->dFields.as<double>() : nullptr, 11L * nc,
-                (history && hist_cap > 0) ? p->dHist.as<double>() : nullptr, hist_cap, nullptr);
+        check(cudaMemcpy(p->dTheta.p, coeffs, sizeof(double) * 11, cudaMemcpyHostToDevice), "coeffs");
+        std::vector<const rq_problem *> probOfRow{p};
+        rq::DevClass saved = p->cls;
+        // launchRows reads the device class pointer of the problem: point it at the view
+        rq_problem view;
+        (void)view;
+        std::vector<rq::DevJob> jobs(1);
+        rq::DevJob &j = jobs[0];
+        j.cls = dAll.as<rq::DevClass>();
+        j.theta = p->dTheta.as<double>();
+        j.row = p->dRows.as<rq::RowOut>();
+        j.pred = p->dPred.as<double>();
+        j.fields = fields ? p->dFields.as<double>() : nullptr;
+        j.hist = wantHist ? p->dHist.as<double>() : nullptr;
+        j.histCap = hist_cap;
+        j.clock = nullptr;
+        (void)saved;
+        const int block = rq::normalizeBlock(p->block);
+        const int arena = chooseArena(probOfRow);
+        p->dJobs.ensure(sizeof(rq::DevJob));
+        p->dWs.ensure(sizeof(double) * p->cls.wsDoubles);
+        p->dCounter.ensure(sizeof(int));
+        check(cudaMemcpy(p->dJobs.p, jobs.data(), sizeof(rq::DevJob), cudaMemcpyHostToDevice), "jobs");
+        check(cudaMemset(p->dCounter.p, 0, sizeof(int)), "counter");
+        check(rq::launchSolve(p->dJobs.as<rq::DevJob>(), 1, p->dCounter.as<int>(),
+                              p->dWs.as<double>(), p->cls.wsDoubles, 1, block, arena, nullptr),
+              "solve launch");
         rq::RowOut o;
         check(cudaMemcpy(&o, p->dRows.p, sizeof(o), cudaMemcpyDeviceToHost), "row");
-        *row = rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik, o.finalWorst,
-                          o.contractionRate};
+        *row = toRow(o);
         if (predictions && p->nObs > 0)
             check(cudaMemcpy(predictions, p->dPred.p, sizeof(double) * p->nObs, cudaMemcpyDeviceToHost), "predictions");
         if (fields)
             check(cudaMemcpy(fields, p->dFields.p, sizeof(double) * 11 * nc, cudaMemcpyDeviceToHost), "fields");
-        if (history && hist_cap > 0)
+        if (wantHist)
             check(cudaMemcpy(history, p->dHist.p, sizeof(double) * 11 * hist_cap, cudaMemcpyDeviceToHost), "history");
     });
 }
@@ -722,12 +758,6 @@ int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells) 
                 cells[4 * c + 3] = m.wd[c];
             }
     });
-}
-
-int rq_evaluate_multi_device(rq_problem *const *, int32_t, const int32_t *, const double *, int32_t,
-                             int64_t, rq_row_out *, double *, int32_t, void *) {
-    g_error = "rq_evaluate_multi_device is not available in this build";
-    return RQ_E_UNSUPPORTED;
 }
 
 int rq_linear_solve(const rq_ldu *, double *, int32_t, double, int32_t, rq_solver_result *) {

@@ -57,6 +57,11 @@ struct DevClass {
     DevAmgLevel lev[kMaxLevels];
     int32_t amgVals, amgVecs;  // per-solve doubles for coarse values / vectors
     int64_t wsDoubles;         // per-solve workspace
+    // InferenceParameterSet: active indices, the coefficients filling the rest,
+    // and the admission bounds (core/include/InferenceParameters.hpp:67-77, 127-165)
+    int32_t nActive, pad2;
+    int32_t active[11], pad3;
+    double base[11], lo[11], hi[11];
 };
 
 // Outcome of one draw; the status values and order follow EvaluationStatus
@@ -68,11 +73,13 @@ struct RowOut {
 
 struct DevJob {
     const DevClass *cls;
-    double coeffs[11];
+    const double *theta; // nActive values of this draw (device)
     RowOut *row;
     double *pred;      // nobs
     double *fields;    // optional 11 x n
     double *hist;      // optional hist_cap x 11
+    long long *clock;  // optional, 12 per row: global-timer ns at start and end, inner
+                       // Krylov iterations, inner pressure iterations, 8 stage cycle counts
     int32_t histCap;
     int32_t pad;
 };

@@ -9,9 +9,11 @@ namespace rq {
 size_t solveSharedBytes();
 // Persistent CTAs: each pulls job indices from *nextJob (zeroed by the caller)
 // until njobs are taken; ws is grid x wsStride doubles of per-CTA workspace.
+// arenaDoubles: shared-memory arena per CTA for the hot arrays (0 = all global).
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
-                        int grid, int block, cudaStream_t stream);
-// CTAs of `block` threads that fit on one SM at once.
-int solveBlocksPerSM(int block);
+                        int grid, int block, int arenaDoubles, cudaStream_t stream);
+// CTAs of `block` threads with the given arena that fit on one SM at once (0: does not fit).
+int solveBlocksPerSM(int block, int arenaDoubles);
+int normalizeBlock(int block);
 
 } // namespace rq

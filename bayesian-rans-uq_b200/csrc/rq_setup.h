@@ -57,7 +57,9 @@ struct AmgHost {
     int coarseN() const { return lev.back().n; }
     size_t coarseNnz() const { return lev.size() > 1 ? lev.back().col.size() : 0; }
 };
-AmgHost buildAmg(const StructMesh &m, int minCoarse = 50, int maxLevels = 20);
+// Coarsening stops at <= 32 rows (the reference stops at 50) so that one warp
+// inverts the coarsest level.
+AmgHost buildAmg(const StructMesh &m, int minCoarse = 32, int maxLevels = 20);
 
 // Velocity/pressure probe (PreparedObservation, core/include/ObservationOperator.hpp:630-670).
 struct ProbeHost {

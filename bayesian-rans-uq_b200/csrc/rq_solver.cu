@@ -51,19 +51,39 @@ struct Shared {
     double q[kMaxProbes], qPrev[kMaxProbes];
     int haveQPrev;
     int job;
+    int admitted;
+    long long innerKrylov, innerPressure; // inner iterations of the solve (work accounting)
+    long long stage[8];                   // clock64 cycles per stage (thread 0)
+    long long tmark;
+    double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
 };
+
+// stage timers, as the reference's momentum / pressure / turbulence timers
+// (rans-uq/include/SIMPLESolver.hpp:293-305): 0 set-up, 1 closure, 2 momentum,
+// 3 pressure assembly, 4 pressure solve, 5 AMG refresh, 6 turbulence, 7 bookkeeping
+__device__ __forceinline__ void mark(Shared &S, int k) {
+    if (threadIdx.x == 0) {
+        const long long t = clock64();
+        S.stage[k] += t - S.tmark;
+        S.tmark = t;
+    }
+}
 
 // ---------------------------------------------------------------- reductions
 template <int K> struct Red {
     double v[K];
 };
 
+// Block reductions. Each warp tree-reduces its lanes (lane 0 holds the sum),
+// lane 0 parks it in shared memory, and after one barrier EVERY warp
+// tree-reduces the same partials in the same order and broadcasts lane 0's
+// result -- so all threads of the CTA hold bit-identical values and branch alike.
 template <int K>
 __device__ __forceinline__ void blockSum(double (&v)[K], Shared &S, int &rp) {
 #pragma unroll
     for (int k = 0; k < K; ++k)
         for (int o = 16; o > 0; o >>= 1)
-            v[k] += __shfl_xor_sync(FULL, v[k], o);
+            v[k] += __shfl_down_sync(FULL, v[k], o);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     if (lane == 0)
 #pragma unroll
@@ -72,10 +92,10 @@ __device__ __forceinline__ void blockSum(double (&v)[K], Shared &S, int &rp) {
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        double s = 0.0;
-        for (int w = 0; w < nw; ++w)
-            s += S.red[rp][k][w];
-        v[k] = s;
+        double s = lane < nw ? S.red[rp][k][lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+            s += __shfl_down_sync(FULL, s, o);
+        v[k] = __shfl_sync(FULL, s, 0);
     }
     rp ^= 1;
 }
@@ -94,9 +114,9 @@ __device__ __forceinline__ void blockMax(double (&v)[K], Shared &S, int &rp) {
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        double s = S.red[rp][k][0];
-        for (int w = 1; w < nw; ++w)
-            s = fmax(s, S.red[rp][k][w]);
+        double s = lane < nw ? S.red[rp][k][lane] : S.red[rp][k][0];
+        for (int o = 16; o > 0; o >>= 1)
+            s = fmax(s, __shfl_xor_sync(FULL, s, o));
         v[k] = s;
     }
     rp ^= 1;
@@ -116,8 +136,8 @@ struct Cell {
 __device__ __forceinline__ Cell cellOf(const DevClass &C, int c) {
     Cell q;
     q.c = c;
-    q.i = c % C.nx;
-    q.j = c / C.nx;
+    q.j = __float2int_rd((static_cast<float>(c) + 0.5f) * __frcp_rn(static_cast<float>(C.nx)));
+    q.i = c - q.j * C.nx;
     q.W = q.i == 0 ? c + C.nx - 1 : c - 1;
     q.E = q.i == C.nx - 1 ? c - C.nx + 1 : c + 1;
     q.south = q.j > 0;
@@ -168,37 +188,37 @@ __device__ __forceinline__ void ggCell(const DevClass &C, const Cell &q, const d
     const int c = q.c;
     const double pc = phi[c];
     // east (owner c)
-    const double wE = C.xw[c];
+    const double wE = __ldg(C.xw + (c));
     const double fE = pc * wE + phi[q.E] * (1.0 - wE);
-    const double sxE = C.xnx[c] * C.xa[c], syE = C.xny[c] * C.xa[c];
+    const double sxE = __ldg(C.xnx + (c)) * __ldg(C.xa + (c)), syE = __ldg(C.xny + (c)) * __ldg(C.xa + (c));
     // west (owner W, neighbour c)
-    const double wWf = C.xw[q.W];
+    const double wWf = __ldg(C.xw + (q.W));
     const double fW = phi[q.W] * wWf + pc * (1.0 - wWf);
-    const double sxW = C.xnx[q.W] * C.xa[q.W], syW = C.xny[q.W] * C.xa[q.W];
+    const double sxW = __ldg(C.xnx + (q.W)) * __ldg(C.xa + (q.W)), syW = __ldg(C.xny + (q.W)) * __ldg(C.xa + (q.W));
     // north: internal (owner c) or top wall (owner c)
     const int fn = c + C.nx;
     double fN;
     if (q.north) {
-        const double w = C.yw[fn];
+        const double w = __ldg(C.yw + (fn));
         fN = pc * w + phi[c + C.nx] * (1.0 - w);
     } else {
         fN = bN;
     }
-    const double sxN = C.ynx[fn] * C.ya[fn], syN = C.yny[fn] * C.ya[fn];
+    const double sxN = __ldg(C.ynx + (fn)) * __ldg(C.ya + (fn)), syN = __ldg(C.yny + (fn)) * __ldg(C.ya + (fn));
     // south: internal (owner c - nx, neighbour c) or bottom wall (owner c)
     const int fs = c;
     double fS;
     if (q.south) {
-        const double w = C.yw[fs];
+        const double w = __ldg(C.yw + (fs));
         fS = phi[c - C.nx] * w + pc * (1.0 - w);
     } else {
         fS = bS;
     }
-    const double sxS = C.ynx[fs] * C.ya[fs], syS = C.yny[fs] * C.ya[fs];
+    const double sxS = __ldg(C.ynx + (fs)) * __ldg(C.ya + (fs)), syS = __ldg(C.yny + (fs)) * __ldg(C.ya + (fs));
     const double sgnS = q.south ? -1.0 : 1.0;
     gx = order4(q, -(sxW * fW), sxE * fE, sgnS * (sxS * fS), sxN * fN);
     gy = order4(q, -(syW * fW), syE * fE, sgnS * (syS * fS), syN * fN);
-    const double V = C.vol[c];
+    const double V = __ldg(C.vol + (c));
     if (V > 1e-30) {
         gx = gx / V;
         gy = gy / V;
@@ -347,15 +367,65 @@ __device__ void amgRefresh(Shared &S) {
         const double *fv = W.amgVal + F.valOff;
         for (int e = threadIdx.x; e < Q.nnz; e += blockDim.x) {
             double s = 0.0;
-            for (int k = F.gPtr[e]; k < F.gPtr[e + 1]; ++k)
-                s += (l == 0) ? level0Entry(W, C.n, F.gSrc[k]) : fv[F.gSrc[k]];
+            for (int k = __ldg(F.gPtr + (e)); k < __ldg(F.gPtr + (e + 1)); ++k)
+                s += (l == 0) ? level0Entry(W, C.n, __ldg(F.gSrc + (k))) : fv[__ldg(F.gSrc + (k))];
             cv[e] = s;
         }
         __syncthreads();
     }
     const DevAmgLevel &Q = C.lev[L - 1];
-    const int m = Q.n, m2 = 2 * m;
+    const int m = Q.n;
     const double *qv = W.amgVal + Q.valOff;
+    if (m <= 32) {
+        // coarsest matrix into shared memory, then in-place Gauss-Jordan inversion by
+        // warp 0 (SPD: no pivoting); lane r owns row r
+        double *a = S.coarse;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x)
+            a[e] = 0.0;
+        __syncthreads();
+        if (L == 1) {
+            for (int r = threadIdx.x; r < m; r += blockDim.x) {
+                const Cell q = cellOf(C, r);
+                a[r * m + r] += W.d[r];
+                a[r * m + q.W] += W.aW[r];
+                a[r * m + q.E] += W.aE[r];
+                if (q.south)
+                    a[r * m + r - C.nx] += W.aS[r];
+                if (q.north)
+                    a[r * m + r + C.nx] += W.aN[r];
+            }
+        } else {
+            for (int r = threadIdx.x; r < m; r += blockDim.x)
+                for (int k = __ldg(Q.ptr + (r)); k < __ldg(Q.ptr + (r + 1)); ++k)
+                    a[r * m + __ldg(Q.col + (k))] = qv[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int r = threadIdx.x;
+            for (int k = 0; k < m; ++k) {
+                const double p = 1.0 / a[k * m + k];
+                const double f = (r < m) ? a[r * m + k] : 0.0;
+                __syncwarp();
+                if (r < m && r != k) {
+                    for (int j = 0; j < m; ++j)
+                        if (j != k)
+                            a[r * m + j] -= f * a[k * m + j] * p;
+                    a[r * m + k] = -f * p;
+                }
+                __syncwarp();
+                if (r == k) {
+                    for (int j = 0; j < m; ++j)
+                        if (j != k)
+                            a[k * m + j] *= p;
+                    a[k * m + k] = p;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    const int m2 = 2 * m;
     double *A0 = W.dense0, *A1 = W.dense1;
     for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
         A0[e] = ((e % m2) == m + e / m2) ? 1.0 : 0.0;
@@ -373,8 +443,8 @@ __device__ void amgRefresh(Shared &S) {
         }
     } else {
         for (int r = threadIdx.x; r < m; r += blockDim.x)
-            for (int k = Q.ptr[r]; k < Q.ptr[r + 1]; ++k)
-                A0[r * m2 + Q.col[k]] = qv[k];
+            for (int k = __ldg(Q.ptr + (r)); k < __ldg(Q.ptr + (r + 1)); ++k)
+                A0[r * m2 + __ldg(Q.col + (k))] = qv[k];
     }
     __syncthreads();
     for (int piv = 0; piv < m; ++piv) {
@@ -400,8 +470,8 @@ __device__ void amgRefresh(Shared &S) {
 __device__ __forceinline__ double csrRow(const DevAmgLevel &L, const double *val, const double *x,
                                          int i) {
     double s = 0.0;
-    for (int k = L.ptr[i]; k < L.ptr[i + 1]; ++k)
-        s += val[k] * x[L.col[k]];
+    for (int k = __ldg(L.ptr + (i)); k < __ldg(L.ptr + (i + 1)); ++k)
+        s += val[k] * x[__ldg(L.col + (k))];
     return s;
 }
 
@@ -439,11 +509,11 @@ __device__ double vcycle(Shared &S, int &rp) {
                 const DevAmgLevel &F = C.lev[l - 1];
                 const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
                 bi = 0.0;
-                for (int k = F.childPtr[i]; k < F.childPtr[i + 1]; ++k)
-                    bi += fr[F.childIdx[k]];
+                for (int k = __ldg(F.childPtr + (i)); k < __ldg(F.childPtr + (i + 1)); ++k)
+                    bi += fr[__ldg(F.childIdx + (k))];
                 b[i] = bi;
             }
-            const double di = (l == 0) ? W.d[i] : val[Lv.diagPos[i]];
+            const double di = (l == 0) ? W.d[i] : val[__ldg(Lv.diagPos + (i))];
             xa[i] = om * bi / di;
         }
         __syncthreads();
@@ -456,7 +526,7 @@ __device__ double vcycle(Shared &S, int &rp) {
                 di = W.d[i];
             } else {
                 ax = csrRow(Lv, val, xa, i);
-                di = val[Lv.diagPos[i]];
+                di = val[__ldg(Lv.diagPos + (i))];
             }
             xb[i] = xa[i] + om * (b[i] - ax) / di;
         }
@@ -488,15 +558,15 @@ __device__ double vcycle(Shared &S, int &rp) {
             const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
             for (int i = threadIdx.x; i < m; i += blockDim.x) {
                 double bi = 0.0;
-                for (int k = F.childPtr[i]; k < F.childPtr[i + 1]; ++k)
-                    bi += fr[F.childIdx[k]];
+                for (int k = __ldg(F.childPtr + (i)); k < __ldg(F.childPtr + (i + 1)); ++k)
+                    bi += fr[__ldg(F.childIdx + (k))];
                 b[i] = bi;
             }
         }
         __syncthreads();
         for (int i = threadIdx.x; i < m; i += blockDim.x) {
             double s = 0.0;
-            const double *row = W.dense0 + i * m2 + m;
+            const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
             for (int j = 0; j < m; ++j)
                 s += row[j] * b[j];
             xb[i] = s;
@@ -523,12 +593,12 @@ __device__ double vcycle(Shared &S, int &rp) {
         const double *val = W.amgVal + Lv.valOff;
         const int *agg = Lv.agg;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const double xi = xprev[i] + xc[agg[i]];
+            const double xi = xprev[i] + xc[__ldg(agg + (i))];
             double ax, di;
             if (l == 0) {
                 const Cell q = cellOf(C, i);
                 const int c = i;
-                auto X = [&](int jj) { return xprev[jj] + xc[agg[jj]]; };
+                auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + (jj))]; };
                 const double tW = W.aW[c] * X(q.W), tE = W.aE[c] * X(q.E);
                 const double tS = q.south ? W.aS[c] * X(c - nx) : 0.0;
                 const double tN = q.north ? W.aN[c] * X(c + nx) : 0.0;
@@ -536,11 +606,11 @@ __device__ double vcycle(Shared &S, int &rp) {
                 di = W.d[c];
             } else {
                 ax = 0.0;
-                for (int k = Lv.ptr[i]; k < Lv.ptr[i + 1]; ++k) {
-                    const int jj = Lv.col[k];
-                    ax += val[k] * (xprev[jj] + xc[agg[jj]]);
+                for (int k = __ldg(Lv.ptr + (i)); k < __ldg(Lv.ptr + (i + 1)); ++k) {
+                    const int jj = __ldg(Lv.col + (k));
+                    ax += val[k] * (xprev[jj] + xc[__ldg(agg + (jj))]);
                 }
-                di = val[Lv.diagPos[i]];
+                di = val[__ldg(Lv.diagPos + (i))];
             }
             xa[i] = xi + om * (b[i] - ax) / di;
         }
@@ -554,7 +624,7 @@ __device__ double vcycle(Shared &S, int &rp) {
                 di = W.d[i];
             } else {
                 ax = csrRow(Lv, val, xa, i);
-                di = val[Lv.diagPos[i]];
+                di = val[__ldg(Lv.diagPos + (i))];
             }
             const double zi = xa[i] + om * (b[i] - ax) / di;
             xb[i] = zi;
@@ -594,8 +664,11 @@ __device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, do
         res.converged = true;
         return res;
     }
-    if (amg)
+    if (amg) {
+        mark(S, 4);
         amgRefresh(S);
+        mark(S, 5);
+    }
     double *r = W.r, *z = W.z, *p = W.pv, *Ap = W.v;
     double rz;
     if (amg) {
@@ -706,27 +779,63 @@ __device__ __forceinline__ void pushSample(Shared &S, int e, double v) {
 }
 
 // ---------------------------------------------------------------- the solve
-__device__ void carve(Shared &S, double *ws) {
+// Workspace placement: arrays in priority order go to the shared-memory arena
+// while it has room (the hot Krylov/AMG vectors and the matrix first), the rest
+// to this CTA's global workspace, which has a slot for every array.
+__device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     const DevClass &C = S.C;
-    const int n = C.n, nf = C.n + C.nfy;
+    const long n = C.n, nf = C.n + C.nfy;
     Work &W = S.W;
-    double *p = ws;
+    double *g = ws;
+    long used = 0;
     auto take = [&](long cnt) {
-        double *r = p;
-        p += (cnt + 31) / 32 * 32;
-        return r;
+        const long sz = (cnt + 31) / 32 * 32;
+        double *gp = g;
+        g += sz;
+        if (used + sz <= arenaDoubles) {
+            double *sp = arena + used;
+            used += sz;
+            return sp;
+        }
+        return gp;
     };
+    const int m = C.lev[C.nlev - 1].n;
+    // tier 1: matrix and Krylov vectors
+    W.d = take(n);
+    W.aW = take(n);
+    W.aE = take(n);
+    W.aS = take(n);
+    W.aN = take(n);
+    W.r = take(n);
+    W.pv = take(n);
+    W.v = take(n);
+    W.ph = take(n);
+    W.s = take(n);
+    W.sh = take(n);
+    W.t = take(n);
+    W.rh = take(n);
+    // tier 2: AMG
+    W.z = take(n);
+    W.xa = take(n);
+    W.xb = take(n);
+    W.rr = take(n);
+    W.amgVal = take(C.amgVals);
+    W.amgVec = take(C.amgVecs);
+    // tier 3: solved fields and assembly inputs
+    W.pp = take(n);
     W.Ux = take(n);
     W.Uy = take(n);
-    W.p = take(n);
     W.k = take(n);
     W.w = take(n);
+    W.b = take(n);
+    W.aP = take(n);
     W.nuT = take(n);
     W.F1 = take(n);
-    W.F2 = take(n);
-    W.Pk = take(n);
-    W.CD = take(n);
-    W.S = take(n);
+    W.phi = take(nf);
+    W.phiPred = take(nf);
+    W.pCoeff = take(nf);
+    W.gPx = take(n);
+    W.gPy = take(n);
     W.gUxx = take(n);
     W.gUxy = take(n);
     W.gUyx = take(n);
@@ -735,40 +844,18 @@ __device__ void carve(Shared &S, double *ws) {
     W.gKy = take(n);
     W.gWx = take(n);
     W.gWy = take(n);
-    W.gPx = take(n);
-    W.gPy = take(n);
-    W.phi = take(nf);
+    // tier 4
+    W.p = take(n);
+    W.F2 = take(n);
+    W.Pk = take(n);
+    W.CD = take(n);
+    W.S = take(n);
     W.phiOld = take(nf);
-    W.phiPred = take(nf);
-    W.pCoeff = take(nf);
-    W.d = take(n);
-    W.aW = take(n);
-    W.aE = take(n);
-    W.aS = take(n);
-    W.aN = take(n);
-    W.b = take(n);
-    W.aP = take(n);
     W.aPraw = take(n);
     W.Uxp = take(n);
     W.Uyp = take(n);
     W.kOld = take(n);
     W.wOld = take(n);
-    W.pp = take(n);
-    W.r = take(n);
-    W.rh = take(n);
-    W.pv = take(n);
-    W.v = take(n);
-    W.s = take(n);
-    W.t = take(n);
-    W.ph = take(n);
-    W.sh = take(n);
-    W.z = take(n);
-    W.xa = take(n);
-    W.xb = take(n);
-    W.rr = take(n);
-    W.amgVal = take(C.amgVals);
-    W.amgVec = take(C.amgVecs);
-    const int m = C.lev[C.nlev - 1].n;
     W.dense0 = take(2L * m * m);
     W.dense1 = take(2L * m * m);
 }
@@ -805,8 +892,14 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
     }
     if (threadIdx.x < 4)
         S.cnt[threadIdx.x] = 0;
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         S.haveQPrev = 0;
+        S.innerKrylov = 0;
+        S.innerPressure = 0;
+        for (int t = 0; t < 8; ++t)
+            S.stage[t] = 0;
+        S.tmark = clock64();
+    }
     __syncthreads();
     // phi = interpolated fluxes of the initial state (wall faces carry U_b = 0)
     for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
@@ -892,6 +985,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         }
         __syncthreads();
 
+        mark(S, 7);
         // ---- SST closure (SSTModel.cpp:157-241) and the startup nuT floor (:1322-1337)
         if (turbUpdate) {
             if (!established && iter >= st.turbStart + st.floorIters)
@@ -929,6 +1023,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             __syncthreads();
         }
 
+        mark(S, 1);
         // ---- momentum x then y (assembleMomentum :303-482)
         LinRes resU[2];
         double momRes = 0.0, momScale = 0.0;
@@ -1121,9 +1216,12 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 momScale = acc[2];
             resU[comp] = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, U, sqrt(acc[1]),
                                   st.innerIter, st.innerTol);
+            if (threadIdx.x == 0)
+                S.innerKrylov += resU[comp].iterations;
             __syncthreads();
         }
 
+        mark(S, 2);
         // ---- predicted flux (stored Rhie-Chow, :1401-1419) and p' assembly (:717-830)
         const double relaxCorr = 1.0 - st.aU;
         double fs[1] = {0.0};
@@ -1222,14 +1320,18 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         blockSum<3>(pacc, S, rp);
         const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
         const double fluxScale = pacc[2];
+        mark(S, 3);
         LinRes resP;
         if (st.pSolver == kPBicgstab)
             resP = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, W.pp, sqrt(pacc[1]), st.innerIter,
                             st.innerTol);
         else
             resP = pcg(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver == kPAmg);
+        if (threadIdx.x == 0)
+            S.innerPressure += resP.iterations;
         __syncthreads();
 
+        mark(S, 4);
         // ---- corrections (:916-940, :1443-1467): grad p' with owner-valued wall faces
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
@@ -1474,6 +1576,8 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     resK = rr;
                 else
                     resW = rr;
+                if (threadIdx.x == 0)
+                    S.innerKrylov += rr.iterations;
                 __syncthreads();
                 if (eq == 0) {
                     FOR_CELLS(c) W.k[c] = dmax(st.kMin, dmin(st.kMax, W.k[c]));
@@ -1491,6 +1595,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             }
         }
 
+        mark(S, 6);
         // ---- change norms and bookkeeping (:1520-1715)
         double mx[6] = {1e-30, 1e-30, 0.0, 0.0, 1e-300, 0.0};
         FOR_CELLS(c) {
@@ -1508,8 +1613,6 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         if (turbUpdate) {
             lastK = mx[2] / mx[0];
             lastW = mx[3] / mx[1];
-            pushSample(S, 1, lastK);
-            pushSample(S, 2, lastW);
         }
         double e[11];
         e[0] = iter;
@@ -1522,7 +1625,19 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         e[7] = momRes / dmax(momScale, 1e-300);
         e[8] = contScaled;
         e[9] = mx[5] / mx[4];
-        pushSample(S, 0, e[9]);
+        // one barrier pair for every sample of this iteration (U, k, omega, monitor)
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            S.ring[0][S.cnt[0] % kWindowCap] = e[9];
+            S.cnt[0] += 1;
+            if (turbUpdate) {
+                S.ring[1][S.cnt[1] % kWindowCap] = lastK;
+                S.cnt[1] += 1;
+                S.ring[2][S.cnt[2] % kWindowCap] = lastW;
+                S.cnt[2] += 1;
+            }
+        }
+        __syncthreads();
         const Est eU = estimate(S, 0, st.window, negligible);
         e[10] = eU.remaining;
         const bool haveMonitor = C.nobs > 0;
@@ -1707,10 +1822,13 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
 
 } // namespace
 
-__global__ void __launch_bounds__(512) solveKernel(const DevJob *jobs, int njobs, int *nextJob,
-                                                   double *wsBase, long wsStride) {
+// One kernel body, instantiated per CTA size so each gets its full register budget.
+template <int NT>
+__global__ void __launch_bounds__(NT) solveKernel(const DevJob *jobs, int njobs, int *nextJob,
+                                                  double *wsBase, long wsStride, int arenaDoubles) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     Shared &S = *reinterpret_cast<Shared *>(smemRaw);
+    double *arena = reinterpret_cast<double *>(smemRaw + ((sizeof(Shared) + 15) / 16) * 16);
     double *ws = wsBase + wsStride * blockIdx.x;
     for (;;) {
         if (threadIdx.x == 0)
@@ -1720,49 +1838,105 @@ __global__ void __launch_bounds__(512) solveKernel(const DevJob *jobs, int njobs
         if (j >= njobs)
             break;
         const DevJob &job = jobs[j];
-        // class descriptor and coefficients into shared memory
+        long long t0 = 0;
+        if (threadIdx.x == 0)
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
         {
             const int words = sizeof(DevClass) / 4;
             const int *src = reinterpret_cast<const int *>(job.cls);
             int *dst = reinterpret_cast<int *>(&S.C);
             for (int t = threadIdx.x; t < words; t += blockDim.x)
                 dst[t] = src[t];
-            if (threadIdx.x < 11)
-                S.coeff[threadIdx.x] = job.coeffs[threadIdx.x];
         }
         __syncthreads();
-        if (threadIdx.x == 0)
-            carve(S, ws);
+        // admission and unpack of theta (InferenceParameterSet::inBounds / unpack)
+        if (threadIdx.x == 0) {
+            bool ok = true;
+            for (int i = 0; i < 11; ++i)
+                S.coeff[i] = S.C.base[i];
+            for (int a = 0; a < S.C.nActive; ++a) {
+                const int idx = S.C.active[a];
+                const double v = job.theta[a];
+                if (v < S.C.lo[idx] || v > S.C.hi[idx] || isnan(v) || isinf(v))
+                    ok = false;
+                S.coeff[idx] = v;
+            }
+            S.admitted = ok;
+            if (ok)
+                carve(S, ws, arena, arenaDoubles);
+        }
         __syncthreads();
-        runSolve(S, job);
+        if (S.admitted) {
+            runSolve(S, job);
+        } else {
+            if (threadIdx.x == 0) {
+                const double nan = __longlong_as_double(0x7ff8000000000000LL);
+                RowOut o{3, 0, 0, 0, -1e30, nan, nan};
+                *job.row = o;
+            }
+            for (int t = threadIdx.x; t < S.C.nobs; t += blockDim.x)
+                job.pred[t] = __longlong_as_double(0x7ff8000000000000LL);
+            if (job.fields)
+                for (long e = threadIdx.x; e < 11L * S.C.n; e += blockDim.x)
+                    job.fields[e] = __longlong_as_double(0x7ff8000000000000LL);
+        }
         __syncthreads();
+        if (threadIdx.x == 0 && job.clock) {
+            long long t1;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            job.clock[0] = t0;
+            job.clock[1] = t1;
+            job.clock[2] = S.admitted ? S.innerKrylov : 0;
+            job.clock[3] = S.admitted ? S.innerPressure : 0;
+            for (int t = 0; t < 8; ++t)
+                job.clock[4 + t] = S.admitted ? S.stage[t] : 0;
+        }
     }
 }
 
-size_t solveSharedBytes() { return sizeof(Shared); }
+size_t solveSharedBytes() { return ((sizeof(Shared) + 15) / 16) * 16; }
+
+namespace {
+template <int NT> void *kernelFor() { return reinterpret_cast<void *>(&solveKernel<NT>); }
+void *pick(int block) {
+    switch (block) {
+    case 64: return kernelFor<64>();
+    case 128: return kernelFor<128>();
+    case 256: return kernelFor<256>();
+    default: return kernelFor<512>();
+    }
+}
+} // namespace
+
+int normalizeBlock(int block) { return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : 512; }
 
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
-                        int grid, int block, cudaStream_t stream) {
-    const size_t smem = sizeof(Shared);
-    cudaError_t e = cudaFuncSetAttribute(solveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        int grid, int block, int arenaDoubles, cudaStream_t stream) {
+    block = normalizeBlock(block);
+    const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
+    void *fn = pick(block);
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
         return e;
-    solveKernel<<<grid, block, smem, stream>>>(jobs, njobs, nextJob, ws, wsStride);
+    void *args[] = {&jobs, &njobs, &nextJob, &ws, &wsStride, &arenaDoubles};
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, stream);
+    if (e != cudaSuccess)
+        return e;
     return cudaGetLastError();
 }
 
-} // namespace rq
-
-namespace rq {
-int solveBlocksPerSM(int block) {
-    int blocks = 0;
-    const size_t smem = sizeof(Shared);
-    cudaFuncSetAttribute(solveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, solveKernel, block, smem) !=
+int solveBlocksPerSM(int block, int arenaDoubles) {
+    block = normalizeBlock(block);
+    const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
+    void *fn = pick(block);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
         cudaSuccess)
-        return 1;
-    return blocks > 0 ? blocks : 1;
+        return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, block, smem) != cudaSuccess)
+        return 0;
+    return blocks;
 }
+
 } // namespace rq

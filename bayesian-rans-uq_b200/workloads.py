@@ -1,0 +1,93 @@
+"""Synthetic stand-ins for the reference's calibration workloads (its Lee-Moser
+DNS data are not shipped): the seeded channel ensemble of the calibration's
+prior design, with a synthetic observed profile per Reynolds-number class.
+
+Draws restate cfdr.statistics.sample_rng / independent_uniform_design
+(rans-uq/python/cfdr/statistics.py:42-57, 69-91): SHA-256 of the identity
+string "cfdr-statistics-v1:{seed}:{id}:{purpose}" seeds a PCG64 stream, and
+each draw is rng.uniform(lower, upper), so the GPU and the reference see
+bit-identical coefficients.
+"""
+from __future__ import annotations
+
+import hashlib
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import core
+
+SEED = 20261010
+BOX_LO = (0.28, 0.084)  # (a1, beta*) -- calibration_coverage.py STAGE1_BOX
+BOX_HI = (0.34, 0.096)
+CLASSES = ((182.088, 128), (550.0, 256), (1000.0, 512))
+ALPHA_U = 0.8           # fixed once by the CPU pilot; the converged state does not depend on it
+MAX_ITER = 300000
+TOL = 1e-8
+NOISE = 0.0014          # relative synthetic observation noise
+
+
+def sample_rng(root_seed: int, sample_id: int, purpose: str) -> np.random.Generator:
+    identity = f"cfdr-statistics-v1:{root_seed}:{sample_id}:{purpose}"
+    digest = hashlib.sha256(identity.encode("utf-8")).digest()
+    words = [int.from_bytes(digest[i:i + 4], "little") for i in range(0, 32, 4)]
+    return np.random.Generator(np.random.PCG64(np.random.SeedSequence(words)))
+
+
+def uniform_design(ids, lower=BOX_LO, upper=BOX_HI, root_seed=SEED) -> np.ndarray:
+    lo, hi = np.asarray(lower, float), np.asarray(upper, float)
+    return np.array([sample_rng(root_seed, i, "prior-design").uniform(lo, hi) for i in ids])
+
+
+def channel_probes(re_tau: float, n: int = 30):
+    """30 stations log-spaced in y+ over [1, 175] at x = 0.5 (u_tau = 1, h = 1)."""
+    yp = np.geomspace(1.0, 175.0, n)
+    return np.full(n, 0.5), yp / re_tau
+
+
+def channel_batch(re_tau: float, ny: int, observed=None, sigma=None, precision="fp64",
+                  alpha_u=ALPHA_U, max_iter=MAX_ITER, tol=TOL, pressure_solver="AMG",
+                  block_threads=0) -> core.ForwardBatch:
+    """One Re_tau class of the channel ensemble as a ForwardBatch (the calibration's
+    forward_batch, docs/figures/calibration_coverage.py:81-113, on 3 x ny cells, y+ 0.5)."""
+    mesh = core.Mesh.make_periodic_channel_2d(3, ny, 1.0, 1.0, re_tau, 0.5)
+    mesh.compute_wall_distance()
+    x, y = channel_probes(re_tau)
+    obs = core.ObservationOperator()
+    observed = np.zeros(len(x)) if observed is None else observed
+    sigma = np.ones(len(x)) if sigma is None else sigma
+    for xi, yi, ui, si in zip(x, y, observed, sigma):
+        obs.add_velocity_profile(core.Vec3(float(xi), float(yi), 0.0), 0, float(ui), float(si))
+    st = core.SolverSettings(max_iterations=max_iter, convergence_tol=tol, alpha_u=alpha_u,
+                             body_force=core.Vec3(1.0, 0.0, 0.0), verbose=False,
+                             precision=precision, pressure_solver=pressure_solver,
+                             block_threads=block_threads)
+    bcs = core.FlowBoundaryConditions.channel_defaults(mesh, 1.0, 1.0, 10.0)
+    return core.ForwardBatch(mesh, core.InferenceParameterSet.a1_betaStar(), obs, bcs,
+                             1.0 / re_tau, st, core.Vec3(15.0, 0.0, 0.0), 0.0, 1.0, 10.0)
+
+
+@dataclass
+class Ensemble:
+    batches: list            # one ForwardBatch per Re_tau class
+    theta: np.ndarray        # (n, 2) draws
+    cls: np.ndarray          # (n,) class of each draw
+    truth: list              # per class: noise-free synthetic profile
+
+
+def channel_ensemble(n: int = 256, precision: str = "fp64", first_id: int = 0,
+                     alpha_u=ALPHA_U, max_iter=MAX_ITER) -> Ensemble:
+    """The 256-draw channel ensemble: draw i -> class i mod 3. The synthetic observed
+    profile of each class is that class's FP64 solve at (a1, beta*) = (0.31, 0.09)
+    times (1 + 0.0014 eps), eps ~ N(0,1) seeded; sigma_i = 0.0014 |u_i|."""
+    batches, truth = [], []
+    for c, (re_tau, ny) in enumerate(CLASSES):
+        probe = channel_batch(re_tau, ny, alpha_u=alpha_u, max_iter=max_iter)
+        res = probe.evaluate(np.array([[0.31, 0.09]]))
+        u = np.asarray(res.rows[0].result.predictions)
+        eps = sample_rng(SEED, c, "synthetic-observation-noise").standard_normal(len(u))
+        batches.append(channel_batch(re_tau, ny, u * (1 + NOISE * eps), NOISE * np.abs(u),
+                                     precision=precision, alpha_u=alpha_u, max_iter=max_iter))
+        truth.append(u)
+    ids = np.arange(first_id, first_id + n)
+    return Ensemble(batches, uniform_design(ids), ids % 3, truth)

@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 forward model on the reference's batched channel
+ensemble: 256 seeded draws of (a1, beta*) in [0.28,0.34]x[0.084,0.096], draw i
+on the Re_tau {182.088, 550, 1000}[i mod 3] periodic channel with {128, 256,
+512} tanh-stretched cells, tol 1e-8, each with a per-draw FP64 Gaussian
+log-likelihood against a seeded synthetic profile.
+
+One step = one batched evaluation of the whole ensemble (every draw solved
+from cold start to its verdict) with inputs already in HBM. Prints ONE JSON
+line (rank 0). `--impl reference` times the reference's own CPU solver
+(oracle/_ref, compiled from the reference sources) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "converged RANS-SST solves/s & p99 latency, batched vs plain GPU, <=1e-6 rel err"
+UNIT = "solves/s"
+# reference iteration counts of the (0.31, 0.09) draw per class at alpha_U 0.8, tol 1e-8
+# (CPU pilot of the compiled reference); used only by the CPU arm's extrapolation
+REF_ITERS = (12460, 58690, 258900)
+BYTES_OUTER, BYTES_KRYLOV, BYTES_PRESSURE = 1600, 360, 400  # algorithmic B/cell (FP64)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--draws", type=int, default=256)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=1500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- CPU arm (reference)
+def cpu_iteration_times(sample_iters: int):
+    """Per-outer-iteration wall time of the reference's own solver (oracle/_ref) for
+    each Re_tau class: one capped cold solve per class, all classes concurrently."""
+    from oracle import checker as ck
+    import rans_uq_b200.workloads as wl
+
+    out = [None] * 3
+
+    def run(c):
+        re_tau, ny = wl.CLASSES[c]
+        x, y = wl.channel_probes(re_tau)
+        case = ck.Case(ny=ny, re_tau=re_tau, nu=1 / re_tau, yplus=0.5, alpha_u=wl.ALPHA_U,
+                       tol=wl.TOL, max_iter=sample_iters, obs_x=x, obs_y=y,
+                       obs_value=np.zeros(30), obs_sigma=np.ones(30)).with_theta(0.31, 0.09)
+        t = time.perf_counter()
+        o = ck.solve(case, "ref")
+        out[c] = (time.perf_counter() - t) / max(o.iterations, 1)
+
+    th = [threading.Thread(target=run, args=(c,)) for c in range(3)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    return out
+
+
+def cpu_baseline(iters_per_draw, cls, sample_iters):
+    t_it = cpu_iteration_times(sample_iters)
+    cores = os.cpu_count() or 1
+    total = sum(iters_per_draw[i] * t_it[cls[i]] for i in range(len(cls)))
+    wall = total / cores  # one solve per core, perfectly packed
+    return dict(value=len(cls) / wall, unit=UNIT, cores=cores, kind="reference",
+                sample=(f"reference ForwardModel (oracle/_ref, g++ -O2) capped at {sample_iters} "
+                        f"outer iterations per Re_tau class, run concurrently; per-iteration "
+                        f"times {['%.3g ms' % (1e3 * t) for t in t_it]} x the ensemble's "
+                        f"iteration counts / {cores} cores (extrapolated)"))
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import rans_uq_b200.workloads as wl
+
+    ids = np.arange(args.draws)
+    cls = ids % 3
+    iters = [REF_ITERS[c] for c in cls]
+    if not (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+        return
+    vals = []
+    for _ in range(max(args.steps, 1)):
+        vals.append(cpu_baseline(iters, cls, args.cpu_sample_iters))
+    cb = vals[-1]
+    v = statistics.median(x["value"] for x in vals)
+    cb["value"] = v
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "256-draw channel ensemble, Re_tau {182,550,1000} x {128,256,512} cells",
+                   "draws": args.draws, "tol": wl.TOL, "alpha_u": wl.ALPHA_U},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ---------------------------------------------------------------- GPU arm
+class Clocks:
+    def __init__(self, index: int):
+        self.index, self.proc, self.path = index, None, ROOT / "gpurun_out" / "clocks.csv"
+
+    def __enter__(self):
+        self.path.parent.mkdir(exist_ok=True)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.index), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=self.f, stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+        self.f.close()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+    import rans_uq_b200 as rq
+    import rans_uq_b200.workloads as wl
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    # ---- set-up (untimed): the three mesh classes and this rank's draws (weak scaling)
+    ens = wl.channel_ensemble(args.draws, precision=args.precision, first_id=rank * args.draws)
+    n = len(ens.theta)
+    theta = torch.tensor(ens.theta, dtype=torch.float64, device=dev)
+    rows = torch.zeros((n, 6), dtype=torch.float64, device=dev)   # 48-byte rq_row_out
+    pred = torch.zeros((n, 30), dtype=torch.float64, device=dev)
+    clock = torch.zeros((n, 12), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        rq.evaluate_multi_device(ens.batches, ens.cls, theta.data_ptr(), rows.data_ptr(),
+                                 pred.data_ptr(), stream.cuda_stream, clock.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)  # L2 flush between timed steps (outside the events)
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- per-row outcomes, latency, work accounting
+    recs = rq.rows_from_device_bytes(rows.cpu().numpy())
+    status = recs["status"]
+    iters = recs["iterations"]
+    ck_ = clock.cpu().numpy()
+    lat = (ck_[:, 1] - ck_[:, 0].min()) / 1e6
+    conv = int(np.sum(status == 0))
+    cells = np.array([ens.batches[c]._problem.n_cells for c in ens.cls])
+    alg_bytes = float(np.sum(cells * (BYTES_OUTER * iters + BYTES_KRYLOV * ck_[:, 2] +
+                                      BYTES_PRESSURE * ck_[:, 3])))
+    total_conv = conv
+    if world > 1:
+        t = torch.tensor([conv], device=dev, dtype=torch.int64)
+        dist.all_reduce(t)
+        total_conv = int(t.item())
+    value = total_conv / (ms / 1e3)
+
+    # ---- end to end through the host API (host theta in, host rows out)
+    t0 = time.perf_counter()
+    res = rq.evaluate_multi(ens.batches, ens.cls, ens.theta)
+    e2e_s = time.perf_counter() - t0
+    e2e_conv = sum(1 for r in res.rows if r.result.status.name == "Converged")
+    h2d = n * 2 * 8 + n * 64  # theta + job descriptors
+    d2h = n * 48 + n * 30 * 8
+
+    # ---- plain path: one FP64 solve at a time (grid of one CTA), per-iteration cost per class,
+    # measured on capped solves and scaled by each draw's iteration count
+    plain = None
+    if rank == 0:
+        per_it = []
+        for c, (re_tau, ny) in enumerate(wl.CLASSES):
+            b = wl.channel_batch(re_tau, ny, precision="fp64", max_iter=3000)
+            t0 = time.perf_counter()
+            r = b.evaluate(np.array([[0.31, 0.09]]))
+            per_it.append((time.perf_counter() - t0) / max(r.rows[0].result.simple_iters, 1))
+        plain_s = float(sum(iters[i] * per_it[ens.cls[i]] for i in range(n)))
+        plain = {"solves_per_s": conv / plain_s, "per_iteration_ms": [1e3 * x for x in per_it],
+                 "method": "capped 3000-iteration single-solve launches x each draw's iterations"}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+        cpu = cpu_baseline(iters, ens.cls, args.cpu_sample_iters)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if \
+        (ROOT / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "256-draw channel ensemble, Re_tau {182,550,1000} x {128,256,512} cells",
+                   "draws_per_gpu": n, "tol": wl.TOL, "alpha_u": wl.ALPHA_U,
+                   "precision": args.precision, "l2": "flushed between timed steps",
+                   "parallelism": f"replicas x{world}"},
+        "converged": conv, "statuses": {s: int(np.sum(status == k)) for k, s in
+                                        enumerate(["converged", "unconverged", "diverged",
+                                                   "invalid", "unknown"])},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "iterations": {"mean": float(iters.mean()), "by_class": [int(np.median(iters[ens.cls == c])) for c in range(3)]},
+        "plain_fp64": plain,
+        "batched_vs_plain": value / plain["solves_per_s"] if plain else None,
+        "e2e": {"value": e2e_conv / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 1,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
+                     "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs", 6650.0),
+                     "traffic": None,
+                     "note": "algorithmic FP64 bytes (1600 B/cell/outer + 360 B/cell/Krylov it + "
+                             "400 B/cell/pressure it); the state is L2/SMEM resident"},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

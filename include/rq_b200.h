@@ -160,11 +160,16 @@ int rq_evaluate_multi(rq_problem *const *problems, int32_t n_problems,
                       const int32_t *problem_of_row, const double *theta, int32_t theta_stride,
                       int64_t n, rq_row_out *rows, double *predictions, int32_t pred_stride);
 
-/* Same on device buffers (device theta, rows, predictions) on a CUDA stream (cudaStream_t as void*). */
+/* Same on device buffers (device theta, rows, predictions) on a CUDA stream (cudaStream_t as
+   void*), queued without waiting. clock_ns_dev (optional, device): 12 int64 per row -- the
+   solve's start and end on the GPU global timer (ns), its inner Krylov iterations, its
+   inner pressure-correction iterations, then SM cycles spent per stage: set-up, closure,
+   momentum, pressure assembly, pressure solve, AMG refresh, turbulence, bookkeeping. */
 int rq_evaluate_multi_device(rq_problem *const *problems, int32_t n_problems,
                              const int32_t *problem_of_row_host, const double *theta_dev,
                              int32_t theta_stride, int64_t n, rq_row_out *rows_dev,
-                             double *predictions_dev, int32_t pred_stride, void *stream);
+                             double *predictions_dev, int32_t pred_stride, void *stream,
+                             int64_t *clock_ns_dev);
 
 /* One solve from a cold start with all eleven coefficients. */
 int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *predictions,

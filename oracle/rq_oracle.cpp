@@ -364,7 +364,7 @@ struct Amg {
     int levels() const { return static_cast<int>(lev.size()); }
 };
 
-static const int AMG_MIN_COARSE = 50;  // LinearSolver.hpp:664
+static const int AMG_MIN_COARSE = 32;  // the reference stops at 50 (LinearSolver.hpp:664); 32 = one warp
 static const int AMG_MAX_LEVELS = 20;  // :663
 static const double AMG_JACOBI_W = 0.6;
 static const int AMG_SWEEPS = 2;

@@ -44,11 +44,13 @@ def test_fields_after_n_iterations(rq, checker, solver, ps, n_iter):
     uscale = np.max(np.abs(want.field("Ux")))
     assert np.max(np.abs(fields[0, 1] - want.field("Uy"))) / uscale < RTOL_TRAJ
     assert np.max(np.abs(fields[0, 3] - want.field("p"))) < 1e-9
-    # residual history: initial residuals of the x-momentum and pressure solves and the
-    # scaled momentum residual / relative change of U judged by the convergence test
+    # residual history: initial residual of the x-momentum solve, the scaled momentum
+    # residual and the relative change of U judged by the convergence test; the
+    # continuity residuals are round-off in an x-invariant channel (compared absolutely)
     h, g = hist[0], want.history
-    for col in (1, 4, 7, 9):
+    for col in (1, 7, 9):
         assert rel(h[:, col], g[:, col]) < 1e-8, col
+    assert np.max(np.abs(h[:, 4] - g[:, 4])) < 1e-10
 
 
 @pytest.mark.parametrize("fixture,solver", [("small_channel_ref", "AMG"),
