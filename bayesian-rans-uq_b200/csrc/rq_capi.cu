@@ -313,7 +313,7 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
             addI(&dl.diagPos, Lv.diagPos);
         }
         if (l > 0 || L == 1)
-            vecOff += static_cast<int>(pad32(4L * Lv.n));
+            vecOff += static_cast<int>(pad32(5L * Lv.n)); // b, xa, xb, r, 1/diag
         if (l + 1 < L) {
             addI(&dl.agg, Lv.agg);
             addI(&dl.childPtr, Lv.childPtr);
@@ -332,7 +332,7 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
         C.hi[a] = kUpper[a];
     }
     const long n = m.n, nf = m.n + m.nfy(), mc = h.coarseN();
-    C.wsDoubles = 46 * pad32(n) + 4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
+    C.wsDoubles = 47 * pad32(n) + 4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
     // upload and patch pointers
     P.dDoubles.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
     P.dInts.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));

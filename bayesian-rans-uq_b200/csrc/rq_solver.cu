@@ -38,6 +38,7 @@ struct Work {
     double *Uxp, *Uyp, *kOld, *wOld, *pp;
     double *r, *rh, *pv, *v, *s, *t, *ph, *sh;
     double *z, *xa, *xb, *rr;                // PCG / level-0 V-cycle
+    double *rd;                              // reciprocal diagonal of the system being solved
     double *amgVal, *amgVec, *dense0, *dense1;
 };
 
@@ -55,6 +56,7 @@ struct Shared {
     long long innerKrylov, innerPressure; // inner iterations of the solve (work accounting)
     long long stage[8];                   // clock64 cycles per stage (thread 0)
     long long tmark;
+    int wallBetaInit; // the wall-face omega still carries applyAllBCs' beta1
     double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
 };
 
@@ -250,7 +252,7 @@ struct LinRes {
 
 // Right-Jacobi BiCGSTAB (LinearSolver.hpp:251-345). r holds b - A x0 on entry
 // and r0n its norm (both computed by the caller's assembly phase).
-__device__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW,
+__device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW,
                            const double *aE, const double *aS, const double *aN, double *x,
                            double r0n, int maxIter, double tol) {
     const DevClass &C = S.C;
@@ -262,10 +264,12 @@ __device__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW
         return res;
     }
     double *r = W.r, *rh = W.rh, *p = W.pv, *v = W.v, *s = W.s, *t = W.t, *ph = W.ph, *sh = W.sh;
+    double *rd = W.rd;
     FOR_CELLS(c) {
         rh[c] = r[c];
         p[c] = 0.0;
         v[c] = 0.0;
+        rd[c] = (fabs(d[c]) > 1e-30) ? 1.0 / d[c] : 1.0; // jacobiPrecond as a product
     }
     double rho = 1, alpha = 1, omega = 1;
     // rhoN of the first iteration
@@ -278,8 +282,9 @@ __device__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW
             break;
         const double beta = (rhoN / (rho + 1e-30)) * (alpha / (omega + 1e-30));
         FOR_CELLS(c) {
-            p[c] = r[c] + beta * (p[c] - omega * v[c]);
-            ph[c] = jac(p[c], d[c]);
+            const double pc = r[c] + beta * (p[c] - omega * v[c]);
+            p[c] = pc;
+            ph[c] = pc * rd[c];
         }
         __syncthreads();
         double a1[1] = {0.0};
@@ -298,7 +303,7 @@ __device__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW
         FOR_CELLS(c) {
             const double sc = r[c] - alpha * v[c];
             s[c] = sc;
-            sh[c] = jac(sc, d[c]);
+            sh[c] = sc * rd[c];
             a2[0] += sc * sc;
         }
         blockSum<1>(a2, S, rp);
@@ -356,7 +361,7 @@ __device__ __forceinline__ double level0Entry(const Work &W, int n, int e) {
 // Galerkin values of every coarse level from the current pressure system,
 // then the dense inverse of the coarsest level by Gauss-Jordan elimination
 // (ping-pong buffers, one barrier per pivot).
-__device__ void amgRefresh(Shared &S) {
+__device__ __noinline__ void amgRefresh(Shared &S) {
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev;
@@ -372,6 +377,14 @@ __device__ void amgRefresh(Shared &S) {
             cv[e] = s;
         }
         __syncthreads();
+    }
+    // reciprocal diagonals of the smoothed coarse levels (vector slot 4 of each level)
+    for (int l = 1; l + 1 < L; ++l) {
+        const DevAmgLevel &Lv = C.lev[l];
+        const double *val = W.amgVal + Lv.valOff;
+        double *rdl = W.amgVec + Lv.vecOff + 4 * Lv.n;
+        for (int i = threadIdx.x; i < Lv.n; i += blockDim.x)
+            rdl[i] = 1.0 / val[__ldg(Lv.diagPos + i)];
     }
     const DevAmgLevel &Q = C.lev[L - 1];
     const int m = Q.n;
@@ -476,7 +489,7 @@ __device__ __forceinline__ double csrRow(const DevAmgLevel &L, const double *val
 }
 
 // z = M^-1 b at level 0 (b = W.r). Returns (r, z) reduced in the last phase.
-__device__ double vcycle(Shared &S, int &rp) {
+__device__ __noinline__ double vcycle(Shared &S, int &rp) {
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev, n0 = C.n, nx = C.nx;
@@ -513,22 +526,22 @@ __device__ double vcycle(Shared &S, int &rp) {
                     bi += fr[__ldg(F.childIdx + (k))];
                 b[i] = bi;
             }
-            const double di = (l == 0) ? W.d[i] : val[__ldg(Lv.diagPos + (i))];
-            xa[i] = om * bi / di;
+            const double ri = (l == 0) ? W.rd[i] : b[4 * n + i];
+            xa[i] = om * bi * ri;
         }
         __syncthreads();
         // P2: second sweep
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ax, di;
+            double ax, ri;
             if (l == 0) {
                 const Cell q = cellOf(C, i);
                 ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
-                di = W.d[i];
+                ri = W.rd[i];
             } else {
                 ax = csrRow(Lv, val, xa, i);
-                di = val[__ldg(Lv.diagPos + (i))];
+                ri = b[4 * n + i];
             }
-            xb[i] = xa[i] + om * (b[i] - ax) / di;
+            xb[i] = xa[i] + om * (b[i] - ax) * ri;
         }
         __syncthreads();
         // P3: residual
@@ -594,7 +607,7 @@ __device__ double vcycle(Shared &S, int &rp) {
         const int *agg = Lv.agg;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const double xi = xprev[i] + xc[__ldg(agg + (i))];
-            double ax, di;
+            double ax, ri;
             if (l == 0) {
                 const Cell q = cellOf(C, i);
                 const int c = i;
@@ -603,30 +616,30 @@ __device__ double vcycle(Shared &S, int &rp) {
                 const double tS = q.south ? W.aS[c] * X(c - nx) : 0.0;
                 const double tN = q.north ? W.aN[c] * X(c + nx) : 0.0;
                 ax = accum4(q, W.d[c] * xi, tW, tE, tS, tN);
-                di = W.d[c];
+                ri = W.rd[c];
             } else {
                 ax = 0.0;
                 for (int k = __ldg(Lv.ptr + (i)); k < __ldg(Lv.ptr + (i + 1)); ++k) {
                     const int jj = __ldg(Lv.col + (k));
                     ax += val[k] * (xprev[jj] + xc[__ldg(agg + (jj))]);
                 }
-                di = val[__ldg(Lv.diagPos + (i))];
+                ri = b[4 * n + i];
             }
-            xa[i] = xi + om * (b[i] - ax) / di;
+            xa[i] = xi + om * (b[i] - ax) * ri;
         }
         __syncthreads();
         double part = 0.0;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ax, di;
+            double ax, ri;
             if (l == 0) {
                 const Cell q = cellOf(C, i);
                 ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
-                di = W.d[i];
+                ri = W.rd[i];
             } else {
                 ax = csrRow(Lv, val, xa, i);
-                di = val[__ldg(Lv.diagPos + (i))];
+                ri = b[4 * n + i];
             }
-            const double zi = xa[i] + om * (b[i] - ax) / di;
+            const double zi = xa[i] + om * (b[i] - ax) * ri;
             xb[i] = zi;
             if (l == 0)
                 part += b[i] * zi;
@@ -654,7 +667,7 @@ __device__ double vcycle(Shared &S, int &rp) {
 }
 
 // PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0; r holds b and r0n its norm.
-__device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, double tol,
+__device__ __noinline__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, double tol,
                       bool amg) {
     const DevClass &C = S.C;
     const Work &W = S.W;
@@ -664,10 +677,13 @@ __device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, do
         res.converged = true;
         return res;
     }
+    FOR_CELLS(c) W.rd[c] = (fabs(W.d[c]) > 1e-30) ? 1.0 / W.d[c] : 1.0;
     if (amg) {
         mark(S, 4);
-        amgRefresh(S);
+        amgRefresh(S); // begins with a barrier-separated phase, so rd is complete after it
         mark(S, 5);
+    } else {
+        __syncthreads();
     }
     double *r = W.r, *z = W.z, *p = W.pv, *Ap = W.v;
     double rz;
@@ -676,7 +692,7 @@ __device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, do
     } else {
         double a[1] = {0.0};
         FOR_CELLS(c) {
-            z[c] = jac(r[c], W.d[c]);
+            z[c] = r[c] * W.rd[c];
             a[0] += r[c] * z[c];
         }
         blockSum<1>(a, S, rp);
@@ -718,7 +734,7 @@ __device__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, do
         } else {
             double a3[1] = {0.0};
             FOR_CELLS(c) {
-                z[c] = jac(r[c], W.d[c]);
+                z[c] = r[c] * W.rd[c];
                 a3[0] += r[c] * z[c];
             }
             blockSum<1>(a3, S, rp);
@@ -814,6 +830,7 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.sh = take(n);
     W.t = take(n);
     W.rh = take(n);
+    W.rd = take(n);
     // tier 2: AMG
     W.z = take(n);
     W.xa = take(n);
@@ -860,21 +877,28 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.dense1 = take(2L * m * m);
 }
 
-__device__ void runSolve(Shared &S, const DevJob &job) {
-    const DevClass &C = S.C;
-    const Work &W = S.W;
-    const DevSettings &st = C.st;
-    const int n = C.n, nx = C.nx, ny = C.ny, nfy = C.nfy;
-    const double nu = C.nu;
-    int rp = 0;
-    // coefficients (InferenceParameterSet order) and their blends (SSTModel.hpp:12-61)
-    const double sk1 = S.coeff[0], sw1 = S.coeff[1], b1 = S.coeff[2], al1 = S.coeff[3];
-    const double sk2 = S.coeff[4], sw2 = S.coeff[5], b2 = S.coeff[6], al2 = S.coeff[7];
-    const double bs = S.coeff[8], a1 = S.coeff[9];
-    auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };
-    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+// Locals shared by the phase functions (read from the CTA's shared state).
+#define RQ_PRELUDE                                                                              \
+    const DevClass &C = S.C;                                                                    \
+    const Work &W = S.W;                                                                        \
+    const DevSettings &st = C.st;                                                               \
+    const int n = C.n, nx = C.nx, ny = C.ny, nfy = C.nfy;                                       \
+    const double nu = C.nu;                                                                     \
+    const double sk1 = S.coeff[0], sw1 = S.coeff[1], b1 = S.coeff[2], al1 = S.coeff[3];         \
+    const double sk2 = S.coeff[4], sw2 = S.coeff[5], b2 = S.coeff[6], al2 = S.coeff[7];         \
+    const double bs = S.coeff[8], a1 = S.coeff[9];                                              \
+    auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };    \
+    auto bwOf = [&](int f) { return wallFaceOmega(C, S.wallBetaInit ? C.beta1Init : b1, f); }; \
+    (void)st; (void)n; (void)nx; (void)ny; (void)nfy; (void)nu; (void)sk1; (void)sw1;          \
+    (void)b1; (void)al1; (void)sk2; (void)sw2; (void)b2; (void)al2; (void)bs; (void)a1;         \
+    (void)blend; (void)bwOf;
 
-    // ---- initUniform (SIMPLESolver.cpp:267-298) and applyAllBCs
+// ---------------------------------------------------------------- phases
+// Each phase is a barrier-free sweep over cells or faces; the caller places
+// the barriers and reductions. Phases are separate (non-inlined) functions so
+// every sweep gets its own register allocation.
+__device__ __noinline__ void phInitCells(Shared &S) {
+    RQ_PRELUDE
     const double U0 = C.init[0], U1 = C.init[1], P0 = C.init[3], K0 = C.init[4], W0 = C.init[5];
     FOR_CELLS(c) {
         W.Ux[c] = U0;
@@ -890,18 +914,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         W.nuT[c] = a1 * K0 / dmax(a1 * om, 1e-20);
         W.S[c] = 0.0;
     }
-    if (threadIdx.x < 4)
-        S.cnt[threadIdx.x] = 0;
-    if (threadIdx.x == 0) {
-        S.haveQPrev = 0;
-        S.innerKrylov = 0;
-        S.innerPressure = 0;
-        for (int t = 0; t < 8; ++t)
-            S.stage[t] = 0;
-        S.tmark = clock64();
-    }
-    __syncthreads();
-    // phi = interpolated fluxes of the initial state (wall faces carry U_b = 0)
+}
+
+__device__ __noinline__ void phInitFlux(Shared &S) {
+    RQ_PRELUDE
     for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
         double v = 0.0;
         if (f < n) {
@@ -922,23 +938,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         }
         W.phi[f] = v;
     }
-    __syncthreads();
+}
 
-    bool established = false;
-    bool wallBetaInit = true; // the face omega still carries applyAllBCs' beta1
-    double lastK = 1.0, lastW = 1.0;
-    const double tol = st.tol, negligible = 0.01 * tol;
-    double worst = inf, fluxRef = 0.0, n0x = 1, n0y = 1, n0p = 1;
-    int status = 1, finalIter = st.maxIter;
-    bool converged = false, diverged = false;
-    double rateU = __longlong_as_double(0x7ff8000000000000LL);
-
-    auto bwOf = [&](int f) { return wallFaceOmega(C, wallBetaInit ? C.beta1Init : b1, f); };
-
-    for (int iter = 0; iter < st.maxIter; ++iter) {
-        const bool turbActive = iter >= st.turbStart;
-        const bool turbUpdate = turbActive && ((iter - st.turbStart) % st.turbInterval == 0);
-        // ---- phase: save U, interpolated old flux, gradients of U and p
+__device__ __noinline__ void phStart(Shared &S, bool turbUpdate) {
+    RQ_PRELUDE
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
             double v = 0.0;
             if (f < n) {
@@ -983,14 +986,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 W.gWy[c] = gy;
             }
         }
-        __syncthreads();
+}
 
-        mark(S, 7);
-        // ---- SST closure (SSTModel.cpp:157-241) and the startup nuT floor (:1322-1337)
-        if (turbUpdate) {
-            if (!established && iter >= st.turbStart + st.floorIters)
-                established = true;
-            const double floorV = established ? 0.0 : 0.1 * nu;
+__device__ __noinline__ void phClosure(Shared &S, double floorV) {
+    RQ_PRELUDE
             FOR_CELLS(c) {
                 const double s11 = W.gUxx[c], s22 = W.gUyy[c];
                 const double s12 = 0.5 * (W.gUxy[c] + W.gUyx[c]);
@@ -1020,15 +1019,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 W.Pk[c] = dmin(raw, lim);
                 W.nuT[c] = dmax(nut, floorV);
             }
-            __syncthreads();
-        }
+}
 
-        mark(S, 1);
-        // ---- momentum x then y (assembleMomentum :303-482)
-        LinRes resU[2];
-        double momRes = 0.0, momScale = 0.0;
-        for (int comp = 0; comp < 2; ++comp) {
-            if (comp == 1) { // gradients of the updated Ux for the y assembly
+__device__ __noinline__ void phGradU(Shared &S) {
+    RQ_PRELUDE
                 FOR_CELLS(c) {
                     const Cell q = cellOf(C, c);
                     double gx, gy;
@@ -1039,15 +1033,16 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     W.gUyx[c] = gx;
                     W.gUyy[c] = gy;
                 }
-                __syncthreads();
-            }
+}
+
+__device__ __noinline__ void phMomentum(Shared &S, int comp, double (&acc)[3]) {
+    RQ_PRELUDE
             double *U = comp == 0 ? W.Ux : W.Uy;
             const double *gUc_x = comp == 0 ? W.gUxx : W.gUyx; // grad of this component
             const double *gUc_y = comp == 0 ? W.gUxy : W.gUyy;
             const double *colX = comp == 0 ? W.gUxx : W.gUxy;  // dUx/dx_comp
             const double *colY = comp == 0 ? W.gUyx : W.gUyy;  // dUy/dx_comp
             const double fb = comp == 0 ? st.fx : st.fy;
-            double acc[3] = {0.0, 0.0, 0.0};
             FOR_CELLS(c) {
                 const Cell q = cellOf(C, c);
                 const int i = q.i, j = q.j;
@@ -1210,21 +1205,11 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     acc[2] += contribution;
                 }
             }
-            blockSum<3>(acc, S, rp);
-            momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
-            if (comp == 0)
-                momScale = acc[2];
-            resU[comp] = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, U, sqrt(acc[1]),
-                                  st.innerIter, st.innerTol);
-            if (threadIdx.x == 0)
-                S.innerKrylov += resU[comp].iterations;
-            __syncthreads();
-        }
+}
 
-        mark(S, 2);
-        // ---- predicted flux (stored Rhie-Chow, :1401-1419) and p' assembly (:717-830)
+__device__ __noinline__ void phPressureFaces(Shared &S, double (&fs)[1]) {
+    RQ_PRELUDE
         const double relaxCorr = 1.0 - st.aU;
-        double fs[1] = {0.0};
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
             int o, q;
             const double *A, *NX, *NY, *WT, *DL, *DX, *DY;
@@ -1266,8 +1251,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             W.pCoeff[f] = pc;
             fs[0] += fabs(ph);
         }
-        __syncthreads();
-        double pacc[3] = {0.0, 0.0, fs[0]};
+}
+
+__device__ __noinline__ void phPressureCells(Shared &S, double (&pacc)[3]) {
+    RQ_PRELUDE
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
             const int fE = c, fW = q.W, fN = n + c + nx, fS = n + c;
@@ -1317,22 +1304,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             pacc[0] += fabs(bsum);
             pacc[1] += bsum * bsum;
         }
-        blockSum<3>(pacc, S, rp);
-        const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
-        const double fluxScale = pacc[2];
-        mark(S, 3);
-        LinRes resP;
-        if (st.pSolver == kPBicgstab)
-            resP = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, W.pp, sqrt(pacc[1]), st.innerIter,
-                            st.innerTol);
-        else
-            resP = pcg(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver == kPAmg);
-        if (threadIdx.x == 0)
-            S.innerPressure += resP.iterations;
-        __syncthreads();
+}
 
-        mark(S, 4);
-        // ---- corrections (:916-940, :1443-1467): grad p' with owner-valued wall faces
+__device__ __noinline__ void phCorrGrad(Shared &S) {
+    RQ_PRELUDE
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
             double gx, gy;
@@ -1340,7 +1315,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             W.gKx[c] = gx; // scratch for grad p' (k gradients are recomputed below)
             W.gKy[c] = gy;
         }
-        __syncthreads();
+}
+
+__device__ __noinline__ void phCorrApply(Shared &S) {
+    RQ_PRELUDE
         FOR_CELLS(c) {
             const double rA = (fabs(W.aP[c]) > 1e-30) ? 1.0 / W.aP[c] : 0.0;
             W.Ux[c] -= rA * W.gKx[c] * C.vol[c];
@@ -1361,11 +1339,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             }
             W.phi[f] = v;
         }
-        __syncthreads();
+}
 
-        // ---- turbulence (:1476-1538)
-        LinRes resK{0, 0, 0, true}, resW{0, 0, 0, true};
-        if (turbUpdate) {
+__device__ __noinline__ void phTurbGradK(Shared &S) {
+    RQ_PRELUDE
             FOR_CELLS(c) {
                 const Cell q = cellOf(C, c);
                 W.kOld[c] = W.k[c];
@@ -1375,11 +1352,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 W.gKx[c] = gx;
                 W.gKy[c] = gy;
             }
-            __syncthreads();
-            for (int eq = 0; eq < 2; ++eq) { // 0: k, 1: omega
-                double *X = eq == 0 ? W.k : W.w;
-                const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
-                if (eq == 1) {
+}
+
+__device__ __noinline__ void phTurbGradW(Shared &S) {
+    RQ_PRELUDE
                     FOR_CELLS(c) {
                         const Cell q = cellOf(C, c);
                         double gx, gy;
@@ -1387,9 +1363,13 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                         W.gWx[c] = gx;
                         W.gWy[c] = gy;
                     }
-                    __syncthreads();
-                }
-                double acc[1] = {0.0};
+}
+
+__device__ __noinline__ void phTurbAssemble(Shared &S, int eq) {
+    RQ_PRELUDE
+    double *X = eq == 0 ? W.k : W.w;
+    const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
+    (void)gX; (void)gY;
                 FOR_CELLS(c) {
                     const Cell q = cellOf(C, c);
                     const bool isWall[4] = {false, false, !q.south, !q.north};
@@ -1548,10 +1528,13 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     W.b[c] = bsum;
                     (void)x0;
                 }
-                __syncthreads();
-                // initial residual with the (constrained) initial guess: wall cells of
-                // omega start from their wall value (read through x0, never from X,
-                // so the in-place update below cannot race with a neighbour's read)
+}
+
+__device__ __noinline__ void phTurbResidual(Shared &S, int eq, double (&acc)[1]) {
+    RQ_PRELUDE
+    double *X = eq == 0 ? W.k : W.w;
+    const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
+    (void)gX; (void)gY;
                 FOR_CELLS(c) {
                     const Cell q = cellOf(C, c);
                     auto x0 = [&](int cc) {
@@ -1569,16 +1552,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     if (eq == 1)
                         X[c] = xc;
                 }
-                blockSum<1>(acc, S, rp);
-                LinRes rr = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, X, sqrt(acc[0]),
-                                     st.innerIter, st.innerTol);
-                if (eq == 0)
-                    resK = rr;
-                else
-                    resW = rr;
-                if (threadIdx.x == 0)
-                    S.innerKrylov += rr.iterations;
-                __syncthreads();
+}
+
+__device__ __noinline__ void phTurbClamp(Shared &S, int eq) {
+    RQ_PRELUDE
                 if (eq == 0) {
                     FOR_CELLS(c) W.k[c] = dmax(st.kMin, dmin(st.kMax, W.k[c]));
                 } else {
@@ -1589,15 +1566,13 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                             v = wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, c)], 1e-20));
                         W.w[c] = v;
                     }
-                    wallBetaInit = false;
+                    if (threadIdx.x == 0)
+                        S.wallBetaInit = 0;
                 }
-                __syncthreads();
-            }
-        }
+}
 
-        mark(S, 6);
-        // ---- change norms and bookkeeping (:1520-1715)
-        double mx[6] = {1e-30, 1e-30, 0.0, 0.0, 1e-300, 0.0};
+__device__ __noinline__ void phNorms(Shared &S, bool turbUpdate, double (&mx)[6]) {
+    RQ_PRELUDE
         FOR_CELLS(c) {
             if (turbUpdate) {
                 mx[0] = dmax(mx[0], fabs(W.k[c]));
@@ -1609,6 +1584,179 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             const double ax = W.Ux[c] - W.Uxp[c], ay = W.Uy[c] - W.Uyp[c];
             mx[5] = dmax(mx[5], sqrt(ax * ax + ay * ay + 0.0));
         }
+}
+
+__device__ __noinline__ void phProbes(Shared &S) {
+    RQ_PRELUDE
+            if (threadIdx.x < C.nobs) { // PreparedObservation::evaluate (:678-772)
+                const int t = threadIdx.x;
+                const int cell = C.pcell[t];
+                const double *X = C.obsComp == 0 ? W.Ux : W.Uy;
+                const double center = X[cell];
+                double bx = 0, by = 0;
+                for (int k = 0; k < C.pnnb[t]; ++k) {
+                    const int nb = C.pnb[4 * t + k];
+                    const double diff = (nb < 0 ? 0.0 : X[nb]) - center;
+                    bx += C.pwt[4 * t + k] * C.pdx[4 * t + k] * diff;
+                    by += C.pwt[4 * t + k] * C.pdy[4 * t + k] * diff;
+                }
+                double gx = 0.0, gy = 0.0;
+                if (fabs(C.pdet[t]) > 1e-14 * (C.paxx[t] * C.payy[t] + 1e-300)) {
+                    gx = (C.payy[t] * bx - C.paxy[t] * by) / C.pdet[t];
+                    gy = (C.paxx[t] * by - C.paxy[t] * bx) / C.pdet[t];
+                }
+                S.q[t] = center + gx * C.pox[t] + gy * C.poy[t];
+            }
+}
+
+__device__ void runSolve(Shared &S, const DevJob &job) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const DevSettings &st = C.st;
+    const int n = C.n, nx = C.nx, ny = C.ny, nfy = C.nfy;
+    const double nu = C.nu;
+    int rp = 0;
+    // coefficients (InferenceParameterSet order) and their blends (SSTModel.hpp:12-61)
+    const double sk1 = S.coeff[0], sw1 = S.coeff[1], b1 = S.coeff[2], al1 = S.coeff[3];
+    const double sk2 = S.coeff[4], sw2 = S.coeff[5], b2 = S.coeff[6], al2 = S.coeff[7];
+    const double bs = S.coeff[8], a1 = S.coeff[9];
+    auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+
+    // ---- initUniform (SIMPLESolver.cpp:267-298) and applyAllBCs
+    phInitCells(S);
+    if (threadIdx.x < 4)
+        S.cnt[threadIdx.x] = 0;
+    if (threadIdx.x == 0)
+        S.wallBetaInit = 1;
+    if (threadIdx.x == 0) {
+        S.haveQPrev = 0;
+        S.innerKrylov = 0;
+        S.innerPressure = 0;
+        for (int t = 0; t < 8; ++t)
+            S.stage[t] = 0;
+        S.tmark = clock64();
+    }
+    __syncthreads();
+    // phi = interpolated fluxes of the initial state (wall faces carry U_b = 0)
+    phInitFlux(S);
+    __syncthreads();
+
+    bool established = false;
+    double lastK = 1.0, lastW = 1.0;
+    const double tol = st.tol, negligible = 0.01 * tol;
+    double worst = inf, fluxRef = 0.0, n0x = 1, n0y = 1, n0p = 1;
+    int status = 1, finalIter = st.maxIter;
+    bool converged = false, diverged = false;
+    double rateU = __longlong_as_double(0x7ff8000000000000LL);
+
+
+    for (int iter = 0; iter < st.maxIter; ++iter) {
+        const bool turbActive = iter >= st.turbStart;
+        const bool turbUpdate = turbActive && ((iter - st.turbStart) % st.turbInterval == 0);
+        // ---- phase: save U, interpolated old flux, gradients of U and p
+        phStart(S, turbUpdate);
+        __syncthreads();
+
+        mark(S, 7);
+        // ---- SST closure (SSTModel.cpp:157-241) and the startup nuT floor (:1322-1337)
+        if (turbUpdate) {
+            if (!established && iter >= st.turbStart + st.floorIters)
+                established = true;
+            const double floorV = established ? 0.0 : 0.1 * nu;
+            phClosure(S, floorV);
+            __syncthreads();
+        }
+
+        mark(S, 1);
+        // ---- momentum x then y (assembleMomentum :303-482)
+        LinRes resU[2];
+        double momRes = 0.0, momScale = 0.0;
+        for (int comp = 0; comp < 2; ++comp) {
+            if (comp == 1) { // gradients of the updated Ux for the y assembly
+                phGradU(S);
+                __syncthreads();
+            }
+            double *U = comp == 0 ? W.Ux : W.Uy;
+            double acc[3] = {0.0, 0.0, 0.0};
+            phMomentum(S, comp, acc);
+            blockSum<3>(acc, S, rp);
+            momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
+            if (comp == 0)
+                momScale = acc[2];
+            resU[comp] = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, U, sqrt(acc[1]),
+                                  st.innerIter, st.innerTol);
+            if (threadIdx.x == 0)
+                S.innerKrylov += resU[comp].iterations;
+            __syncthreads();
+        }
+
+        mark(S, 2);
+        // ---- predicted flux (stored Rhie-Chow, :1401-1419) and p' assembly (:717-830)
+        double fs[1] = {0.0};
+        phPressureFaces(S, fs);
+        __syncthreads();
+        double pacc[3] = {0.0, 0.0, fs[0]};
+        phPressureCells(S, pacc);
+        blockSum<3>(pacc, S, rp);
+        const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
+        const double fluxScale = pacc[2];
+        mark(S, 3);
+        LinRes resP;
+        if (st.pSolver == kPBicgstab)
+            resP = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, W.pp, sqrt(pacc[1]), st.innerIter,
+                            st.innerTol);
+        else
+            resP = pcg(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver == kPAmg);
+        if (threadIdx.x == 0)
+            S.innerPressure += resP.iterations;
+        __syncthreads();
+
+        mark(S, 4);
+        // ---- corrections (:916-940, :1443-1467): grad p' with owner-valued wall faces
+        phCorrGrad(S);
+        __syncthreads();
+        phCorrApply(S);
+        __syncthreads();
+
+        // ---- turbulence (:1476-1538)
+        LinRes resK{0, 0, 0, true}, resW{0, 0, 0, true};
+        if (turbUpdate) {
+            phTurbGradK(S);
+            __syncthreads();
+            for (int eq = 0; eq < 2; ++eq) { // 0: k, 1: omega
+                double *X = eq == 0 ? W.k : W.w;
+                const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
+                if (eq == 1) {
+                    phTurbGradW(S);
+                    __syncthreads();
+                }
+                double acc[1] = {0.0};
+                phTurbAssemble(S, eq);
+                __syncthreads();
+                // initial residual with the (constrained) initial guess: wall cells of
+                // omega start from their wall value (read through x0, never from X,
+                // so the in-place update below cannot race with a neighbour's read)
+                phTurbResidual(S, eq, acc);
+                blockSum<1>(acc, S, rp);
+                LinRes rr = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, X, sqrt(acc[0]),
+                                     st.innerIter, st.innerTol);
+                if (eq == 0)
+                    resK = rr;
+                else
+                    resW = rr;
+                if (threadIdx.x == 0)
+                    S.innerKrylov += rr.iterations;
+                __syncthreads();
+                phTurbClamp(S, eq);
+                __syncthreads();
+            }
+        }
+
+        mark(S, 6);
+        // ---- change norms and bookkeeping (:1520-1715)
+        double mx[6] = {1e-30, 1e-30, 0.0, 0.0, 1e-300, 0.0};
+        phNorms(S, turbUpdate, mx);
         blockMax<6>(mx, S, rp);
         if (turbUpdate) {
             lastK = mx[2] / mx[0];
@@ -1642,25 +1790,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         e[10] = eU.remaining;
         const bool haveMonitor = C.nobs > 0;
         if (haveMonitor && iter % (st.monitorInterval > 1 ? st.monitorInterval : 1) == 0) {
-            if (threadIdx.x < C.nobs) { // PreparedObservation::evaluate (:678-772)
-                const int t = threadIdx.x;
-                const int cell = C.pcell[t];
-                const double *X = C.obsComp == 0 ? W.Ux : W.Uy;
-                const double center = X[cell];
-                double bx = 0, by = 0;
-                for (int k = 0; k < C.pnnb[t]; ++k) {
-                    const int nb = C.pnb[4 * t + k];
-                    const double diff = (nb < 0 ? 0.0 : X[nb]) - center;
-                    bx += C.pwt[4 * t + k] * C.pdx[4 * t + k] * diff;
-                    by += C.pwt[4 * t + k] * C.pdy[4 * t + k] * diff;
-                }
-                double gx = 0.0, gy = 0.0;
-                if (fabs(C.pdet[t]) > 1e-14 * (C.paxx[t] * C.payy[t] + 1e-300)) {
-                    gx = (C.payy[t] * bx - C.paxy[t] * by) / C.pdet[t];
-                    gy = (C.paxx[t] * by - C.paxy[t] * bx) / C.pdet[t];
-                }
-                S.q[t] = center + gx * C.pox[t] + gy * C.poy[t];
-            }
+            phProbes(S);
             __syncthreads();
             bool finite = true;
             for (int t = 0; t < C.nobs; ++t)
@@ -1760,25 +1890,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
 
     // ---- outputs: verdict, probe predictions, log-likelihood (ObservationOperator.hpp:592-609)
     if (status == 0 || status == 1) {
-        if (threadIdx.x < C.nobs) {
-            const int t = threadIdx.x;
-            const int cell = C.pcell[t];
-            const double *X = C.obsComp == 0 ? W.Ux : W.Uy;
-            const double center = X[cell];
-            double bx = 0, by = 0;
-            for (int k = 0; k < C.pnnb[t]; ++k) {
-                const int nb = C.pnb[4 * t + k];
-                const double diff = (nb < 0 ? 0.0 : X[nb]) - center;
-                bx += C.pwt[4 * t + k] * C.pdx[4 * t + k] * diff;
-                by += C.pwt[4 * t + k] * C.pdy[4 * t + k] * diff;
-            }
-            double gx = 0.0, gy = 0.0;
-            if (fabs(C.pdet[t]) > 1e-14 * (C.paxx[t] * C.payy[t] + 1e-300)) {
-                gx = (C.payy[t] * bx - C.paxy[t] * by) / C.pdet[t];
-                gy = (C.paxx[t] * by - C.paxy[t] * bx) / C.pdet[t];
-            }
-            S.q[t] = center + gx * C.pox[t] + gy * C.poy[t];
-        }
+        phProbes(S);
         __syncthreads();
     }
     if (threadIdx.x == 0) {
