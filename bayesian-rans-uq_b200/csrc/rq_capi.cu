@@ -96,7 +96,16 @@ struct rq_problem {
     double base[11];
     int32_t nObs = 0;
     int block = 256;
+    int cpt = 0;     // cells per thread of the register-blocked solvers (0 = generic kernel)
     int arenaKb = 0; // shared-memory arena per CTA, 0 = automatic
+    cudaStream_t stream = nullptr; // for concurrent per-class launches of a multi-class batch
+    cudaEvent_t done = nullptr;
+    ~rq_problem() {
+        if (done)
+            cudaEventDestroy(done);
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
     // launch scratch, reused across calls
     DevBuf dWs, dJobs, dRows, dPred, dFields, dHist, dTheta, dCounter, dClock;
     std::mutex mu;
@@ -135,8 +144,8 @@ void validateSettings(const rq_settings &s) {
     if (s.precision != RQ_PREC_FP64 && s.precision != RQ_PREC_MIXED)
         throw std::invalid_argument("unknown precision");
     if (s.block_threads != 0 &&
-        (s.block_threads < 64 || s.block_threads > 512 || s.block_threads % 32 != 0))
-        throw std::invalid_argument("block_threads must be 0 or a multiple of 32 in [64, 512]");
+        (s.block_threads < 64 || s.block_threads > 1024 || s.block_threads % 32 != 0))
+        throw std::invalid_argument("block_threads must be 0 or a multiple of 32 in [64, 1024]");
 }
 
 rq::StructMesh buildMesh(const rq_mesh_desc &d) {
@@ -332,7 +341,10 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
         C.hi[a] = kUpper[a];
     }
     const long n = m.n, nf = m.n + m.nfy(), mc = h.coarseN();
-    C.wsDoubles = 47 * pad32(n) + 4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
+    // FP64 arrays, FP32 inner-solver copies (mixed form), faces, AMG, dense coarse
+    C.wsDoubles = 43 * pad32(n) + 15 * pad32((n + 1) / 2) + pad32((valOff + 1) / 2) +
+                  pad32((vecOff + 1) / 2) +
+                  4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
     // upload and patch pointers
     P.dDoubles.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
     P.dInts.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));
@@ -346,10 +358,12 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     check(cudaMemcpy(P.dCls.p, &C, sizeof(rq::DevClass), cudaMemcpyHostToDevice), "upload");
 }
 
-int defaultBlock(int n) {
-    if (n <= 512)
-        return 256;
-    return 512;
+// Default kernel variant for a class of n cells: the register-blocked solvers
+// when one CTA's registers can own every cell, the generic kernel otherwise.
+void defaultVariant(int n, int &block, int &cpt) {
+    (void)n;
+    block = 512; // fastest measured for 384-1536 cells
+    cpt = 0;
 }
 
 int maxSmemOptin() {
@@ -384,28 +398,15 @@ int chooseArena(const std::vector<const rq_problem *> &probs) {
     return static_cast<int>(bytes / 8 / 32 * 32);
 }
 
-// Launches one persistent solve over rows whose problems are probOfRow[r];
-// theta rows live on the device at thetaDev + r * thetaStride. Output buffers
-// are device pointers indexed by row.
-void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOfRow,
-                const double *thetaDev, int thetaStride, rq::RowOut *rowsDev, double *predDev,
-                int predStride, double *fieldsDev, long fieldStride, double *histDev, int histCap,
-                long long *clockDev, cudaStream_t stream) {
-    const int n = static_cast<int>(probOfRow.size());
-    if (n == 0)
-        return;
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    // longest solves first (cells as the cost proxy); results do not depend on order
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return probOfRow[a]->mesh.n > probOfRow[b]->mesh.n;
-    });
+// One persistent launch of a single mesh class over its rows.
+void launchClass(rq_problem &P, const std::vector<int> &rows, const double *thetaDev,
+                 int thetaStride, rq::RowOut *rowsDev, double *predDev, int predStride,
+                 double *fieldsDev, long fieldStride, double *histDev, int histCap,
+                 long long *clockDev, cudaStream_t stream) {
+    const int n = static_cast<int>(rows.size());
     std::vector<rq::DevJob> jobs(n);
-    int block = 32;
-    long wsStride = 0;
     for (int k = 0; k < n; ++k) {
-        const int r = order[k];
-        const rq_problem &P = *probOfRow[r];
+        const int r = rows[k];
         rq::DevJob &j = jobs[k];
         j.cls = P.dCls.as<rq::DevClass>();
         j.theta = thetaDev + static_cast<long>(r) * thetaStride;
@@ -415,27 +416,76 @@ void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOf
         j.hist = histDev ? histDev + static_cast<long>(r) * histCap * 11 : nullptr;
         j.histCap = histCap;
         j.clock = clockDev ? clockDev + 12L * r : nullptr;
-        block = std::max(block, P.block);
-        wsStride = std::max(wsStride, static_cast<long>(P.cls.wsDoubles));
     }
-    block = rq::normalizeBlock(block);
-    const int arena = chooseArena(probOfRow);
+    const long wsStride = P.cls.wsDoubles;
+    const int arena = chooseArena({&P});
     int dev = 0, sms = 1;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    const int perSM = rq::solveBlocksPerSM(block, arena);
+    const int perSM = rq::solveBlocksPerSM(P.block, P.cpt, arena);
     if (perSM < 1)
         throw RqError(RQ_E_CUDA, "solve kernel does not fit on an SM with this arena");
     const int grid = std::max(1, std::min(n, sms * perSM));
-    owner.dJobs.ensure(sizeof(rq::DevJob) * n);
-    owner.dWs.ensure(sizeof(double) * wsStride * grid);
-    owner.dCounter.ensure(sizeof(int));
-    check(cudaMemcpyAsync(owner.dJobs.p, jobs.data(), sizeof(rq::DevJob) * n,
-                          cudaMemcpyHostToDevice, stream), "jobs");
-    check(cudaMemsetAsync(owner.dCounter.p, 0, sizeof(int), stream), "counter");
-    check(rq::launchSolve(owner.dJobs.as<rq::DevJob>(), n, owner.dCounter.as<int>(),
-                          owner.dWs.as<double>(), wsStride, grid, block, arena, stream),
+    P.dJobs.ensure(sizeof(rq::DevJob) * n);
+    P.dWs.ensure(sizeof(double) * wsStride * grid);
+    P.dCounter.ensure(sizeof(int));
+    check(cudaMemcpyAsync(P.dJobs.p, jobs.data(), sizeof(rq::DevJob) * n, cudaMemcpyHostToDevice,
+                          stream), "jobs");
+    check(cudaMemsetAsync(P.dCounter.p, 0, sizeof(int), stream), "counter");
+    check(rq::launchSolve(P.dJobs.as<rq::DevJob>(), n, P.dCounter.as<int>(), P.dWs.as<double>(),
+                          wsStride, grid, P.block, P.cpt, arena, stream),
           "solve launch");
+}
+
+// Launches the rows (row r belongs to mesh class probOfRow[r]; theta rows live on the
+// device at thetaDev + r * thetaStride; outputs are device buffers indexed by row).
+// Each class is one persistent launch with its own kernel variant; several classes
+// run concurrently on per-class streams (largest class first) joined back into `stream`.
+void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOfRow,
+                const double *thetaDev, int thetaStride, rq::RowOut *rowsDev, double *predDev,
+                int predStride, double *fieldsDev, long fieldStride, double *histDev, int histCap,
+                long long *clockDev, cudaStream_t stream) {
+    (void)owner;
+    std::vector<rq_problem *> classes;
+    std::vector<std::vector<int>> rowsOf;
+    for (int r = 0; r < static_cast<int>(probOfRow.size()); ++r) {
+        rq_problem *P = const_cast<rq_problem *>(probOfRow[r]);
+        auto it = std::find(classes.begin(), classes.end(), P);
+        if (it == classes.end()) {
+            classes.push_back(P);
+            rowsOf.push_back({r});
+        } else {
+            rowsOf[it - classes.begin()].push_back(r);
+        }
+    }
+    if (classes.empty())
+        return;
+    std::vector<int> order(classes.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return classes[a]->mesh.n > classes[b]->mesh.n; });
+    if (classes.size() == 1) {
+        launchClass(*classes[0], rowsOf[0], thetaDev, thetaStride, rowsDev, predDev, predStride,
+                    fieldsDev, fieldStride, histDev, histCap, clockDev, stream);
+        return;
+    }
+    cudaEvent_t fork;
+    check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+    check(cudaEventRecord(fork, stream), "event record");
+    for (int g : order) {
+        rq_problem &P = *classes[g];
+        if (!P.stream)
+            check(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking), "stream");
+        if (!P.done)
+            check(cudaEventCreateWithFlags(&P.done, cudaEventDisableTiming), "event");
+        check(cudaStreamWaitEvent(P.stream, fork, 0), "stream wait");
+        launchClass(P, rowsOf[g], thetaDev, thetaStride, rowsDev, predDev, predStride, fieldsDev,
+                    fieldStride, histDev, histCap, clockDev, P.stream);
+        check(cudaEventRecord(P.done, P.stream), "event record");
+    }
+    for (int g : order)
+        check(cudaStreamWaitEvent(stream, classes[g]->done, 0), "stream wait");
+    cudaEventDestroy(fork);
 }
 
 rq_row_out toRow(const rq::RowOut &o) {
@@ -522,7 +572,11 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
         P->active.assign(active, active + n_active);
         std::memcpy(P->base, base, sizeof(P->base));
         P->nObs = obs ? obs->n_obs : 0;
-        P->block = settings->block_threads ? settings->block_threads : defaultBlock(P->mesh.n);
+        defaultVariant(P->mesh.n, P->block, P->cpt);
+        if (settings->block_threads) { // an explicit CTA size selects the generic kernel
+            P->block = rq::normalizeBlock(settings->block_threads);
+            P->cpt = 0;
+        }
         upload(*P, obs, nu, *settings, init);
         *out = P.release();
     });
@@ -722,7 +776,6 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
         j.histCap = hist_cap;
         j.clock = nullptr;
         (void)saved;
-        const int block = rq::normalizeBlock(p->block);
         const int arena = chooseArena(probOfRow);
         p->dJobs.ensure(sizeof(rq::DevJob));
         p->dWs.ensure(sizeof(double) * p->cls.wsDoubles);
@@ -730,7 +783,8 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
         check(cudaMemcpy(p->dJobs.p, jobs.data(), sizeof(rq::DevJob), cudaMemcpyHostToDevice), "jobs");
         check(cudaMemset(p->dCounter.p, 0, sizeof(int)), "counter");
         check(rq::launchSolve(p->dJobs.as<rq::DevJob>(), 1, p->dCounter.as<int>(),
-                              p->dWs.as<double>(), p->cls.wsDoubles, 1, block, arena, nullptr),
+                              p->dWs.as<double>(), p->cls.wsDoubles, 1, p->block, p->cpt, arena,
+                              nullptr),
               "solve launch");
         rq::RowOut o;
         check(cudaMemcpy(&o, p->dRows.p, sizeof(o), cudaMemcpyDeviceToHost), "row");

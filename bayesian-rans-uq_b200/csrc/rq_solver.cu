@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 namespace rq {
 
 namespace {
@@ -42,9 +44,21 @@ struct Work {
     double *amgVal, *amgVec, *dense0, *dense1;
 };
 
+// Krylov / AMG storage of one value type (see "inner linear solvers").
+template <typename T> struct KW {
+    T *d, *aW, *aE, *aS, *aN, *rd;        // matrix and reciprocal diagonal
+    T *r, *rh, *pv, *v, *s, *t, *ph, *sh; // BiCGSTAB
+    T *z, *xa, *xb, *rr;                  // PCG / level-0 V-cycle (share BiCGSTAB-only storage)
+    T *x;                                 // FP32 correction of the mixed form
+    T *amgVal, *amgVec;                   // coarse levels: values; b, xa, xb, r, 1/diag
+    T *coarse;                            // inverse of a coarsest level of <= 32 rows
+};
+
 struct Shared {
     DevClass C;
     Work W;
+    KW<double> K64;
+    KW<float> K32;
     double coeff[11];
     double red[2][kRedSlots][32];
     double ring[4][kWindowCap];  // U, k, omega, Q change samples
@@ -58,6 +72,7 @@ struct Shared {
     long long tmark;
     int wallBetaInit; // the wall-face omega still carries applyAllBCs' beta1
     double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
+    float coarse32[32 * 32];              // its FP32 copy (mixed form)
 };
 
 // stage timers, as the reference's momentum / pressure / turbulence timers
@@ -250,39 +265,66 @@ struct LinRes {
 
 #define FOR_CELLS(c) for (int c = threadIdx.x; c < n; c += blockDim.x)
 
-// Right-Jacobi BiCGSTAB (LinearSolver.hpp:251-345). r holds b - A x0 on entry
-// and r0n its norm (both computed by the caller's assembly phase).
-__device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, const double *aW,
-                           const double *aE, const double *aS, const double *aN, double *x,
-                           double r0n, int maxIter, double tol) {
+// ---------------------------------------------------------------- inner linear solvers
+// The Krylov and AMG routines are templated on the value type T of their
+// vectors and matrices: T = double for the plain FP64 form, where they work
+// directly on the arrays the assembly wrote; T = float for the mixed form,
+// which solves for an FP32 correction inside an FP64 residual-refinement loop
+// (mixedSolve below). Scalar coefficients and every reduction stay FP64.
+
+// the five coefficient arrays of a 5-point system, held by value in registers
+template <typename T> struct Mat {
+    const T *d, *aW, *aE, *aS, *aN;
+};
+template <typename T> __device__ __forceinline__ Mat<T> matOf(const KW<T> &K) {
+    return Mat<T>{K.d, K.aW, K.aE, K.aS, K.aN};
+}
+
+// row of a 5-point system times x, diagonal first then faces in the reference's
+// matvec order (LinearSystem::matvec, LinearSolver.hpp:99-108)
+template <typename T>
+__device__ __forceinline__ T rowDotT(const Cell &q, const Mat<T> &M, const T *x, int nx) {
+    const int c = q.c;
+    const T tW = M.aW[c] * x[q.W], tE = M.aE[c] * x[q.E];
+    const T tS = q.south ? M.aS[c] * x[c - nx] : T(0);
+    const T tN = q.north ? M.aN[c] * x[c + nx] : T(0);
+    const T x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+    const T y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
+    return (((M.d[c] * x[c] + x1) + x2) + y1) + y2;
+}
+
+// Right-Jacobi BiCGSTAB (LinearSolver.hpp:251-345). K.r holds b - A x0 on entry and
+// r0n its norm; x is updated in place.
+template <typename T>
+__device__ __noinline__ LinRes bicgstabT(Shared &S, int &rp, const KW<T> &K, T *x, double r0n,
+                                         int maxIter, double tol) {
     const DevClass &C = S.C;
-    const Work &W = S.W;
     const int n = C.n, nx = C.nx;
     LinRes res{0, 0.0, r0n, false};
     if (r0n < 1e-30) {
         res.converged = true;
         return res;
     }
-    double *r = W.r, *rh = W.rh, *p = W.pv, *v = W.v, *s = W.s, *t = W.t, *ph = W.ph, *sh = W.sh;
-    double *rd = W.rd;
+    T *r = K.r, *rh = K.rh, *p = K.pv, *v = K.v, *s = K.s, *t = K.t, *ph = K.ph, *sh = K.sh,
+      *rd = K.rd;
+    const Mat<T> M = matOf(K);
+    double acc[1] = {0.0};
     FOR_CELLS(c) {
         rh[c] = r[c];
-        p[c] = 0.0;
-        v[c] = 0.0;
-        rd[c] = (fabs(d[c]) > 1e-30) ? 1.0 / d[c] : 1.0; // jacobiPrecond as a product
+        p[c] = T(0);
+        v[c] = T(0);
+        const T dc = M.d[c];
+        rd[c] = (fabs(double(dc)) > 1e-30) ? T(1) / dc : T(1); // jacobiPrecond as a product
+        acc[0] += double(r[c]) * double(r[c]);
     }
-    double rho = 1, alpha = 1, omega = 1;
-    // rhoN of the first iteration
-    double acc[1] = {0.0};
-    FOR_CELLS(c) acc[0] += r[c] * r[c];
     blockSum<1>(acc, S, rp);
-    double rhoN = acc[0];
+    double rhoN = acc[0], rho = 1, alpha = 1, omega = 1;
     for (int it = 0; it < maxIter; ++it) {
         if (fabs(rhoN) < 1e-30)
             break;
         const double beta = (rhoN / (rho + 1e-30)) * (alpha / (omega + 1e-30));
         FOR_CELLS(c) {
-            const double pc = r[c] + beta * (p[c] - omega * v[c]);
+            const T pc = r[c] + T(beta) * (p[c] - T(omega) * v[c]);
             p[c] = pc;
             ph[c] = pc * rd[c];
         }
@@ -290,9 +332,9 @@ __device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, con
         double a1[1] = {0.0};
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
-            const double vc = rowDot(q, d, aW, aE, aS, aN, ph, nx);
+            const T vc = rowDotT(q, M, ph, nx);
             v[c] = vc;
-            a1[0] += rh[c] * vc;
+            a1[0] += double(rh[c]) * double(vc);
         }
         blockSum<1>(a1, S, rp);
         const double rv = a1[0];
@@ -301,15 +343,15 @@ __device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, con
         alpha = rhoN / rv;
         double a2[1] = {0.0};
         FOR_CELLS(c) {
-            const double sc = r[c] - alpha * v[c];
+            const T sc = r[c] - T(alpha) * v[c];
             s[c] = sc;
             sh[c] = sc * rd[c];
-            a2[0] += sc * sc;
+            a2[0] += double(sc) * double(sc);
         }
         blockSum<1>(a2, S, rp);
         const double sn = sqrt(a2[0]);
         if (sn / r0n < tol) {
-            FOR_CELLS(c) x[c] += alpha * ph[c];
+            FOR_CELLS(c) x[c] += T(alpha) * ph[c];
             __syncthreads();
             res.iterations = it + 1;
             res.finalRes = sn / r0n;
@@ -319,21 +361,21 @@ __device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, con
         double a3[2] = {0.0, 0.0};
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
-            const double tc = rowDot(q, d, aW, aE, aS, aN, sh, nx);
+            const T tc = rowDotT(q, M, sh, nx);
             t[c] = tc;
-            a3[0] += tc * tc;
-            a3[1] += tc * s[c];
+            a3[0] += double(tc) * double(tc);
+            a3[1] += double(tc) * double(s[c]);
         }
         blockSum<2>(a3, S, rp);
         const double tt = a3[0];
         omega = (tt > 1e-30) ? a3[1] / tt : 0.0;
         double a4[2] = {0.0, 0.0};
         FOR_CELLS(c) {
-            x[c] += alpha * ph[c] + omega * sh[c];
-            const double rc = s[c] - omega * t[c];
+            x[c] += T(alpha) * ph[c] + T(omega) * sh[c];
+            const T rc = s[c] - T(omega) * t[c];
             r[c] = rc;
-            a4[0] += rc * rc;
-            a4[1] += rh[c] * rc;
+            a4[0] += double(rc) * double(rc);
+            a4[1] += double(rh[c]) * double(rc);
         }
         blockSum<2>(a4, S, rp);
         const double rn = sqrt(a4[0]);
@@ -348,50 +390,53 @@ __device__ __noinline__ LinRes bicgstab(Shared &S, int &rp, const double *d, con
         rho = rhoN;
         rhoN = a4[1];
     }
+    __syncthreads();
     return res;
 }
 
 // ---------------------------------------------------------------- AMG V-cycle
-__device__ __forceinline__ double level0Entry(const Work &W, int n, int e) {
+template <typename T> __device__ __forceinline__ T level0EntryT(const KW<T> &K, int n, int e) {
     const int slot = e / n, c = e - slot * n;
-    const double *a = slot == 0 ? W.d : slot == 1 ? W.aW : slot == 2 ? W.aE : slot == 3 ? W.aS : W.aN;
+    const T *a = slot == 0 ? K.d : slot == 1 ? K.aW : slot == 2 ? K.aE : slot == 3 ? K.aS : K.aN;
     return a[c];
 }
 
-// Galerkin values of every coarse level from the current pressure system,
-// then the dense inverse of the coarsest level by Gauss-Jordan elimination
-// (ping-pong buffers, one barrier per pivot).
-__device__ __noinline__ void amgRefresh(Shared &S) {
+// Galerkin values of every coarse level from the current pressure system, the
+// reciprocal diagonals of the smoothed levels, then the inverse of the coarsest
+// level: in place by one warp (Gauss-Jordan, SPD: no pivoting) when it has at
+// most 32 rows, else by the whole CTA with ping-pong buffers. The inversion
+// itself is always FP64; the mixed form stores the result in FP32.
+template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev;
     for (int l = 0; l + 1 < L; ++l) {
         const DevAmgLevel &F = C.lev[l];
         const DevAmgLevel &Q = C.lev[l + 1];
-        double *cv = W.amgVal + Q.valOff;
-        const double *fv = W.amgVal + F.valOff;
+        T *cv = K.amgVal + Q.valOff;
+        const T *fv = K.amgVal + F.valOff;
+        // the first Galerkin sums cancel strongly (diagonal against off-diagonals of
+        // one aggregate), so they are always formed from the FP64 finest matrix
         for (int e = threadIdx.x; e < Q.nnz; e += blockDim.x) {
             double s = 0.0;
-            for (int k = __ldg(F.gPtr + (e)); k < __ldg(F.gPtr + (e + 1)); ++k)
-                s += (l == 0) ? level0Entry(W, C.n, __ldg(F.gSrc + (k))) : fv[__ldg(F.gSrc + (k))];
-            cv[e] = s;
+            for (int k = __ldg(F.gPtr + e); k < __ldg(F.gPtr + e + 1); ++k)
+                s += (l == 0) ? level0EntryT(S.K64, C.n, __ldg(F.gSrc + k))
+                              : double(fv[__ldg(F.gSrc + k)]);
+            cv[e] = T(s);
         }
         __syncthreads();
     }
-    // reciprocal diagonals of the smoothed coarse levels (vector slot 4 of each level)
     for (int l = 1; l + 1 < L; ++l) {
         const DevAmgLevel &Lv = C.lev[l];
-        const double *val = W.amgVal + Lv.valOff;
-        double *rdl = W.amgVec + Lv.vecOff + 4 * Lv.n;
+        const T *val = K.amgVal + Lv.valOff;
+        T *rdl = K.amgVec + Lv.vecOff + 4 * Lv.n;
         for (int i = threadIdx.x; i < Lv.n; i += blockDim.x)
-            rdl[i] = 1.0 / val[__ldg(Lv.diagPos + i)];
+            rdl[i] = T(1) / val[__ldg(Lv.diagPos + i)];
     }
     const DevAmgLevel &Q = C.lev[L - 1];
     const int m = Q.n;
-    const double *qv = W.amgVal + Q.valOff;
+    const T *qv = K.amgVal + Q.valOff;
     if (m <= 32) {
-        // coarsest matrix into shared memory, then in-place Gauss-Jordan inversion by
-        // warp 0 (SPD: no pivoting); lane r owns row r
         double *a = S.coarse;
         for (int e = threadIdx.x; e < m * m; e += blockDim.x)
             a[e] = 0.0;
@@ -399,18 +444,18 @@ __device__ __noinline__ void amgRefresh(Shared &S) {
         if (L == 1) {
             for (int r = threadIdx.x; r < m; r += blockDim.x) {
                 const Cell q = cellOf(C, r);
-                a[r * m + r] += W.d[r];
-                a[r * m + q.W] += W.aW[r];
-                a[r * m + q.E] += W.aE[r];
+                a[r * m + r] += double(K.d[r]);
+                a[r * m + q.W] += double(K.aW[r]);
+                a[r * m + q.E] += double(K.aE[r]);
                 if (q.south)
-                    a[r * m + r - C.nx] += W.aS[r];
+                    a[r * m + r - C.nx] += double(K.aS[r]);
                 if (q.north)
-                    a[r * m + r + C.nx] += W.aN[r];
+                    a[r * m + r + C.nx] += double(K.aN[r]);
             }
         } else {
             for (int r = threadIdx.x; r < m; r += blockDim.x)
-                for (int k = __ldg(Q.ptr + (r)); k < __ldg(Q.ptr + (r + 1)); ++k)
-                    a[r * m + __ldg(Q.col + (k))] = qv[k];
+                for (int k = __ldg(Q.ptr + r); k < __ldg(Q.ptr + r + 1); ++k)
+                    a[r * m + __ldg(Q.col + k)] = double(qv[k]);
         }
         __syncthreads();
         if (threadIdx.x < 32) {
@@ -436,6 +481,11 @@ __device__ __noinline__ void amgRefresh(Shared &S) {
             }
         }
         __syncthreads();
+        if (!std::is_same<T, double>::value) {
+            for (int e = threadIdx.x; e < m * m; e += blockDim.x)
+                K.coarse[e] = T(a[e]);
+            __syncthreads();
+        }
         return;
     }
     const int m2 = 2 * m;
@@ -443,21 +493,21 @@ __device__ __noinline__ void amgRefresh(Shared &S) {
     for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
         A0[e] = ((e % m2) == m + e / m2) ? 1.0 : 0.0;
     __syncthreads();
-    if (L == 1) { // the whole (small) pressure system is the coarsest level
+    if (L == 1) {
         for (int r = threadIdx.x; r < m; r += blockDim.x) {
             const Cell q = cellOf(C, r);
-            A0[r * m2 + r] += W.d[r];
-            A0[r * m2 + q.W] += W.aW[r];
-            A0[r * m2 + q.E] += W.aE[r];
+            A0[r * m2 + r] += double(K.d[r]);
+            A0[r * m2 + q.W] += double(K.aW[r]);
+            A0[r * m2 + q.E] += double(K.aE[r]);
             if (q.south)
-                A0[r * m2 + r - C.nx] += W.aS[r];
+                A0[r * m2 + r - C.nx] += double(K.aS[r]);
             if (q.north)
-                A0[r * m2 + r + C.nx] += W.aN[r];
+                A0[r * m2 + r + C.nx] += double(K.aN[r]);
         }
     } else {
         for (int r = threadIdx.x; r < m; r += blockDim.x)
-            for (int k = __ldg(Q.ptr + (r)); k < __ldg(Q.ptr + (r + 1)); ++k)
-                A0[r * m2 + __ldg(Q.col + (k))] = qv[k];
+            for (int k = __ldg(Q.ptr + r); k < __ldg(Q.ptr + r + 1); ++k)
+                A0[r * m2 + __ldg(Q.col + k)] = double(qv[k]);
     }
     __syncthreads();
     for (int piv = 0; piv < m; ++piv) {
@@ -479,149 +529,144 @@ __device__ __noinline__ void amgRefresh(Shared &S) {
     }
 }
 
-// CSR row of level l >= 1 times x
-__device__ __forceinline__ double csrRow(const DevAmgLevel &L, const double *val, const double *x,
-                                         int i) {
-    double s = 0.0;
-    for (int k = __ldg(L.ptr + (i)); k < __ldg(L.ptr + (i + 1)); ++k)
-        s += val[k] * x[__ldg(L.col + (k))];
+template <typename T>
+__device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
+    T s = T(0);
+    for (int k = __ldg(L.ptr + i); k < __ldg(L.ptr + i + 1); ++k)
+        s += val[k] * x[__ldg(L.col + k)];
     return s;
 }
 
-// z = M^-1 b at level 0 (b = W.r). Returns (r, z) reduced in the last phase.
-__device__ __noinline__ double vcycle(Shared &S, int &rp) {
+// z = M^-1 b at level 0 (b = K.r, z -> K.z): pre-smoothing from zero (two damped
+// Jacobi sweeps), aggregate-sum restriction fused into the next level's first
+// sweep, dense coarsest solve, aggregate-broadcast prolongation fused into the
+// first of two post sweeps (symmetric). Returns (r, z), reduced in the last phase.
+template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev, n0 = C.n, nx = C.nx;
-    const double om = kJacobiW;
-    // vectors of coarse level l: b, xa, xb, r at amgVec + vecOff + {0,1,2,3}*n
-    auto vb = [&](int l) { return W.amgVec + C.lev[l].vecOff; };
-    // ---- down
+    const T om = T(kJacobiW);
+    const Mat<T> M = matOf(K);
+    T *const Krd = K.rd, *const Kr = K.r, *const Kz = K.z, *const Kxa = K.xa, *const Kxb = K.xb,
+             *const Krr = K.rr, *const amgVec = K.amgVec, *const amgVal = K.amgVal;
+    auto vb = [&](int l) { return amgVec + C.lev[l].vecOff; }; // b, xa, xb, r, 1/diag
     for (int l = 0; l + 1 < L; ++l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
-        double *b, *xa, *xb, *rr;
+        T *b, *xa, *xb, *rr;
         if (l == 0) {
-            b = W.r;
-            xa = W.xa;
-            xb = W.xb;
-            rr = W.rr;
+            b = Kr;
+            xa = Kxa;
+            xb = Kxb;
+            rr = Krr;
         } else {
             b = vb(l);
             xa = b + n;
             xb = b + 2 * n;
             rr = b + 3 * n;
         }
-        const double *val = W.amgVal + Lv.valOff;
-        // P1: restriction (l >= 1) and the first sweep from zero
+        const T *val = amgVal + Lv.valOff;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double bi;
+            T bi;
             if (l == 0) {
                 bi = b[i];
             } else {
                 const DevAmgLevel &F = C.lev[l - 1];
-                const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
-                bi = 0.0;
-                for (int k = __ldg(F.childPtr + (i)); k < __ldg(F.childPtr + (i + 1)); ++k)
-                    bi += fr[__ldg(F.childIdx + (k))];
+                const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
+                bi = T(0);
+                for (int k = __ldg(F.childPtr + i); k < __ldg(F.childPtr + i + 1); ++k)
+                    bi += fr[__ldg(F.childIdx + k)];
                 b[i] = bi;
             }
-            const double ri = (l == 0) ? W.rd[i] : b[4 * n + i];
+            const T ri = (l == 0) ? Krd[i] : b[4 * n + i];
             xa[i] = om * bi * ri;
         }
         __syncthreads();
-        // P2: second sweep
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ax, ri;
+            T ax, ri;
             if (l == 0) {
-                const Cell q = cellOf(C, i);
-                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
-                ri = W.rd[i];
+                ax = rowDotT(cellOf(C, i), M, xa, nx);
+                ri = Krd[i];
             } else {
-                ax = csrRow(Lv, val, xa, i);
+                ax = csrRowT(Lv, val, xa, i);
                 ri = b[4 * n + i];
             }
             xb[i] = xa[i] + om * (b[i] - ax) * ri;
         }
         __syncthreads();
-        // P3: residual
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ax;
-            if (l == 0) {
-                const Cell q = cellOf(C, i);
-                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xb, nx);
-            } else {
-                ax = csrRow(Lv, val, xb, i);
-            }
+            const T ax = (l == 0) ? rowDotT(cellOf(C, i), M, xb, nx) : csrRowT(Lv, val, xb, i);
             rr[i] = b[i] - ax;
         }
         __syncthreads();
     }
-    // ---- coarsest: restriction, dense solve into xb
     {
         const int l = L - 1;
-        const DevAmgLevel &Lv = C.lev[l];
-        const int m = Lv.n, m2 = 2 * m;
-        double *b = vb(l), *xb = b + 2 * m;
-        if (L == 1) { // a single level: direct solve of the whole system
+        const int m = C.lev[l].n, m2 = 2 * m;
+        T *b = vb(l), *xb = b + 2 * m;
+        if (L == 1) {
             for (int i = threadIdx.x; i < m; i += blockDim.x)
-                b[i] = W.r[i];
+                b[i] = Kr[i];
         } else {
             const DevAmgLevel &F = C.lev[l - 1];
-            const double *fr = (l == 1) ? W.rr : vb(l - 1) + 3 * F.n;
+            const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
             for (int i = threadIdx.x; i < m; i += blockDim.x) {
-                double bi = 0.0;
-                for (int k = __ldg(F.childPtr + (i)); k < __ldg(F.childPtr + (i + 1)); ++k)
-                    bi += fr[__ldg(F.childIdx + (k))];
+                T bi = T(0);
+                for (int k = __ldg(F.childPtr + i); k < __ldg(F.childPtr + i + 1); ++k)
+                    bi += fr[__ldg(F.childIdx + k)];
                 b[i] = bi;
             }
         }
         __syncthreads();
+        // the coarsest solve stays FP64 in both forms: the coarsest level of the
+        // pinned all-Neumann pressure system is nearly singular, and an FP32
+        // copy of its inverse loses the coarse correction
         for (int i = threadIdx.x; i < m; i += blockDim.x) {
             double s = 0.0;
             const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
             for (int j = 0; j < m; ++j)
-                s += row[j] * b[j];
-            xb[i] = s;
+                s += row[j] * double(b[j]);
+            xb[i] = T(s);
         }
         __syncthreads();
     }
-    // ---- up: prolongation fused into the first post sweep
     double rz = 0.0;
     for (int l = L - 2; l >= 0; --l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
-        const double *xc = vb(l + 1) + 2 * C.lev[l + 1].n; // coarse xb
-        double *b, *xa, *xb;
+        const T *xc = vb(l + 1) + 2 * C.lev[l + 1].n;
+        T *b, *xa, *xb;
         if (l == 0) {
-            b = W.r;
-            xa = W.xa;
-            xb = W.z;
+            b = Kr;
+            xa = Kxa;
+            xb = Kz;
         } else {
             b = vb(l);
             xa = b + n;
             xb = b + 2 * n;
         }
-        const double *xprev = (l == 0) ? W.xb : xb; // down-pass result
-        const double *val = W.amgVal + Lv.valOff;
+        const T *xprev = (l == 0) ? Kxb : xb;
+        const T *val = amgVal + Lv.valOff;
         const int *agg = Lv.agg;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const double xi = xprev[i] + xc[__ldg(agg + (i))];
-            double ax, ri;
+            const T xi = xprev[i] + xc[__ldg(agg + i)];
+            T ax, ri;
             if (l == 0) {
                 const Cell q = cellOf(C, i);
                 const int c = i;
-                auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + (jj))]; };
-                const double tW = W.aW[c] * X(q.W), tE = W.aE[c] * X(q.E);
-                const double tS = q.south ? W.aS[c] * X(c - nx) : 0.0;
-                const double tN = q.north ? W.aN[c] * X(c + nx) : 0.0;
-                ax = accum4(q, W.d[c] * xi, tW, tE, tS, tN);
-                ri = W.rd[c];
+                auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + jj)]; };
+                const T tW = M.aW[c] * X(q.W), tE = M.aE[c] * X(q.E);
+                const T tS = q.south ? M.aS[c] * X(c - nx) : T(0);
+                const T tN = q.north ? M.aN[c] * X(c + nx) : T(0);
+                const T x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+                const T y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
+                ax = (((M.d[c] * xi + x1) + x2) + y1) + y2;
+                ri = Krd[c];
             } else {
-                ax = 0.0;
-                for (int k = __ldg(Lv.ptr + (i)); k < __ldg(Lv.ptr + (i + 1)); ++k) {
-                    const int jj = __ldg(Lv.col + (k));
-                    ax += val[k] * (xprev[jj] + xc[__ldg(agg + (jj))]);
+                ax = T(0);
+                for (int k = __ldg(Lv.ptr + i); k < __ldg(Lv.ptr + i + 1); ++k) {
+                    const int jj = __ldg(Lv.col + k);
+                    ax += val[k] * (xprev[jj] + xc[__ldg(agg + jj)]);
                 }
                 ri = b[4 * n + i];
             }
@@ -630,19 +675,18 @@ __device__ __noinline__ double vcycle(Shared &S, int &rp) {
         __syncthreads();
         double part = 0.0;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double ax, ri;
+            T ax, ri;
             if (l == 0) {
-                const Cell q = cellOf(C, i);
-                ax = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, xa, nx);
-                ri = W.rd[i];
+                ax = rowDotT(cellOf(C, i), M, xa, nx);
+                ri = Krd[i];
             } else {
-                ax = csrRow(Lv, val, xa, i);
+                ax = csrRowT(Lv, val, xa, i);
                 ri = b[4 * n + i];
             }
-            const double zi = xa[i] + om * (b[i] - ax) * ri;
+            const T zi = xa[i] + om * (b[i] - ax) * ri;
             xb[i] = zi;
             if (l == 0)
-                part += b[i] * zi;
+                part += double(b[i]) * double(zi);
         }
         if (l == 0) {
             double a[1] = {part};
@@ -652,12 +696,12 @@ __device__ __noinline__ double vcycle(Shared &S, int &rp) {
             __syncthreads();
         }
     }
-    if (L == 1) { // the coarsest solve is the whole preconditioner
-        const double *xb = vb(0) + 2 * C.lev[0].n;
+    if (L == 1) {
+        const T *xb = vb(0) + 2 * C.lev[0].n;
         double part = 0.0;
         for (int i = threadIdx.x; i < n0; i += blockDim.x) {
-            W.z[i] = xb[i];
-            part += W.r[i] * xb[i];
+            Kz[i] = xb[i];
+            part += double(Kr[i]) * double(xb[i]);
         }
         double a[1] = {part};
         blockSum<1>(a, S, rp);
@@ -666,34 +710,76 @@ __device__ __noinline__ double vcycle(Shared &S, int &rp) {
     return rz;
 }
 
-// PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0; r holds b and r0n its norm.
-__device__ __noinline__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, int maxIter, double tol,
-                      bool amg) {
+// PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0 with the Jacobi or the AMG
+// preconditioner; K.r holds b and r0n its norm, x receives the solution.
+// With F32Precond the AMG V-cycle runs on the FP32 copies (S.K32) while PCG itself
+// stays in T = double: the mixed form of the pressure solve.
+template <typename T, bool F32Precond>
+__device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, double r0n,
+                                    int maxIter, double tol, bool amg, bool refresh) {
     const DevClass &C = S.C;
-    const Work &W = S.W;
     const int n = C.n, nx = C.nx;
     LinRes res{0, 0.0, r0n, false};
     if (r0n < 1e-30) {
         res.converged = true;
         return res;
     }
-    FOR_CELLS(c) W.rd[c] = (fabs(W.d[c]) > 1e-30) ? 1.0 / W.d[c] : 1.0;
-    if (amg) {
+    const Mat<T> M = matOf(K);
+    T *const rdv = K.rd;
+    FOR_CELLS(c) {
+        const T dc = M.d[c];
+        rdv[c] = (fabs(double(dc)) > 1e-30) ? T(1) / dc : T(1);
+        x[c] = T(0);
+    }
+    if constexpr (F32Precond) {
+        if (amg) { // FP32 copy of the finest level for the FP32 V-cycle
+            const KW<float> &F = S.K32;
+            FOR_CELLS(c) {
+                F.d[c] = float(M.d[c]);
+                F.aW[c] = float(M.aW[c]);
+                F.aE[c] = float(M.aE[c]);
+                F.aS[c] = float(M.aS[c]);
+                F.aN[c] = float(M.aN[c]);
+                F.rd[c] = (fabs(double(F.d[c])) > 1e-30) ? 1.0f / F.d[c] : 1.0f;
+            }
+            __syncthreads();
+        }
+    }
+    if (amg && refresh) {
         mark(S, 4);
-        amgRefresh(S); // begins with a barrier-separated phase, so rd is complete after it
+        if constexpr (F32Precond)
+            amgRefreshT<float>(S, S.K32);
+        else
+            amgRefreshT(S, K); // begins with a barrier-separated phase
         mark(S, 5);
     } else {
         __syncthreads();
     }
-    double *r = W.r, *z = W.z, *p = W.pv, *Ap = W.v;
+    T *r = K.r, *z = K.z, *p = K.pv, *Ap = K.v;
+    // z = M^-1 r through the FP32 V-cycle, (r, z) in FP64
+    auto precondF32 = [&]() {
+        const KW<float> &F = S.K32;
+        FOR_CELLS(c) F.r[c] = float(r[c]);
+        vcycleT<float>(S, rp, F);
+        double a[1] = {0.0};
+        FOR_CELLS(c) {
+            z[c] = T(F.z[c]);
+            a[0] += double(r[c]) * double(z[c]);
+        }
+        blockSum<1>(a, S, rp);
+        return a[0];
+    };
     double rz;
     if (amg) {
-        rz = vcycle(S, rp);
+        if constexpr (F32Precond)
+            rz = precondF32();
+        else
+            rz = vcycleT(S, rp, K);
     } else {
         double a[1] = {0.0};
         FOR_CELLS(c) {
-            z[c] = r[c] * W.rd[c];
-            a[0] += r[c] * z[c];
+            z[c] = r[c] * rdv[c];
+            a[0] += double(r[c]) * double(z[c]);
         }
         blockSum<1>(a, S, rp);
         rz = a[0];
@@ -703,10 +789,9 @@ __device__ __noinline__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, in
     for (int it = 0; it < maxIter; ++it) {
         double a1[1] = {0.0};
         FOR_CELLS(c) {
-            const Cell q = cellOf(C, c);
-            const double v = rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, p, nx);
+            const T v = rowDotT(cellOf(C, c), M, p, nx);
             Ap[c] = v;
-            a1[0] += p[c] * v;
+            a1[0] += double(p[c]) * double(v);
         }
         blockSum<1>(a1, S, rp);
         const double pAp = a1[0];
@@ -715,10 +800,10 @@ __device__ __noinline__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, in
         const double alpha = rz / pAp;
         double a2[1] = {0.0};
         FOR_CELLS(c) {
-            x[c] += alpha * p[c];
-            const double rc = r[c] - alpha * Ap[c];
+            x[c] += T(alpha) * p[c];
+            const T rc = r[c] - T(alpha) * Ap[c];
             r[c] = rc;
-            a2[0] += rc * rc;
+            a2[0] += double(rc) * double(rc);
         }
         blockSum<1>(a2, S, rp);
         const double rn = sqrt(a2[0]);
@@ -730,20 +815,128 @@ __device__ __noinline__ LinRes pcg(Shared &S, int &rp, double *x, double r0n, in
         }
         double rzNew;
         if (amg) {
-            rzNew = vcycle(S, rp);
+            if constexpr (F32Precond)
+                rzNew = precondF32();
+            else
+                rzNew = vcycleT(S, rp, K);
         } else {
             double a3[1] = {0.0};
             FOR_CELLS(c) {
-                z[c] = r[c] * W.rd[c];
-                a3[0] += r[c] * z[c];
+                z[c] = r[c] * rdv[c];
+                a3[0] += double(r[c]) * double(z[c]);
             }
             blockSum<1>(a3, S, rp);
             rzNew = a3[0];
         }
         const double beta = rzNew / (rz + 1e-30);
-        FOR_CELLS(c) p[c] = z[c] + beta * p[c];
+        FOR_CELLS(c) p[c] = z[c] + T(beta) * p[c];
         __syncthreads();
         rz = rzNew;
+    }
+    return res;
+}
+
+// Mixed form of one linear solve: FP32 Krylov (and AMG) iterations for a
+// correction of the FP64 solution, with the residual of the FP64 system
+// recomputed after each correction (iterative refinement) until it has dropped
+// by tol relative to the initial residual or the iteration budget is spent.
+// On entry W.b and W.r hold the FP64 right-hand side and b - A x (x = x64) and
+// r0n its norm; initialRes is that FP64 norm, as in the plain form.
+__device__ __noinline__ LinRes mixedSolve(Shared &S, int &rp, double *x64, double r0n, int maxIter,
+                                          double tol, int kind, bool refresh) {
+    const DevClass &C = S.C;
+    const Work &W = S.W;
+    const KW<float> &K = S.K32;
+    const int n = C.n, nx = C.nx;
+    LinRes out{0, 0.0, r0n, false};
+    if (r0n < 1e-30) {
+        out.converged = true;
+        return out;
+    }
+    FOR_CELLS(c) {
+        K.d[c] = float(W.d[c]);
+        K.aW[c] = float(W.aW[c]);
+        K.aE[c] = float(W.aE[c]);
+        K.aS[c] = float(W.aS[c]);
+        K.aN[c] = float(W.aN[c]);
+        K.r[c] = float(W.r[c]);
+    }
+    __syncthreads();
+    double rn = r0n;
+    bool refreshNow = refresh;
+    for (int round = 0; round < 8 && out.iterations < maxIter; ++round) {
+        // the FP32 solve targets the remaining reduction of the FP64 residual
+        const double innerTol = tol * r0n / rn;
+        double an[1] = {0.0};
+        FOR_CELLS(c) an[0] += double(K.r[c]) * double(K.r[c]);
+        blockSum<1>(an, S, rp);
+        const double r32n = sqrt(an[0]);
+        LinRes in;
+        FOR_CELLS(c) K.x[c] = 0.0f;
+        __syncthreads();
+        in = bicgstabT<float>(S, rp, K, K.x, r32n, maxIter - out.iterations, innerTol);
+        (void)refreshNow;
+        out.iterations += in.iterations;
+        FOR_CELLS(c) x64[c] += double(K.x[c]);
+        __syncthreads();
+        double a[1] = {0.0};
+        FOR_CELLS(c) {
+            const Cell q = cellOf(C, c);
+            const double rc = W.b[c] - rowDot(q, W.d, W.aW, W.aE, W.aS, W.aN, x64, nx);
+            W.r[c] = rc;
+            K.r[c] = float(rc);
+            a[0] += rc * rc;
+        }
+        blockSum<1>(a, S, rp);
+        rn = sqrt(a[0]);
+        if (rn / r0n < tol) {
+            out.converged = true;
+            break;
+        }
+        if (in.iterations == 0 || !isfinite(rn))
+            break;
+    }
+    out.finalRes = rn / r0n;
+    return out;
+}
+
+// Linear-solve dispatch for the precision of the class.
+__device__ __forceinline__ LinRes solveBicg(Shared &S, int &rp, double *x, double r0n, int maxIter,
+                                            double tol) {
+    if (S.C.st.precision == kMixed)
+        return mixedSolve(S, rp, x, r0n, maxIter, tol, kPBicgstab, false);
+    return bicgstabT<double>(S, rp, S.K64, x, r0n, maxIter, tol);
+}
+
+// The AMG coarse values (Galerkin sums and the coarsest inverse) are refreshed
+// when the previous pressure solve degraded -- more than 1.5x (+2) the PCG
+// iterations of the solve right after the last refresh, or not converged --
+// the rule AMGSolver applies to its aggregation (LinearSolver.hpp:924-941). The
+// stale coarse operator stays SPD, so PCG remains valid; the finest level
+// always uses the current matrix.
+__device__ __forceinline__ LinRes solvePressure(Shared &S, int &rp, double *x, double r0n,
+                                                int maxIter, double tol, int kind,
+                                                int &needRefresh, int &itersAfterRefresh) {
+    const bool amg = kind == kPAmg;
+    const bool refresh = amg && needRefresh;
+    LinRes res;
+    const bool mixed = S.C.st.precision == kMixed;
+    if (kind == kPBicgstab)
+        res = mixed ? mixedSolve(S, rp, x, r0n, maxIter, tol, kind, refresh)
+                    : bicgstabT<double>(S, rp, S.K64, x, r0n, maxIter, tol);
+    else if (mixed) // FP64 PCG, FP32 AMG V-cycle
+        res = pcgT<double, true>(S, rp, S.K64, x, r0n, maxIter, tol, amg, refresh);
+    else
+        res = pcgT<double, false>(S, rp, S.K64, x, r0n, maxIter, tol, amg, refresh);
+    if (amg && r0n >= 1e-30) {
+        if (refresh) {
+            needRefresh = 0;
+            itersAfterRefresh = res.iterations;
+        } else if (itersAfterRefresh <= 0) {
+            itersAfterRefresh = res.iterations;
+        } else if (!res.converged || res.iterations > 1.5 * itersAfterRefresh + 2) {
+            needRefresh = 1;
+        }
     }
     return res;
 }
@@ -815,7 +1008,34 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
         }
         return gp;
     };
+    auto takeF = [&](long cnt) { return reinterpret_cast<float *>(take((cnt + 1) / 2)); };
     const int m = C.lev[C.nlev - 1].n;
+    const bool mixed = C.st.precision == kMixed;
+    KW<float> &F = S.K32;
+    if (mixed) { // the FP32 inner-solver storage is the hot set of the mixed form
+        F.d = takeF(n);
+        F.aW = takeF(n);
+        F.aE = takeF(n);
+        F.aS = takeF(n);
+        F.aN = takeF(n);
+        F.rd = takeF(n);
+        F.r = takeF(n);
+        F.pv = takeF(n);
+        F.v = takeF(n);
+        F.ph = takeF(n);
+        F.s = takeF(n);
+        F.sh = takeF(n);
+        F.t = takeF(n);
+        F.rh = takeF(n);
+        F.x = takeF(n);
+        F.amgVec = takeF(C.amgVecs);
+        F.amgVal = takeF(C.amgVals);
+        F.z = F.s;
+        F.xa = F.t;
+        F.xb = F.sh;
+        F.rr = F.rh;
+        F.coarse = S.coarse32;
+    }
     // tier 1: matrix and Krylov vectors
     W.d = take(n);
     W.aW = take(n);
@@ -823,21 +1043,29 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.aS = take(n);
     W.aN = take(n);
     W.r = take(n);
-    W.pv = take(n);
-    W.v = take(n);
-    W.ph = take(n);
-    W.s = take(n);
-    W.sh = take(n);
-    W.t = take(n);
-    W.rh = take(n);
-    W.rd = take(n);
-    // tier 2: AMG
-    W.z = take(n);
-    W.xa = take(n);
-    W.xb = take(n);
-    W.rr = take(n);
-    W.amgVal = take(C.amgVals);
-    W.amgVec = take(C.amgVecs);
+    if (mixed) { // the mixed form keeps only the FP64 vectors of the pressure PCG
+        W.pv = take(n);
+        W.v = take(n);
+        W.z = take(n);
+        W.rd = take(n);
+    } else {
+        W.pv = take(n);
+        W.v = take(n);
+        W.ph = take(n);
+        W.s = take(n);
+        W.sh = take(n);
+        W.t = take(n);
+        W.rh = take(n);
+        W.rd = take(n);
+        // the pressure PCG / V-cycle vectors share storage with the BiCGSTAB-only
+        // vectors: the two solvers never run at the same time
+        W.z = W.s;
+        W.xa = W.t;
+        W.xb = W.sh;
+        W.rr = W.rh;
+        W.amgVec = take(C.amgVecs); // tier 2: AMG (vectors first: touched more often)
+        W.amgVal = take(C.amgVals);
+    }
     // tier 3: solved fields and assembly inputs
     W.pp = take(n);
     W.Ux = take(n);
@@ -875,6 +1103,33 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.wOld = take(n);
     W.dense0 = take(2L * m * m);
     W.dense1 = take(2L * m * m);
+    if (mixed) {
+        W.ph = W.s = W.sh = W.t = W.rh = nullptr;
+        W.xa = W.xb = W.rr = W.amgVec = W.amgVal = nullptr;
+    }
+    KW<double> &K = S.K64;
+    K.d = W.d;
+    K.aW = W.aW;
+    K.aE = W.aE;
+    K.aS = W.aS;
+    K.aN = W.aN;
+    K.rd = W.rd;
+    K.r = W.r;
+    K.rh = W.rh;
+    K.pv = W.pv;
+    K.v = W.v;
+    K.s = W.s;
+    K.t = W.t;
+    K.ph = W.ph;
+    K.sh = W.sh;
+    K.z = W.z;
+    K.xa = W.xa;
+    K.xb = W.xb;
+    K.rr = W.rr;
+    K.x = nullptr;
+    K.amgVal = W.amgVal;
+    K.amgVec = W.amgVec;
+    K.coarse = S.coarse;
 }
 
 // Locals shared by the phase functions (read from the CTA's shared state).
@@ -1643,6 +1898,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
     __syncthreads();
 
     bool established = false;
+    int amgNeed = 1, amgAfter = -1; // AMG coarse-value refresh state
     double lastK = 1.0, lastW = 1.0;
     const double tol = st.tol, negligible = 0.01 * tol;
     double worst = inf, fluxRef = 0.0, n0x = 1, n0y = 1, n0p = 1;
@@ -1684,8 +1940,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
             if (comp == 0)
                 momScale = acc[2];
-            resU[comp] = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, U, sqrt(acc[1]),
-                                  st.innerIter, st.innerTol);
+            resU[comp] = solveBicg(S, rp, U, sqrt(acc[1]), st.innerIter, st.innerTol);
             if (threadIdx.x == 0)
                 S.innerKrylov += resU[comp].iterations;
             __syncthreads();
@@ -1702,12 +1957,8 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
         const double fluxScale = pacc[2];
         mark(S, 3);
-        LinRes resP;
-        if (st.pSolver == kPBicgstab)
-            resP = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, W.pp, sqrt(pacc[1]), st.innerIter,
-                            st.innerTol);
-        else
-            resP = pcg(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver == kPAmg);
+        LinRes resP = solvePressure(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol,
+                                    st.pSolver, amgNeed, amgAfter);
         if (threadIdx.x == 0)
             S.innerPressure += resP.iterations;
         __syncthreads();
@@ -1739,8 +1990,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 // so the in-place update below cannot race with a neighbour's read)
                 phTurbResidual(S, eq, acc);
                 blockSum<1>(acc, S, rp);
-                LinRes rr = bicgstab(S, rp, W.d, W.aW, W.aE, W.aS, W.aN, X, sqrt(acc[0]),
-                                     st.innerIter, st.innerTol);
+                LinRes rr = solveBicg(S, rp, X, sqrt(acc[0]), st.innerIter, st.innerTol);
                 if (eq == 0)
                     resK = rr;
                 else
@@ -1773,6 +2023,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         e[7] = momRes / dmax(momScale, 1e-300);
         e[8] = contScaled;
         e[9] = mx[5] / mx[4];
+        e[10] = inf;
         // one barrier pair for every sample of this iteration (U, k, omega, monitor)
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1786,8 +2037,6 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             }
         }
         __syncthreads();
-        const Est eU = estimate(S, 0, st.window, negligible);
-        e[10] = eU.remaining;
         const bool haveMonitor = C.nobs > 0;
         if (haveMonitor && iter % (st.monitorInterval > 1 ? st.monitorInterval : 1) == 0) {
             phProbes(S);
@@ -1817,33 +2066,6 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 S.haveQPrev = 1;
             __syncthreads();
         }
-        {
-            double wv = e[7];
-            wv = dmax(wv, e[8]);
-            wv = dmax(wv, e[9]);
-            wv = dmax(wv, e[10]);
-            worst = wv;
-        }
-        if (turbActive) {
-            const Est eK = estimate(S, 1, st.window, negligible);
-            const Est eW = estimate(S, 2, st.window, negligible);
-            double wv = worst;
-            wv = dmax(wv, lastK);
-            wv = dmax(wv, eK.remaining);
-            wv = dmax(wv, lastW);
-            wv = dmax(wv, eW.remaining);
-            worst = wv;
-        }
-        if (haveMonitor) {
-            const Est eQ = estimate(S, 3, st.window, negligible);
-            const double last = S.cnt[3] > 0 ? S.ring[3][(S.cnt[3] - 1) % kWindowCap] : inf;
-            double wv = worst;
-            wv = dmax(wv, last);
-            wv = dmax(wv, eQ.remaining);
-            worst = wv;
-        }
-        if (!isfinite(worst))
-            worst = inf;
         if (iter == 0) {
             n0x = dmax(e[1], 1e-30);
             n0y = dmax(e[2], 1e-30);
@@ -1857,20 +2079,60 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         const double nm = dmax(n0x, n0y);
         const double nUx = safe(e[1], nm), nUy = safe(e[2], nm);
         const double nP = safe(e[4], dmax(n0p, fluxRef));
-        if (job.hist && iter < job.histCap && threadIdx.x == 0)
-            for (int t = 0; t < 11; ++t)
-                job.hist[11L * iter + t] = e[t];
         double maxRes = dmax(dmax(nUx, nUy), nP);
         if (turbActive)
             maxRes = dmax(dmax(maxRes, lastK), lastW);
         bool bad = !isfinite(lastK) || !isfinite(lastW);
         for (int t = 1; t <= 9; ++t)
             bad = bad || !isfinite(e[t]);
-        if (bad) {
+        if (bad)
             maxRes = inf;
-            worst = inf;
+        // The contraction estimates only change the verdict when every directly
+        // measured quantity already passes, so they are evaluated then, on the
+        // last iteration, on a divergence exit and for recorded history.
+        const double qLast = (haveMonitor && S.cnt[3] > 0) ? S.ring[3][(S.cnt[3] - 1) % kWindowCap] : inf;
+        double cheap = dmax(dmax(e[7], e[8]), e[9]);
+        if (turbActive)
+            cheap = dmax(dmax(cheap, lastK), lastW);
+        if (haveMonitor)
+            cheap = dmax(cheap, qLast);
+        const bool divergingNow = isnan(maxRes) || isinf(maxRes) || maxRes > st.divLimit;
+        const bool needEst = cheap < tol || iter == st.maxIter - 1 || divergingNow ||
+                             (job.hist && iter < job.histCap);
+        if (needEst) {
+            const Est eU = estimate(S, 0, st.window, negligible);
+            e[10] = eU.remaining;
+            rateU = eU.rate;
+            double wv = e[7];
+            wv = dmax(wv, e[8]);
+            wv = dmax(wv, e[9]);
+            wv = dmax(wv, e[10]);
+            worst = wv;
+            if (turbActive) {
+                const Est eK = estimate(S, 1, st.window, negligible);
+                const Est eW = estimate(S, 2, st.window, negligible);
+                wv = dmax(wv, lastK);
+                wv = dmax(wv, eK.remaining);
+                wv = dmax(wv, lastW);
+                wv = dmax(wv, eW.remaining);
+                worst = wv;
+            }
+            if (haveMonitor) {
+                const Est eQ = estimate(S, 3, st.window, negligible);
+                wv = dmax(wv, qLast);
+                wv = dmax(wv, eQ.remaining);
+                worst = wv;
+            }
+            if (!isfinite(worst))
+                worst = inf;
+        } else {
+            worst = cheap; // >= tol: not a verdict iteration
         }
-        rateU = eU.rate;
+        if (job.hist && iter < job.histCap && threadIdx.x == 0)
+            for (int t = 0; t < 11; ++t)
+                job.hist[11L * iter + t] = e[t];
+        if (bad)
+            worst = inf;
         const bool turbScheduled = st.turbStart < st.maxIter;
         if (worst < tol && iter > 0 && (!turbScheduled || (turbActive && established))) {
             converged = true;
@@ -2010,23 +2272,32 @@ size_t solveSharedBytes() { return ((sizeof(Shared) + 15) / 16) * 16; }
 
 namespace {
 template <int NT> void *kernelFor() { return reinterpret_cast<void *>(&solveKernel<NT>); }
-void *pick(int block) {
+void *pick(int block, int cpt) {
+    if (cpt != 0)
+        return nullptr;
     switch (block) {
     case 64: return kernelFor<64>();
     case 128: return kernelFor<128>();
     case 256: return kernelFor<256>();
-    default: return kernelFor<512>();
+    case 512: return kernelFor<512>();
+    case 1024: return kernelFor<1024>();
+    default: return nullptr;
     }
 }
 } // namespace
 
-int normalizeBlock(int block) { return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : 512; }
+bool launchVariantExists(int block, int cpt) { return pick(block, cpt) != nullptr; }
+
+int normalizeBlock(int block) {
+    return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : block <= 512 ? 512 : 1024;
+}
 
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
-                        int grid, int block, int arenaDoubles, cudaStream_t stream) {
-    block = normalizeBlock(block);
+                        int grid, int block, int cpt, int arenaDoubles, cudaStream_t stream) {
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
-    void *fn = pick(block);
+    void *fn = pick(block, cpt);
+    if (!fn)
+        return cudaErrorInvalidConfiguration;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess)
@@ -2038,10 +2309,11 @@ cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws,
     return cudaGetLastError();
 }
 
-int solveBlocksPerSM(int block, int arenaDoubles) {
-    block = normalizeBlock(block);
+int solveBlocksPerSM(int block, int cpt, int arenaDoubles) {
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
-    void *fn = pick(block);
+    void *fn = pick(block, cpt);
+    if (!fn)
+        return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
         cudaSuccess)
         return 0;

@@ -361,6 +361,10 @@ struct Amg {
     std::vector<AmgLevel> lev;
     std::vector<int> upPos, loPos; // LDU face -> level-0 nnz
     Vec inv;                        // dense inverse of the coarsest level (row major)
+    // coarse values are re-summed only when the previous solve degraded, the rule
+    // AMGSolver applies to its aggregation (LinearSolver.hpp:924-941)
+    bool needRefresh = true;
+    int itersAfterRefresh = -1;
     int levels() const { return static_cast<int>(lev.size()); }
 };
 
@@ -559,7 +563,7 @@ static Amg buildAmg(const Mesh &m) {
     return h;
 }
 
-static void amgRefresh(Amg &h, const Ldu &A) {
+static void amgLevel0(Amg &h, const Ldu &A) {
     AmgLevel &l0 = h.lev[0];
     for (int i = 0; i < A.n; ++i) {
         l0.A.val[l0.dpos[i]] = A.d[i];
@@ -569,6 +573,9 @@ static void amgRefresh(Amg &h, const Ldu &A) {
         l0.A.val[h.upPos[f]] = A.up[f];
         l0.A.val[h.loPos[f]] = A.lo[f];
     }
+}
+
+static void amgCoarse(Amg &h) {
     for (int l = 0; l + 1 < h.levels(); ++l)
         sumCoarse(h.lev[l], h.lev[l + 1]);
     denseInverse(h.lev.back().A, h.inv);
@@ -622,10 +629,35 @@ static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
 
 // PCG with the Jacobi (amg == nullptr) or AMG preconditioner: the reference's
 // PCG loop (LinearSolver.hpp:184-246 and :908-982 share it).
+static LinResult pcgBody(const Ldu &A, Vec &x, int maxIter, double tol, Amg *amg);
 static LinResult pcg(const Ldu &A, Vec &x, int maxIter, double tol, Amg *amg) {
     const int n = A.n;
-    if (amg)
-        amgRefresh(*amg, A);
+    bool refreshed = false;
+    if (amg) {
+        amgLevel0(*amg, A);
+        Vec r0(n);
+        A.residual(x, r0);
+        if (norm2(r0) < 1e-30) // solved at once: no preconditioner and no refresh bookkeeping
+            return pcgBody(A, x, maxIter, tol, amg);
+        if (amg->needRefresh) {
+            amgCoarse(*amg);
+            amg->needRefresh = false;
+            refreshed = true;
+        }
+    }
+    (void)n;
+    LinResult res = pcgBody(A, x, maxIter, tol, amg);
+    if (amg) {
+        if (refreshed || amg->itersAfterRefresh <= 0)
+            amg->itersAfterRefresh = res.iterations;
+        else if (!res.converged || res.iterations > 1.5 * amg->itersAfterRefresh + 2)
+            amg->needRefresh = true;
+    }
+    return res;
+}
+
+static LinResult pcgBody(const Ldu &A, Vec &x, int maxIter, double tol, Amg *amg) {
+    const int n = A.n;
     Vec r(n), z(n), p(n), Ap(n);
     LinResult res;
     A.residual(x, r);

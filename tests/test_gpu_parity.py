@@ -106,3 +106,27 @@ def test_multi_class_launch_equals_separate(rq):
     np.testing.assert_array_equal(multi.rows[0].result.predictions, sa.rows[0].result.predictions)
     np.testing.assert_array_equal(multi.rows[1].result.predictions, sb.rows[0].result.predictions)
     np.testing.assert_array_equal(multi.rows[2].result.predictions, sb.rows[1].result.predictions)
+
+
+@pytest.mark.parametrize("solver", ["AMG", "PCG"])
+def test_mixed_precision_small_channel_within_1e6(rq, solver):
+    """Mixed form (FP32 inner Krylov/AMG, FP64 refinement): converged profiles within
+    1e-6 relative of the reference's FP64 solve, same verdict."""
+    g = np.load(GOLDEN + "small_channel_ref.npz")
+    case = cases.small_channel()
+    batch = cases.product_batch(rq, case, pressure_solver=solver, precision="mixed")
+    res, fields, _ = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]])
+    row = res.rows[0]
+    assert row.result.status.name == str(g["status"])
+    assert rel(row.result.predictions, g["predictions"]) < 1e-6
+    assert rel(fields[0, 0], g["Ux"]) < 1e-6
+
+
+def test_config1_mixed_within_1e6(rq):
+    g = np.load(GOLDEN + "config1_ref.npz")
+    batch = cases.product_batch(rq, ck.config1_case(), precision="mixed")
+    res, fields, _ = batch.evaluate_fields([[0.31, 0.09]])
+    row = res.rows[0]
+    assert row.result.status.name == "Converged"
+    assert rel(row.result.predictions, g["predictions"]) < 1e-6
+    assert rel(fields[0, 0], g["Ux"]) < 1e-6
