@@ -515,8 +515,8 @@ def evaluate_multi(batches, problem_of_row, theta) -> ForwardBatchResult:
 def evaluate_multi_device(batches, problem_of_row, theta_dev, rows_dev, pred_dev, stream=0,
                           clock_dev=None) -> None:
     """Device-resident form of evaluate_multi (rq_evaluate_multi_device): theta_dev
-    (n x max n_active doubles), rows_dev (n x 48-byte rq_row_out), pred_dev
-    (n x max n_obs doubles) and clock_dev (n x 2 int64 ns, optional) are device
+    (n x max n_active doubles), rows_dev (n x 40-byte rq_row_out), pred_dev
+    (n x max n_obs doubles) and clock_dev (n x 12 int64, optional) are device
     pointers (ints); the launch is queued on `stream` and not waited for."""
     nb = len(batches)
     handles = (C.c_void_p * nb)(*[b._problem.handle.value for b in batches])

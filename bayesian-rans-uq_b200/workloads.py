@@ -11,7 +11,9 @@ bit-identical coefficients.
 from __future__ import annotations
 
 import hashlib
+import json
 from dataclasses import dataclass
+from pathlib import Path
 
 import numpy as np
 
@@ -79,12 +81,23 @@ def channel_ensemble(n: int = 256, precision: str = "fp64", first_id: int = 0,
                      alpha_u=ALPHA_U, max_iter=MAX_ITER) -> Ensemble:
     """The 256-draw channel ensemble: draw i -> class i mod 3. The synthetic observed
     profile of each class is that class's FP64 solve at (a1, beta*) = (0.31, 0.09)
-    times (1 + 0.0014 eps), eps ~ N(0,1) seeded; sigma_i = 0.0014 |u_i|."""
+    times (1 + 0.0014 eps), eps ~ N(0,1) seeded; sigma_i = 0.0014 |u_i|. The
+    noise-free profiles come from data/channel_truth.json (the reference solver's
+    own converged solve, written by data/make_channel_truth.py) when present, else
+    from a GPU solve here."""
     batches, truth = [], []
+    stored = {}
+    path = Path(__file__).parent / "data" / "channel_truth.json"
+    if path.exists():
+        stored = json.loads(path.read_text())
     for c, (re_tau, ny) in enumerate(CLASSES):
-        probe = channel_batch(re_tau, ny, alpha_u=alpha_u, max_iter=max_iter)
-        res = probe.evaluate(np.array([[0.31, 0.09]]))
-        u = np.asarray(res.rows[0].result.predictions)
+        rec = stored.get(str(c))
+        if rec is not None and rec["ny"] == ny and rec["status"] == "Converged":
+            u = np.asarray(rec["profile"], dtype=np.float64)
+        else:
+            probe = channel_batch(re_tau, ny, alpha_u=alpha_u, max_iter=MAX_ITER)
+            res = probe.evaluate(np.array([[0.31, 0.09]]))
+            u = np.asarray(res.rows[0].result.predictions)
         eps = sample_rng(SEED, c, "synthetic-observation-noise").standard_normal(len(u))
         batches.append(channel_batch(re_tau, ny, u * (1 + NOISE * eps), NOISE * np.abs(u),
                                      precision=precision, alpha_u=alpha_u, max_iter=max_iter))

@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--draws", type=int, default=256)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-sample-iters", type=int, default=1500)
+    ap.add_argument("--max-iter", type=int, default=None,
+                    help="cap on outer iterations per draw (profiling runs only; the "
+                         "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -160,6 +163,7 @@ def gpu_arm(args):
     import torch
     import torch.distributed as dist
     import rans_uq_b200 as rq
+    import rans_uq_b200.replicas as rp
     import rans_uq_b200.workloads as wl
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -173,10 +177,13 @@ def gpu_arm(args):
     stream = torch.cuda.current_stream(dev)
 
     # ---- set-up (untimed): the three mesh classes and this rank's draws (weak scaling)
-    ens = wl.channel_ensemble(args.draws, precision=args.precision, first_id=rank * args.draws)
+    max_iter = args.max_iter or wl.MAX_ITER
+    ids = rp.shard_ids(rank, world, args.draws)
+    ens = wl.channel_ensemble(args.draws, precision=args.precision, first_id=int(ids[0]),
+                              max_iter=max_iter)
     n = len(ens.theta)
     theta = torch.tensor(ens.theta, dtype=torch.float64, device=dev)
-    rows = torch.zeros((n, 6), dtype=torch.float64, device=dev)   # 48-byte rq_row_out
+    rows = torch.zeros(n * 40, dtype=torch.uint8, device=dev)     # n x 40-byte rq_row_out
     pred = torch.zeros((n, 30), dtype=torch.float64, device=dev)
     clock = torch.zeros((n, 12), dtype=torch.int64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -185,9 +192,15 @@ def gpu_arm(args):
         rq.evaluate_multi_device(ens.batches, ens.cls, theta.data_ptr(), rows.data_ptr(),
                                  pred.data_ptr(), stream.cuda_stream, clock.data_ptr())
 
-    for _ in range(args.warmup):
+    # W warm-up steps; the last one goes through the host API (theta from host
+    # memory in, rows and predictions back to host memory) and is the e2e timing.
+    for _ in range(max(args.warmup - 1, 0)):
         step()
     torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = rq.evaluate_multi(ens.batches, ens.cls, ens.theta)
+    e2e_s = time.perf_counter() - t0
+    e2e_conv = sum(1 for r in res.rows if r.result.status.name == "Converged")
     times = []
     with Clocks(local) as clk:
         for _ in range(args.steps):
@@ -201,62 +214,69 @@ def gpu_arm(args):
             e1.record(stream)
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
-    ms = float(np.median(times))
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-
-    # ---- per-row outcomes, latency, work accounting
+    ms_rank = float(np.median(times))
+    print(f"bench: timed step(s) {times} ms, e2e {e2e_s:.3f} s", file=sys.stderr, flush=True)
     recs = rq.rows_from_device_bytes(rows.cpu().numpy())
-    status = recs["status"]
-    iters = recs["iterations"]
-    ck_ = clock.cpu().numpy()
-    lat = (ck_[:, 1] - ck_[:, 0].min()) / 1e6
-    conv = int(np.sum(status == 0))
-    cells = np.array([ens.batches[c]._problem.n_cells for c in ens.cls])
-    alg_bytes = float(np.sum(cells * (BYTES_OUTER * iters + BYTES_KRYLOV * ck_[:, 2] +
-                                      BYTES_PRESSURE * ck_[:, 3])))
-    total_conv = conv
-    if world > 1:
-        t = torch.tensor([conv], device=dev, dtype=torch.int64)
-        dist.all_reduce(t)
-        total_conv = int(t.item())
-    value = total_conv / (ms / 1e3)
-
-    # ---- end to end through the host API (host theta in, host rows out)
-    t0 = time.perf_counter()
-    res = rq.evaluate_multi(ens.batches, ens.cls, ens.theta)
-    e2e_s = time.perf_counter() - t0
-    e2e_conv = sum(1 for r in res.rows if r.result.status.name == "Converged")
-    h2d = n * 2 * 8 + n * 64  # theta + job descriptors
-    d2h = n * 48 + n * 30 * 8
+    clock_host = clock.cpu().numpy()
+    conv = int(np.sum(recs["status"] == 0))
+    # step time = max over ranks, converged solves summed over ranks
+    ms, total_conv, _ = rp.reduce_step(ms_rank, conv, device=dev)
 
     # ---- plain path: one FP64 solve at a time (grid of one CTA), per-iteration cost per class,
     # measured on capped solves and scaled by each draw's iteration count
-    plain = None
-    if rank == 0:
-        per_it = []
-        for c, (re_tau, ny) in enumerate(wl.CLASSES):
-            b = wl.channel_batch(re_tau, ny, precision="fp64", max_iter=3000)
-            t0 = time.perf_counter()
-            r = b.evaluate(np.array([[0.31, 0.09]]))
-            per_it.append((time.perf_counter() - t0) / max(r.rows[0].result.simple_iters, 1))
-        plain_s = float(sum(iters[i] * per_it[ens.cls[i]] for i in range(n)))
-        plain = {"solves_per_s": conv / plain_s, "per_iteration_ms": [1e3 * x for x in per_it],
-                 "method": "capped 3000-iteration single-solve launches x each draw's iterations"}
-
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
+    per_it = []
+    for c, (re_tau, ny) in enumerate(wl.CLASSES):
+        b = wl.channel_batch(re_tau, ny, precision="fp64", max_iter=3000)
+        t0 = time.perf_counter()
+        r = b.evaluate(np.array([[0.31, 0.09]]))
+        per_it.append((time.perf_counter() - t0) / max(r.rows[0].result.simple_iters, 1))
     cpu = None
     if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
-        cpu = cpu_baseline(iters, ens.cls, args.cpu_sample_iters)
+        cpu = cpu_baseline(recs["iterations"], ens.cls, args.cpu_sample_iters)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if \
         (ROOT / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
-    achieved = alg_bytes / (ms / 1e3) / 1e9
-    out = {
+    cells = np.array([ens.batches[c]._problem.n_cells for c in ens.cls])
+    out = summarize(recs, clock_host, ens.cls, cells, ms, total_conv, world, args, max_iter,
+                    e2e_conv / e2e_s, n * 2 * 8 + n * 64, n * 40 + n * 30 * 8, per_it, peaks,
+                    clk.summary(), cpu)
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2e_value, h2d,
+              d2h, per_it, peaks, clocks, cpu):
+    """The JSON line from the host copies of one timed step: rows (status, iterations),
+    the 12-int64 clock record per row, the class and cell count per row."""
+    import rans_uq_b200.workloads as wl
+
+    status, iters = recs["status"], recs["iterations"].astype(np.int64)
+    n = len(status)
+    conv = int(np.sum(status == 0))
+    value = total_conv / (ms / 1e3)
+    lat = (clock[:, 1] - clock[:, 0].min()) / 1e6
+    work = cells * (BYTES_OUTER * iters + BYTES_KRYLOV * clock[:, 2] + BYTES_PRESSURE * clock[:, 3])
+    alg_bytes = float(np.sum(work))
+    # dominant launch: the longest per-class solve kernel of the step (device
+    # globaltimer: first CTA start to last CTA end of that class's rows)
+    per_class = []
+    for c in sorted(set(int(x) for x in cls)):
+        sel = cls == c
+        dur = (clock[sel, 1].max() - clock[sel, 0].min()) / 1e9
+        per_class.append((dur, float(np.sum(work[sel])), c))
+    dom_s, dom_bytes, dom_c = max(per_class)
+    achieved = dom_bytes / dom_s / 1e9
+    plain = None
+    if per_it is not None:
+        plain_s = float(sum(iters[i] * per_it[cls[i]] for i in range(n)))
+        plain = {"solves_per_s": conv / plain_s, "per_iteration_ms": [1e3 * x for x in per_it],
+                 "method": "capped 3000-iteration single-solve launches x each draw's iterations"}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    return {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
@@ -264,29 +284,32 @@ def gpu_arm(args):
         "config": {"workload": "256-draw channel ensemble, Re_tau {182,550,1000} x {128,256,512} cells",
                    "draws_per_gpu": n, "tol": wl.TOL, "alpha_u": wl.ALPHA_U,
                    "precision": args.precision, "l2": "flushed between timed steps",
-                   "parallelism": f"replicas x{world}"},
-        "converged": conv, "statuses": {s: int(np.sum(status == k)) for k, s in
-                                        enumerate(["converged", "unconverged", "diverged",
-                                                   "invalid", "unknown"])},
+                   "max_iter": max_iter, "parallelism": f"replicas x{world}"},
+        "converged": conv,
+        "statuses": {s: int(np.sum(status == k)) for k, s in
+                     enumerate(["converged", "unconverged", "diverged", "invalid", "unknown"])},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "max": float(lat.max())},
-        "iterations": {"mean": float(iters.mean()), "by_class": [int(np.median(iters[ens.cls == c])) for c in range(3)]},
+                       "max": float(lat.max()),
+                       "note": "per-solve completion time from the start of the step (device timer)"},
+        "iterations": {"mean": float(iters.mean()),
+                       "by_class": [int(np.median(iters[cls == c])) for c in range(3)
+                                    if np.any(cls == c)]},
         "plain_fp64": plain,
         "batched_vs_plain": value / plain["solves_per_s"] if plain else None,
-        "e2e": {"value": e2e_conv / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 1,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"),
-                     "unit": "GB/s", "frac": achieved / peaks.get("hbm_gbs", 6650.0),
-                     "traffic": None,
+        "gpu_launches": len(per_class) * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": "measured" if "gpu_name" in peaks else "fallback",
+                     "kernel": f"solveKernel, Re_tau class {dom_c} ({int(np.sum(cls == dom_c))} rows)",
+                     "kernel_ms": dom_s * 1e3, "step_bytes_per_s": alg_bytes / (ms / 1e3),
                      "note": "algorithmic FP64 bytes (1600 B/cell/outer + 360 B/cell/Krylov it + "
-                             "400 B/cell/pressure it); the state is L2/SMEM resident"},
-        "clocks": clk.summary(),
+                             "400 B/cell/pressure it); the state is SMEM/L2 resident, so the "
+                             "bound in practice is per-phase latency, not HBM"},
+        "clocks": clocks,
         "cpu_baseline": cpu,
     }
-    print(json.dumps(out))
-    if world > 1:
-        dist.destroy_process_group()
 
 
 def main():

@@ -1,0 +1,57 @@
+"""bench.py's JSON line from host copies of a step, on synthetic records (no GPU):
+the row decoding of the 40-byte rq_row_out, the contract's keys, and the
+roofline / latency arithmetic."""
+import argparse
+import json
+
+import numpy as np
+
+import bench
+import rans_uq_b200 as rq
+
+
+def fake_step(n=12):
+    cls = np.arange(n) % 3
+    rec = np.zeros(n, dtype=np.dtype([("status", "<i4"), ("iterations", "<i4"),
+                                      ("stalled", "<i4"), ("converged", "<i4"),
+                                      ("loglik", "<f8"), ("final_worst", "<f8"),
+                                      ("contraction_rate", "<f8")]))
+    rec["iterations"] = np.array([100, 200, 400])[cls]
+    rec["status"][-1] = 1
+    raw = np.frombuffer(rec.tobytes(), dtype=np.uint8)  # as copied from the device
+    clock = np.zeros((n, 12), dtype=np.int64)
+    clock[:, 0] = 1_000_000
+    clock[:, 1] = 1_000_000 + np.array([1, 2, 4])[cls] * 1_000_000
+    clock[:, 2] = 10 * rec["iterations"]
+    clock[:, 3] = 5 * rec["iterations"]
+    cells = np.array([384, 768, 1536])[cls]
+    return raw, clock, cls, cells
+
+
+def test_rows_decode_40_byte_records():
+    raw, _, _, _ = fake_step()
+    assert raw.size == 12 * 40
+    recs = rq.rows_from_device_bytes(raw)
+    assert len(recs) == 12 and recs["iterations"][2] == 400 and recs["status"][-1] == 1
+
+
+def test_summary_has_contract_keys():
+    raw, clock, cls, cells = fake_step()
+    recs = rq.rows_from_device_bytes(raw)
+    args = argparse.Namespace(steps=1, warmup=3, precision="fp64")
+    out = bench.summarize(recs, clock, cls, cells, 4.0, 11, 1, args, 300000, 1.5, 100, 200,
+                          [1e-4, 2e-4, 4e-4], {"hbm_gbs": 6552.3, "gpu_name": "x"},
+                          {"sm_mhz": 1900}, None)
+    json.dumps(out)
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config", "e2e",
+                "gpu_launches", "roofline", "clocks", "cpu_baseline"):
+        assert key in out, key
+    assert out["value"] == 11 / 4e-3 and out["converged"] == 11
+    assert out["gpu_launches"] == 3
+    # dominant class 2: 4 rows x 1536 cells x (1600*400 + 360*4000 + 400*2000) over 4 ms
+    want = 4 * 1536 * (1600 * 400 + 360 * 4000 + 400 * 2000) / 4e-3 / 1e9
+    assert abs(out["roofline"]["achieved"] - want) < 1e-9 * want
+    assert out["roofline"]["peak"] == 6552.3
+    assert abs(out["latency_ms"]["max"] - 4.0) < 1e-12
+    assert out["plain_fp64"]["solves_per_s"] > 0 and out["batched_vs_plain"] > 0

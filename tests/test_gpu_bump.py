@@ -1,0 +1,55 @@
+"""GPU parity on the bump-wall geometry (periodic channel over a cosine bump:
+h = 1, L = 9h, W = 4h, top 3.04h; Mesh::makeCurvedChannelPeriodic2D), on a
+coarse 24 x 16 mesh: skewed, non-orthogonal faces, no planar omega balance.
+
+* After N outer iterations the device fields equal the C++ restatement run with
+  the same pressure solver (rtol 1e-9 on the max-norm of each field).
+* With the PCG pressure solver the restatement is bitwise equal to the compiled
+  reference (tests/test_oracle_pins.py), so the device is also compared with the
+  reference itself.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import checker as ck
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-9
+
+
+def field_errors(got, want):
+    out = {}
+    for name in ("Ux", "Uy", "p", "k", "omega", "nuT", "F1"):
+        i = ck.FIELD_NAMES.index(name)
+        scale = max(np.max(np.abs(want.fields[i])), 1e-300)
+        out[name] = float(np.max(np.abs(got[i] - want.fields[i])) / scale)
+    return out
+
+
+@pytest.mark.parametrize("solver,ps", [("AMG", ck.P_AMG), ("PCG", ck.P_PCG),
+                                       ("BiCGSTAB", ck.P_BICGSTAB)])
+@pytest.mark.parametrize("n_iter", [1, 12, 60])
+def test_bump_fields_after_n_iterations(rq, checker, solver, ps, n_iter):
+    case = cases.bump_case(24, 16, max_iter=n_iter, pressure_solver=ps)
+    want = checker.solve(case, "oracle", hist_cap=n_iter)
+    batch = cases.product_batch(rq, case, pressure_solver=solver)
+    res, fields, hist = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]], hist_cap=n_iter)
+    row = res.rows[0]
+    assert row.result.simple_iters == want.iterations
+    assert row.result.status.name == want.status
+    errs = field_errors(fields[0], want)
+    assert max(errs.values()) < RTOL, errs
+    np.testing.assert_allclose(row.result.predictions, want.predictions, rtol=RTOL,
+                               atol=RTOL * np.max(np.abs(want.predictions)))
+
+
+@pytest.mark.skipif(not ck.have("ref"), reason="oracle/_ref not built")
+def test_bump_pcg_matches_reference(rq):
+    case = cases.bump_case(24, 16, max_iter=60, pressure_solver=ck.P_PCG)
+    want = ck.solve(case, "ref")
+    batch = cases.product_batch(rq, case, pressure_solver="PCG")
+    res, fields, _ = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]])
+    assert res.rows[0].result.status.name == want.status
+    errs = field_errors(fields[0], want)
+    assert max(errs.values()) < RTOL, errs
