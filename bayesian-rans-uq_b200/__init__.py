@@ -6,13 +6,13 @@ ForwardBatch, run by hand-written sm_100a CUDA kernels behind a C ABI
 from . import _native
 from .core import (EvaluationResult, EvaluationStatus, FlowBoundaryConditions, ForwardBatch,
                    ForwardBatchResult, ForwardBatchRow, ForwardEvaluationResult, ForwardModel,
-                   InferenceParameterSet, Mesh, ObservationOperator, SST_DEFAULTS, SST_NAMES,
-                   SolverSettings, Vec3, evaluate_multi, evaluate_multi_device,
-                   rows_from_device_bytes)
+                   ForwardServer, InferenceParameterSet, Mesh, ObservationOperator,
+                   SST_DEFAULTS, SST_NAMES, ServedResult, SolverSettings, Vec3, evaluate_multi,
+                   evaluate_multi_device, rows_from_device_bytes)
 
 __all__ = ["EvaluationResult", "EvaluationStatus", "FlowBoundaryConditions", "ForwardBatch",
            "ForwardBatchResult", "ForwardBatchRow", "ForwardEvaluationResult", "ForwardModel",
-           "InferenceParameterSet", "Mesh", "ObservationOperator", "SST_DEFAULTS", "SST_NAMES",
+           "ForwardServer", "InferenceParameterSet", "ServedResult", "Mesh", "ObservationOperator", "SST_DEFAULTS", "SST_NAMES",
            "SolverSettings", "Vec3", "evaluate_multi", "evaluate_multi_device",
            "rows_from_device_bytes", "lib"]
 

@@ -86,6 +86,16 @@ SIGNATURES = {
     "rq_mesh_geometry": ([C.POINTER(MeshDesc), IP, DP], C.c_int),
     "rq_linear_solve": ([C.POINTER(Ldu), DP, C.c_int32, C.c_double, C.c_int32,
                          C.POINTER(SolverResult)], C.c_int),
+    "rq_server_create": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                          C.POINTER(C.c_void_p)], C.c_int),
+    "rq_server_submit": ([C.c_void_p, C.c_int32, DP, C.POINTER(C.c_int64)], C.c_int),
+    "rq_server_poll": ([C.c_void_p, C.c_int64, IP, C.POINTER(RowOut), DP,
+                        C.POINTER(C.c_int64)], C.c_int),
+    "rq_server_wait": ([C.c_void_p, C.c_double, C.POINTER(C.c_int64)], C.c_int),
+    "rq_server_close": ([C.c_void_p], C.c_int),
+    "rq_server_info": ([C.c_void_p, IP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), IP],
+                       C.c_int),
+    "rq_server_destroy": ([C.c_void_p], C.c_int),
 }
 
 _lib = None

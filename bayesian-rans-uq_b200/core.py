@@ -539,6 +539,95 @@ def rows_from_device_bytes(raw: np.ndarray) -> list:
 
 
 @dataclass
+class ServedResult:
+    """Outcome of one served request. `predictions` is None unless the solve
+    converged: failed requests are flagged (status, loglik sentinel), not returned."""
+    ticket: int
+    status: EvaluationStatus
+    loglik: float
+    iterations: int
+    predictions: np.ndarray | None
+    start_ns: int       # GPU global timer at the start / end of the solve
+    end_ns: int
+
+    @property
+    def flagged(self) -> bool:
+        return self.status != EvaluationStatus.Converged
+
+
+class ForwardServer:
+    """Continuous-batching serving loop over several ForwardBatch mesh classes
+    (rq_server_*; no counterpart in the reference, which evaluates fixed batches).
+    A persistent kernel claims requests in submission order as they arrive; each
+    solve runs on its own slot and a slot is reused as soon as its solve retires,
+    so requests submitted while others run overlap with them on the device. The
+    result of a request does not depend on what else is in flight."""
+
+    def __init__(self, batches, capacity: int = 4096, idle_timeout: float = 2.0,
+                 max_slots: int = 0):
+        self._batches = list(batches)  # the mesh classes must outlive the server
+        nb = len(self._batches)
+        handles = (C.c_void_p * nb)(*[b._problem.handle.value for b in self._batches])
+        h = C.c_void_p()
+        N.call("rq_server_create", handles, C.c_int32(nb), C.c_int32(capacity),
+               C.c_double(idle_timeout), C.c_int32(max_slots), C.byref(h))
+        self.handle = h
+        self._no = max(max(b.n_observations() for b in self._batches), 1)
+        self._cls: list[int] = []
+
+    def submit(self, cls: int, theta) -> int:
+        th = np.ascontiguousarray(np.asarray(theta, dtype=np.float64).ravel())
+        if th.size != self._batches[cls].n_parameters():
+            raise ValueError("theta must have the class's n_parameters values")
+        t = C.c_int64()
+        N.call("rq_server_submit", self.handle, C.c_int32(cls), N.dptr(th), C.byref(t))
+        self._cls.append(cls)
+        return int(t.value)
+
+    def poll(self, ticket: int) -> ServedResult | None:
+        done = C.c_int32()
+        row = N.RowOut()
+        pred = np.full(self._no, np.nan)
+        clk = (C.c_int64 * 12)()
+        N.call("rq_server_poll", self.handle, C.c_int64(ticket), C.byref(done), C.byref(row),
+               N.dptr(pred), clk)
+        if not done.value:
+            return None
+        status = EvaluationStatus(row.status)
+        k = self._batches[self._cls[ticket]].n_observations()
+        p = pred[:k].copy() if status == EvaluationStatus.Converged else None
+        return ServedResult(ticket, status, row.loglik, row.iterations, p, clk[0], clk[1])
+
+    def wait(self, timeout: float = 3600.0) -> int:
+        n = C.c_int64()
+        N.call("rq_server_wait", self.handle, C.c_double(timeout), C.byref(n))
+        return int(n.value)
+
+    def close(self) -> None:
+        N.call("rq_server_close", self.handle)
+
+    def info(self) -> dict:
+        slots, lau = C.c_int32(), C.c_int32()
+        sub, comp = C.c_int64(), C.c_int64()
+        N.call("rq_server_info", self.handle, C.byref(slots), C.byref(sub), C.byref(comp),
+               C.byref(lau))
+        return {"slots": slots.value, "submitted": sub.value, "completed": comp.value,
+                "launches": lau.value}
+
+    def destroy(self) -> None:
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            N.lib().rq_server_destroy(h)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+@dataclass
 class ForwardEvaluationResult:
     result: EvaluationResult
     final_worst_measure: float

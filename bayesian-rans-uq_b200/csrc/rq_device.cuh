@@ -84,4 +84,19 @@ struct DevJob {
     int32_t pad;
 };
 
+// Request queue of the serving loop. The host appends requests (jobs[i], with
+// theta, row and prediction slots) to host-mapped memory and then raises
+// *published; CTAs claim them in order through *head (device memory) and raise
+// done[i] when request i's results are in place.
+struct ServeQueue {
+    const DevJob *jobs;      // host-mapped, capacity entries
+    const int *published;    // host-mapped: requests published so far
+    const int *closed;       // host-mapped: 1 = no more requests (drain), 2 = cancel the rest
+    int *done;               // host-mapped: one flag per request
+    int *head;               // device: next request to claim
+    int *idleExits;          // device: CTAs that left after idleNs without work
+    int capacity, pad;
+    long long idleNs;
+};
+
 } // namespace rq

@@ -17,6 +17,12 @@ cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws,
 // CTAs of the variant with the given arena that fit on one SM at once (0: does not fit).
 int solveBlocksPerSM(int block, int cpt, int arenaDoubles);
 bool launchVariantExists(int block, int cpt);
+// The serving loop (serveKernel): grid persistent CTAs of `block` threads (256, 512
+// or 1024) serving q until it is closed and drained, or until q.idleNs passes
+// without a request.
+cudaError_t launchServe(const ServeQueue &q, double *ws, long wsStride, int grid, int block,
+                        int arenaDoubles, cudaStream_t stream);
+int serveBlocksPerSM(int block, int arenaDoubles);
 int normalizeBlock(int block);
 
 } // namespace rq

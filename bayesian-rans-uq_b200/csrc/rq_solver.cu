@@ -66,6 +66,7 @@ struct Shared {
     double q[kMaxProbes], qPrev[kMaxProbes];
     int haveQPrev;
     int job;
+    DevJob jd; // the request being served (a copy out of host-mapped memory)
     int admitted;
     long long innerKrylov, innerPressure; // inner iterations of the solve (work accounting)
     long long stage[8];                   // clock64 cycles per stage (thread 0)
@@ -2196,6 +2197,70 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
 
 } // namespace
 
+// One job on this CTA: class descriptor into shared memory, admission and unpack
+// of theta (InferenceParameterSet::inBounds / unpack), the solve or the
+// InvalidParameters row, then the per-row timing record.
+__device__ void runJob(Shared &S, const DevJob &job, double *ws, double *arena, int arenaDoubles) {
+    long long t0 = 0;
+    if (threadIdx.x == 0)
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    {
+        const int words = sizeof(DevClass) / 4;
+        const int *src = reinterpret_cast<const int *>(job.cls);
+        int *dst = reinterpret_cast<int *>(&S.C);
+        for (int t = threadIdx.x; t < words; t += blockDim.x)
+            dst[t] = src[t];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool ok = true;
+        for (int i = 0; i < 11; ++i)
+            S.coeff[i] = S.C.base[i];
+        for (int a = 0; a < S.C.nActive; ++a) {
+            const int idx = S.C.active[a];
+            const double v = job.theta[a];
+            if (v < S.C.lo[idx] || v > S.C.hi[idx] || isnan(v) || isinf(v))
+                ok = false;
+            S.coeff[idx] = v;
+        }
+        S.admitted = ok;
+        if (ok)
+            carve(S, ws, arena, arenaDoubles);
+    }
+    __syncthreads();
+    if (S.admitted) {
+        runSolve(S, job);
+    } else {
+        if (threadIdx.x == 0) {
+            const double nan = __longlong_as_double(0x7ff8000000000000LL);
+            RowOut o{3, 0, 0, 0, -1e30, nan, nan};
+            *job.row = o;
+        }
+        for (int t = threadIdx.x; t < S.C.nobs; t += blockDim.x)
+            job.pred[t] = __longlong_as_double(0x7ff8000000000000LL);
+        if (job.fields)
+            for (long e = threadIdx.x; e < 11L * S.C.n; e += blockDim.x)
+                job.fields[e] = __longlong_as_double(0x7ff8000000000000LL);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && job.clock) {
+        long long t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        job.clock[0] = t0;
+        job.clock[1] = t1;
+        job.clock[2] = S.admitted ? S.innerKrylov : 0;
+        job.clock[3] = S.admitted ? S.innerPressure : 0;
+        for (int t = 0; t < 8; ++t)
+            job.clock[4 + t] = S.admitted ? S.stage[t] : 0;
+    }
+}
+
+__device__ __forceinline__ long long globalNs() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // One kernel body, instantiated per CTA size so each gets its full register budget.
 template <int NT>
 __global__ void __launch_bounds__(NT) solveKernel(const DevJob *jobs, int njobs, int *nextJob,
@@ -2211,60 +2276,66 @@ __global__ void __launch_bounds__(NT) solveKernel(const DevJob *jobs, int njobs,
         const int j = S.job;
         if (j >= njobs)
             break;
-        const DevJob &job = jobs[j];
-        long long t0 = 0;
-        if (threadIdx.x == 0)
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-        {
-            const int words = sizeof(DevClass) / 4;
-            const int *src = reinterpret_cast<const int *>(job.cls);
-            int *dst = reinterpret_cast<int *>(&S.C);
-            for (int t = threadIdx.x; t < words; t += blockDim.x)
-                dst[t] = src[t];
-        }
-        __syncthreads();
-        // admission and unpack of theta (InferenceParameterSet::inBounds / unpack)
+        runJob(S, jobs[j], ws, arena, arenaDoubles);
+    }
+}
+
+// The serving loop: persistent CTAs claim requests as the host publishes them.
+// Requests live in host-mapped memory (ServeQueue); a CTA claims request h only
+// once h < published, by a compare-and-swap on the device-side head, so no
+// ticket is ever held for an unpublished request. A CTA leaves when the host
+// closes the queue and nothing is left, or after idleNs without work (the host
+// relaunches if requests arrive later); closed = 2 cancels the requests not yet
+// claimed (solves in flight still finish). Results go straight to host-mapped
+// rows; the request's done flag is raised after a system-scope fence.
+template <int NT>
+__global__ void __launch_bounds__(NT) serveKernel(ServeQueue q, double *wsBase, long wsStride,
+                                                  int arenaDoubles) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    Shared &S = *reinterpret_cast<Shared *>(smemRaw);
+    double *arena = reinterpret_cast<double *>(smemRaw + ((sizeof(Shared) + 15) / 16) * 16);
+    double *ws = wsBase + wsStride * blockIdx.x;
+    for (;;) {
         if (threadIdx.x == 0) {
-            bool ok = true;
-            for (int i = 0; i < 11; ++i)
-                S.coeff[i] = S.C.base[i];
-            for (int a = 0; a < S.C.nActive; ++a) {
-                const int idx = S.C.active[a];
-                const double v = job.theta[a];
-                if (v < S.C.lo[idx] || v > S.C.hi[idx] || isnan(v) || isinf(v))
-                    ok = false;
-                S.coeff[idx] = v;
+            int got = -1;
+            const long long idleFrom = globalNs();
+            for (;;) {
+                int closed, pub;
+                asm volatile("ld.acquire.sys.global.s32 %0, [%1];" : "=r"(closed) : "l"(q.closed) : "memory");
+                if (closed >= 2) // cancelled: leave unclaimed requests alone
+                    break;
+                asm volatile("ld.acquire.sys.global.s32 %0, [%1];" : "=r"(pub) : "l"(q.published) : "memory");
+                pub = min(pub, q.capacity);
+                const int h = atomicAdd(q.head, 0);
+                if (h < pub) {
+                    if (atomicCAS(q.head, h, h + 1) == h) {
+                        got = h;
+                        break;
+                    }
+                    continue;
+                }
+                if (closed) // closed and drained
+                    break;
+                if (globalNs() - idleFrom > q.idleNs) {
+                    atomicAdd(q.idleExits, 1);
+                    break;
+                }
+                __nanosleep(4000);
             }
-            S.admitted = ok;
-            if (ok)
-                carve(S, ws, arena, arenaDoubles);
+            S.job = got;
+            if (got >= 0)
+                S.jd = q.jobs[got];
         }
         __syncthreads();
-        if (S.admitted) {
-            runSolve(S, job);
-        } else {
-            if (threadIdx.x == 0) {
-                const double nan = __longlong_as_double(0x7ff8000000000000LL);
-                RowOut o{3, 0, 0, 0, -1e30, nan, nan};
-                *job.row = o;
-            }
-            for (int t = threadIdx.x; t < S.C.nobs; t += blockDim.x)
-                job.pred[t] = __longlong_as_double(0x7ff8000000000000LL);
-            if (job.fields)
-                for (long e = threadIdx.x; e < 11L * S.C.n; e += blockDim.x)
-                    job.fields[e] = __longlong_as_double(0x7ff8000000000000LL);
-        }
+        const int j = S.job;
+        if (j < 0)
+            break;
+        runJob(S, S.jd, ws, arena, arenaDoubles);
+        __threadfence_system();
         __syncthreads();
-        if (threadIdx.x == 0 && job.clock) {
-            long long t1;
-            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-            job.clock[0] = t0;
-            job.clock[1] = t1;
-            job.clock[2] = S.admitted ? S.innerKrylov : 0;
-            job.clock[3] = S.admitted ? S.innerPressure : 0;
-            for (int t = 0; t < 8; ++t)
-                job.clock[4 + t] = S.admitted ? S.stage[t] : 0;
-        }
+        if (threadIdx.x == 0)
+            asm volatile("st.release.sys.global.s32 [%0], %1;" ::"l"(q.done + j), "r"(1) : "memory");
+        __syncthreads();
     }
 }
 
@@ -2272,6 +2343,7 @@ size_t solveSharedBytes() { return ((sizeof(Shared) + 15) / 16) * 16; }
 
 namespace {
 template <int NT> void *kernelFor() { return reinterpret_cast<void *>(&solveKernel<NT>); }
+template <int NT> void *serveFor() { return reinterpret_cast<void *>(&serveKernel<NT>); }
 void *pick(int block, int cpt) {
     if (cpt != 0)
         return nullptr;
@@ -2281,6 +2353,14 @@ void *pick(int block, int cpt) {
     case 256: return kernelFor<256>();
     case 512: return kernelFor<512>();
     case 1024: return kernelFor<1024>();
+    default: return nullptr;
+    }
+}
+void *pickServe(int block) {
+    switch (block) {
+    case 256: return serveFor<256>();
+    case 512: return serveFor<512>();
+    case 1024: return serveFor<1024>();
     default: return nullptr;
     }
 }
@@ -2312,6 +2392,38 @@ cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws,
 int solveBlocksPerSM(int block, int cpt, int arenaDoubles) {
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
     void *fn = pick(block, cpt);
+    if (!fn)
+        return 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+        cudaSuccess)
+        return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, block, smem) != cudaSuccess)
+        return 0;
+    return blocks;
+}
+
+cudaError_t launchServe(const ServeQueue &q, double *ws, long wsStride, int grid, int block,
+                        int arenaDoubles, cudaStream_t stream) {
+    const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
+    void *fn = pickServe(block);
+    if (!fn)
+        return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    ServeQueue qq = q;
+    void *args[] = {&qq, &ws, &wsStride, &arenaDoubles};
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(block), args, smem, stream);
+    if (e != cudaSuccess)
+        return e;
+    return cudaGetLastError();
+}
+
+int serveBlocksPerSM(int block, int arenaDoubles) {
+    const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
+    void *fn = pickServe(block);
     if (!fn)
         return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=

@@ -183,6 +183,34 @@ int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells);
 int rq_linear_solve(const rq_ldu *A, double *x, int32_t max_iter, double tol, int32_t kind,
                     rq_solver_result *result);
 
+/* ---- serving loop (no reference counterpart: the reference evaluates fixed
+   batches only, ForwardBatch.hpp:52-124). A server owns a persistent kernel whose
+   CTAs claim requests as they are submitted, in submission order, each on its own
+   solve slot (per-CTA workspace); a slot is reused as soon as its solve retires.
+   Slots = min(SMs x resident CTAs, max_slots if > 0, what 80% of free device memory
+   holds). Requests and results live in pinned host memory mapped into the device,
+   so a request needs no copy and a result is visible to rq_server_poll as soon as
+   its done flag is raised. The problems must outlive the server. CTAs leave after
+   idle_timeout_s without requests; submit / poll / wait relaunch them when needed.
+   capacity bounds the requests over the server's lifetime. */
+typedef struct rq_server rq_server;
+int rq_server_create(rq_problem *const *problems, int32_t n_problems, int32_t capacity,
+                     double idle_timeout_s, int32_t max_slots, rq_server **out);
+/* theta: the problem's n_active values (host, copied). ticket: request index. */
+int rq_server_submit(rq_server *s, int32_t problem, const double *theta, int64_t *ticket);
+/* done = 1 once the request's row, predictions and clock record (12 int64, as
+   rq_evaluate_multi_device) are final; the optional outputs are filled then. */
+int rq_server_poll(rq_server *s, int64_t ticket, int32_t *done, rq_row_out *row,
+                   double *predictions, int64_t *clock12);
+/* Waits until every submitted request is done or timeout_s passes. */
+int rq_server_wait(rq_server *s, double timeout_s, int64_t *completed);
+/* No more submissions: the kernel drains what was submitted and leaves. */
+int rq_server_close(rq_server *s);
+int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *completed,
+                   int32_t *launches);
+/* Cancels requests not yet claimed, waits for the solves in flight, frees. */
+int rq_server_destroy(rq_server *s);
+
 #ifdef __cplusplus
 }
 #endif

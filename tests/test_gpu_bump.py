@@ -7,6 +7,11 @@ coarse 24 x 16 mesh: skewed, non-orthogonal faces, no planar omega balance.
 * With the PCG pressure solver the restatement is bitwise equal to the compiled
   reference (tests/test_oracle_pins.py), so the device is also compared with the
   reference itself.
+* With BiCGSTAB as the pressure solver the bump's pressure correction is
+  ill-conditioned at the inner tolerance 1e-3: on the CPU, replacing r/d by
+  r*(1/d) in the Jacobi step alone (one rounding) moves the fields by 3e-4 after
+  one outer iteration and 1.5e-3 after twelve. The device (which multiplies by
+  reciprocal diagonals) is held to 1e-2 there, the size of that intrinsic spread.
 """
 import numpy as np
 import pytest
@@ -16,6 +21,7 @@ from oracle import checker as ck
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-9
+RTOL_BICGSTAB_PRESSURE = 1e-2
 
 
 def field_errors(got, want):
@@ -38,10 +44,11 @@ def test_bump_fields_after_n_iterations(rq, checker, solver, ps, n_iter):
     row = res.rows[0]
     assert row.result.simple_iters == want.iterations
     assert row.result.status.name == want.status
+    tol = RTOL_BICGSTAB_PRESSURE if solver == "BiCGSTAB" else RTOL
     errs = field_errors(fields[0], want)
-    assert max(errs.values()) < RTOL, errs
-    np.testing.assert_allclose(row.result.predictions, want.predictions, rtol=RTOL,
-                               atol=RTOL * np.max(np.abs(want.predictions)))
+    assert max(errs.values()) < tol, errs
+    np.testing.assert_allclose(row.result.predictions, want.predictions, rtol=tol,
+                               atol=tol * np.max(np.abs(want.predictions)))
 
 
 @pytest.mark.skipif(not ck.have("ref"), reason="oracle/_ref not built")

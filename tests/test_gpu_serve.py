@@ -1,0 +1,104 @@
+"""The serving loop (rq_server_*): requests of mixed mesh classes submitted while
+others are on the GPU are admitted as slots free up, and each result equals the
+same request evaluated alone by ForwardBatch.evaluate. The tolerance is 1e-12
+relative on predictions and loglik (the serving kernel runs the same per-solve
+code at the same CTA size, so the results are expected to be bitwise equal),
+and status and iteration count must match exactly. Failed requests are flagged
+(status, sentinel loglik, no predictions), not returned.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-12
+
+
+def classes(rq):
+    """Three mesh classes: two small channels and a capped bump (never converges)."""
+    a = cases.product_batch(rq, cases.small_channel())
+    b = cases.product_batch(rq, cases.small_channel(ny=32, max_iter=60000))
+    c = cases.product_batch(rq, cases.bump_case(24, 16, max_iter=150))
+    return [a, b, c]
+
+
+def stream(n=24, seed=7):
+    """Request mix: class per request, theta, with two out-of-bounds (poisoned) rows."""
+    rng = np.random.default_rng(seed)
+    cls = rng.choice(3, size=n, p=[0.45, 0.35, 0.20])
+    theta = np.column_stack([rng.uniform(0.29, 0.33, n), rng.uniform(0.086, 0.094, n)])
+    theta[5] = (0.95, 0.09)   # a1 above its bound 0.8 -> InvalidParameters
+    theta[17] = (0.31, 0.5)   # beta* above its bound 0.2 -> InvalidParameters
+    return cls, theta
+
+
+def alone(batches, cls, theta):
+    return [batches[c].evaluate(theta[i:i + 1]).rows[0].result for i, c in enumerate(cls)]
+
+
+def check_same(served, ref):
+    assert served.status == ref.status, (served.ticket, served.status, ref.status)
+    assert served.iterations == ref.simple_iters
+    if ref.status.name == "Converged":
+        np.testing.assert_allclose(served.predictions, ref.predictions, rtol=RTOL, atol=0)
+        assert abs(served.loglik - ref.loglik) <= RTOL * abs(ref.loglik)
+    else:
+        assert served.flagged and served.predictions is None
+        assert served.loglik == ref.loglik  # the reference's sentinels
+
+
+def test_served_results_equal_alone_results(rq):
+    batches = classes(rq)
+    cls, theta = stream()
+    srv = rq.ForwardServer(batches, capacity=64, idle_timeout=5.0)
+    tickets = []
+    for i in range(len(cls)):
+        tickets.append(srv.submit(int(cls[i]), theta[i]))
+        if i % 4 == 3:
+            time.sleep(0.05)  # arrivals while earlier requests run
+    assert srv.wait(600.0) == len(cls)
+    served = [srv.poll(t) for t in tickets]
+    info = srv.info()
+    srv.destroy()
+    ref = alone(batches, cls, theta)
+    for s, r in zip(served, ref):
+        check_same(s, r)
+    assert served[5].status.name == "InvalidParameters" and served[5].loglik == -1e30
+    assert served[17].status.name == "InvalidParameters"
+    assert all(s.status.name == "Unconverged" for s, c in zip(served, cls) if c == 2)
+    assert info["completed"] == len(cls) and info["slots"] >= 1
+    # requests overlapped on the device: some solve started before another ended
+    spans = sorted((s.start_ns, s.end_ns) for s in served if s.iterations > 0)
+    assert any(b[0] < a[1] for a, b in zip(spans, spans[1:]))
+
+
+def test_idle_exit_and_relaunch(rq):
+    batches = classes(rq)[:1]
+    srv = rq.ForwardServer(batches, capacity=8, idle_timeout=0.2)
+    t0 = srv.submit(0, (0.31, 0.09))
+    assert srv.wait(300.0) == 1
+    time.sleep(1.0)  # the kernel's CTAs leave after 0.2 s without requests
+    t1 = srv.submit(0, (0.30, 0.088))
+    assert srv.wait(300.0) == 2
+    r0, r1 = srv.poll(t0), srv.poll(t1)
+    assert srv.info()["launches"] >= 2
+    srv.destroy()
+    ref = alone(batches, [0, 0], np.array([(0.31, 0.09), (0.30, 0.088)]))
+    check_same(r0, ref[0])
+    check_same(r1, ref[1])
+
+
+def test_close_drains_and_rejects_new_requests(rq):
+    batches = classes(rq)[:1]
+    srv = rq.ForwardServer(batches, capacity=8, idle_timeout=5.0, max_slots=2)
+    ts = [srv.submit(0, (0.30 + 0.005 * i, 0.09)) for i in range(4)]
+    srv.close()
+    with pytest.raises(ValueError):
+        srv.submit(0, (0.31, 0.09))
+    assert srv.wait(300.0) == 4
+    assert srv.info()["slots"] == 2
+    assert all(srv.poll(t) is not None for t in ts)
+    srv.destroy()
