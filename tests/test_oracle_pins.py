@@ -44,8 +44,9 @@ def test_trajectory_bitwise_equal_to_reference(checker, ps):
 
 
 @need_ref
-def test_bump_trajectory_bitwise_equal_to_reference(checker):
-    case = cases.bump_case(24, 16, max_iter=40, pressure_solver=ck.P_PCG)
+@pytest.mark.parametrize("ps", [ck.P_PCG, ck.P_BICGSTAB])
+def test_bump_trajectory_bitwise_equal_to_reference(checker, ps):
+    case = cases.bump_case(24, 16, max_iter=40, pressure_solver=ps)
     a = checker.solve(case, "ref")
     b = checker.solve(case, "oracle")
     np.testing.assert_array_equal(a.fields, b.fields)
