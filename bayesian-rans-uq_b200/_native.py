@@ -86,6 +86,17 @@ SIGNATURES = {
     "rq_mesh_geometry": ([C.POINTER(MeshDesc), IP, DP], C.c_int),
     "rq_linear_solve": ([C.POINTER(Ldu), DP, C.c_int32, C.c_double, C.c_int32,
                          C.POINTER(SolverResult)], C.c_int),
+    "rq_linear_solve_batch": ([C.POINTER(Ldu), C.c_int32, C.POINTER(DP), C.c_int32, C.c_double,
+                               C.c_int32, C.c_int32, C.POINTER(SolverResult)], C.c_int),
+    "rq_linsys_create": ([C.POINTER(Ldu), C.c_int32, C.c_int32, C.c_int32,
+                          C.POINTER(C.c_void_p)], C.c_int),
+    "rq_linsys_solve": ([C.c_void_p, C.c_int32, C.c_double, C.POINTER(DP),
+                         C.POINTER(SolverResult)], C.c_int),
+    "rq_linsys_solve_device": ([C.c_void_p, C.c_int32, C.c_double, C.c_void_p], C.c_int),
+    "rq_linsys_results": ([C.c_void_p, C.POINTER(SolverResult), C.POINTER(DP)], C.c_int),
+    "rq_linsys_info": ([C.c_void_p, IP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), IP],
+                       C.c_int),
+    "rq_linsys_destroy": ([C.c_void_p], C.c_int),
     "rq_server_create": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_int32,
                           C.POINTER(C.c_void_p)], C.c_int),
     "rq_server_submit": ([C.c_void_p, C.c_int32, DP, C.POINTER(C.c_int64)], C.c_int),

@@ -104,3 +104,43 @@ def channel_ensemble(n: int = 256, precision: str = "fp64", first_id: int = 0,
         truth.append(u)
     ids = np.arange(first_id, first_id + n)
     return Ensemble(batches, uniform_design(ids), ids % 3, truth)
+
+
+# ---------------------------------------------------------------- linear systems
+LINEAR_SIZES = (64, 128, 256, 512)
+LINEAR_SEED = 20261011
+
+
+def poisson_system(n: int, seed: int):
+    """Variable-coefficient 5-point Poisson system on an n x n grid of unit cells:
+    face coefficients log-normal (sigma 1), a Dirichlet right edge by diagonal
+    augmentation (twice a log-normal coefficient: the half-cell distance, as the
+    reference adds area/delta for outlet faces, core/tests/test_amg_reuse.cpp:55-63),
+    Neumann elsewhere, right-hand side N(0, 1). Faces: x-faces row by row, then
+    y-faces row by row; cell c = j*n + i."""
+    from .linear import LinearSystem
+
+    rng = np.random.default_rng(seed)
+    idx = np.arange(n * n).reshape(n, n)           # [j, i]
+    own_x, nbr_x = idx[:, :-1].ravel(), idx[:, 1:].ravel()
+    own_y, nbr_y = idx[:-1, :].ravel(), idx[1:, :].ravel()
+    own = np.concatenate([own_x, own_y]).astype(np.int32)
+    nbr = np.concatenate([nbr_x, nbr_y]).astype(np.int32)
+    c = np.exp(rng.standard_normal(len(own)))
+    diag = np.zeros(n * n)
+    np.add.at(diag, own, c)
+    np.add.at(diag, nbr, c)
+    diag[idx[:, -1]] += 2.0 * np.exp(rng.standard_normal(n))
+    source = rng.standard_normal(n * n)
+    return LinearSystem.from_arrays(diag, -c, -c, source, own, nbr)
+
+
+def linear_batch_sizes(count: int = 512, seed: int = LINEAR_SEED) -> np.ndarray:
+    """n of each system, uniform over {64, 128, 256, 512}."""
+    return np.random.default_rng(seed).choice(LINEAR_SIZES, size=count)
+
+
+def linear_workload(count: int = 512, seed: int = LINEAR_SEED, sizes=None):
+    """The batch of `count` systems; system k uses seed + 1 + k."""
+    sizes = linear_batch_sizes(count, seed) if sizes is None else sizes
+    return [poisson_system(int(n), seed + 1 + k) for k, n in enumerate(sizes)]

@@ -178,10 +178,35 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
 /* Mesh geometry as built for the device (nCells x 4: cx, cy, volume, wall distance). */
 int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells);
 
-/* The linear solvers of the forward model on one LDU system (kind RQ_SOLVER_*);
-   x: initial guess in, solution out (host). */
+/* The linear solvers of the forward model on one LDU system, in FP64
+   (ILinearSolver::solve, core/include/LinearSolver.hpp:137-153; kinds RQ_SOLVER_*
+   for the factory names "AMG", "PCG", "BiCGSTAB" of makeSolver, :988-998;
+   "GaussSeidel" returns RQ_E_UNSUPPORTED). x: initial guess in, solution out
+   (host). The AMG is this project's device variant: greedy strength-0.25
+   aggregation of the matrix, damped-Jacobi V-cycle, dense coarsest inverse. */
 int rq_linear_solve(const rq_ldu *A, double *x, int32_t max_iter, double tol, int32_t kind,
                     rq_solver_result *result);
+/* Many systems in one persistent launch (one CTA per system, largest first).
+   x[s]: per-system initial guess in, solution out (host). precision RQ_PREC_MIXED:
+   FP32 PCG corrections inside an FP64 residual-refinement loop (AMG and PCG kinds;
+   BiCGSTAB stays FP64); result iterations count the inner FP32 iterations. */
+int rq_linear_solve_batch(const rq_ldu *systems, int32_t n_systems, double *const *x,
+                          int32_t max_iter, double tol, int32_t kind, int32_t precision,
+                          rq_solver_result *results);
+/* The same with the set-up kept on the device between solves: create builds and
+   uploads every system's operator and hierarchy once; solve runs them from x
+   (or from zero when x is NULL); solve_device queues a zero-start solve on a
+   CUDA stream (void*) and returns; results copies results and solutions back. */
+typedef struct rq_linsys rq_linsys;
+int rq_linsys_create(const rq_ldu *systems, int32_t n_systems, int32_t kind, int32_t precision,
+                     rq_linsys **out);
+int rq_linsys_solve(rq_linsys *L, int32_t max_iter, double tol, double *const *x,
+                    rq_solver_result *results);
+int rq_linsys_solve_device(rq_linsys *L, int32_t max_iter, double tol, void *stream);
+int rq_linsys_results(rq_linsys *L, rq_solver_result *results, double *const *x);
+int rq_linsys_info(const rq_linsys *L, int32_t *n_systems, int64_t *total_rows, int64_t *total_nnz,
+                   int32_t *max_levels);
+int rq_linsys_destroy(rq_linsys *L);
 
 /* ---- serving loop (no reference counterpart: the reference evaluates fixed
    batches only, ForwardBatch.hpp:52-124). A server owns a persistent kernel whose

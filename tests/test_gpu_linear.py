@@ -1,0 +1,113 @@
+"""GPU parity of the standalone linear solves (rq_linear_solve*, rq_linsys_*) on
+variable-coefficient Poisson systems of the linear-solve workload.
+
+* PCG and BiCGSTAB against the compiled reference's own solvers: the device
+  multiplies by reciprocal diagonals and sums dot products as block
+  reductions, so iteration counts may differ by one and solutions agree to
+  1e-7 relative at tol 1e-10 (Jacobi-preconditioned PCG is slow and sensitive).
+* AMG against the oracle's restatement of the same device algorithm (iteration
+  counts within one, solutions 1e-8) and against the reference's AMG (a
+  different smoother: solutions 1e-8 at tol 1e-10).
+* Every converged solution has a true FP64 relative residual below 1.01 x tol.
+* A batch of uneven systems equals the systems solved one at a time, bitwise.
+* The mixed form (FP32 corrections, FP64 refinement) reaches the FP64
+  tolerance and agrees with the FP64 solution to 1e-8.
+"""
+import numpy as np
+import pytest
+
+import rans_uq_b200.linear as lin
+import rans_uq_b200.workloads as wl
+from oracle import checker as ck
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel_residual(s, x):
+    r = s.diag * x
+    np.add.at(r, s.own, s.upper * x[s.nbr])
+    np.add.at(r, s.nbr, s.lower * x[s.own])
+    return float(np.linalg.norm(s.source - r) / np.linalg.norm(s.source))
+
+
+def ref_solve(kind, s, max_iter, lib_kind="ref"):
+    return ck.linear_solve(kind, s.diag, s.upper, s.lower, s.source, s.own, s.nbr,
+                           np.zeros(s.n_cells), max_iter, TOL, lib_kind=lib_kind)
+
+
+@pytest.mark.skipif(not ck.have("ref"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name,kind,n", [("PCG", 1, 16), ("PCG", 1, 40), ("BiCGSTAB", 2, 16),
+                                         ("BiCGSTAB", 2, 40)])
+def test_krylov_matches_reference(name, kind, n):
+    s = wl.poisson_system(n, 11 + n)
+    xr, ir = ref_solve(kind, s, 2000)
+    x = np.zeros(s.n_cells)
+    r = lin.make_solver(name).solve(s, x, 2000, TOL)
+    assert r.converged and ir["converged"]
+    assert abs(r.iterations - ir["iterations"]) <= 1
+    assert abs(r.initial_res - ir["initial_res"]) <= 1e-12 * ir["initial_res"]
+    assert ck.rel_err(x, xr) < 1e-7
+    assert rel_residual(s, x) < 1.01 * TOL
+
+
+@pytest.mark.parametrize("n", [8, 32, 64, 100])
+def test_amg_matches_oracle_and_reference(n):
+    s = wl.poisson_system(n, 100 + n)
+    xo, io = ref_solve(10, s, 500, lib_kind="oracle")
+    x = np.zeros(s.n_cells)
+    r = lin.make_solver("AMG").solve(s, x, 500, TOL)
+    assert r.converged and io["converged"]
+    assert abs(r.iterations - io["iterations"]) <= 1
+    assert ck.rel_err(x, xo) < 1e-8
+    assert rel_residual(s, x) < 1.01 * TOL
+    if ck.have("ref"):
+        xr, ir = ref_solve(0, s, 500)
+        assert ck.rel_err(x, xr) < 1e-8
+
+
+def test_batch_equals_single_solves():
+    sizes = [64, 16, 100, 8, 33]
+    systems = [wl.poisson_system(n, 7 + k) for k, n in enumerate(sizes)]
+    res, xs = lin.solve_batch(systems, kind="AMG", max_iter=500, tol=TOL)
+    for s, r, x in zip(systems, res, xs):
+        x1 = np.zeros(s.n_cells)
+        r1 = lin.make_solver("AMG").solve(s, x1, 500, TOL)
+        assert r.iterations == r1.iterations and r.converged
+        np.testing.assert_array_equal(x, x1)
+
+
+@pytest.mark.parametrize("kind", ["AMG", "PCG"])
+def test_mixed_precision_reaches_fp64_tolerance(kind):
+    systems = [wl.poisson_system(n, 50 + n) for n in (24, 64)]
+    res64, x64 = lin.solve_batch(systems, kind=kind, precision="fp64", max_iter=4000, tol=TOL)
+    res32, x32 = lin.solve_batch(systems, kind=kind, precision="mixed", max_iter=4000, tol=TOL)
+    for s, r, x, xr in zip(systems, res32, x32, x64):
+        assert r.converged
+        assert rel_residual(s, x) < 1.01 * TOL
+        assert ck.rel_err(x, xr) < 1e-8
+
+
+def test_device_resident_batch_repeats_and_edge_cases():
+    systems = [wl.poisson_system(n, 3 + n) for n in (16, 48)]
+    zero = wl.poisson_system(8, 1)
+    zero.source = np.zeros(zero.n_cells)
+    one = lin.LinearSystem.from_arrays([2.0], [], [], [3.0], np.zeros(0, np.int32),
+                                       np.zeros(0, np.int32))
+    batch = lin.LinearBatch(systems + [zero, one], kind="AMG")
+    r1, x1 = batch.solve(500, TOL)
+    r2, x2 = batch.solve(500, TOL)
+    for a, b in zip(x1, x2):
+        np.testing.assert_array_equal(a, b)
+    batch.solve_device(500, TOL)
+    r3, x3 = batch.results(with_x=True)
+    for a, b in zip(x1, x3):
+        np.testing.assert_array_equal(a, b)
+    assert r1[2].converged and r1[2].iterations == 0 and np.all(x1[2] == 0)  # zero right-hand side
+    assert r1[3].converged and abs(x1[3][0] - 1.5) < 1e-15                   # one cell: the inverse
+    assert batch.info()["systems"] == 4
+    batch.destroy()
+    # a zero iteration cap leaves x at the initial guess, not converged
+    x = np.zeros(systems[0].n_cells)
+    r = lin.make_solver("PCG").solve(systems[0], x, 0, TOL)
+    assert not r.converged and r.iterations == 0 and np.all(x == 0)
