@@ -48,6 +48,11 @@ def parse():
                     help="cap on outer iterations per draw (profiling runs only; the "
                          "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "linear"],
+                    help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
+                         "variable-coefficient Poisson systems by AMG-PCG")
+    ap.add_argument("--systems", type=int, default=512)
+    ap.add_argument("--cpu-sample-systems", type=int, default=12)
     return ap.parse_args()
 
 
@@ -312,9 +317,157 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
     }
 
 
+# ---------------------------------------------------------------- linear-solve workload
+LIN_METRIC = "converged AMG-PCG linear solves/s, 512 Poisson systems n^2, n in {64..512}, tol 1e-10"
+LIN_TOL, LIN_MAX_ITER = 1e-10, 500
+
+
+def lin_bytes_per_iteration(n_rows, nnz, precision):
+    """Algorithmic bytes of one AMG-PCG iteration on level 0 (coarse levels not counted):
+    5 CSR passes (matvec, 4 in the V-cycle) and ~32 vector passes."""
+    vb, cb = (8, 12) if precision == "fp64" else (4, 8)
+    return 5 * (cb * nnz + 4 * n_rows) + 32 * vb * n_rows
+
+
+def linear_cpu_sample(systems, sample):
+    """The reference's AMGSolver::solve (oracle/_ref) on a seeded sample of the
+    systems, one thread per system on all host cores; returns (solves/s for the
+    whole batch extrapolated by rows x iterations, description)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import checker as ck
+
+    rng = np.random.default_rng(7)
+    idx = sorted(rng.choice(len(systems), size=min(sample, len(systems)), replace=False))
+    cores = os.cpu_count() or 1
+
+    def run(k):
+        s = systems[k]
+        t = time.perf_counter()
+        _, info = ck.linear_solve(0, s.diag, s.upper, s.lower, s.source, s.own, s.nbr,
+                                  np.zeros(s.n_cells), LIN_MAX_ITER, LIN_TOL, lib_kind="ref")
+        return time.perf_counter() - t, info["iterations"]
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        out = list(ex.map(run, idx))
+    wall = time.perf_counter() - t0
+    per_row = sum(t for t, _ in out) / sum(systems[k].n_cells for k in idx)
+    total_cpu = per_row * sum(s.n_cells for s in systems)
+    value = len(systems) / (total_cpu / cores)
+    return value, cores, (f"reference AMGSolver::solve (oracle/_ref, g++ -O2) on {len(idx)} of "
+                          f"{len(systems)} systems ({wall:.1f} s wall on {cores} threads); "
+                          f"seconds per row x all rows / {cores} cores (extrapolated)")
+
+
+def linear_arm(args):
+    import rans_uq_b200.linear as lin
+    import rans_uq_b200.workloads as wl
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    systems = wl.linear_workload(args.systems, seed=wl.LINEAR_SEED + 1000 * rank)
+    config = {"workload": f"{args.systems} variable-coefficient 5-point Poisson systems, n x n, "
+                          "n uniform in {64,128,256,512}, log-normal faces, Dirichlet edge",
+              "systems_per_gpu": args.systems, "tol": LIN_TOL, "solver": "AMG-PCG",
+              "precision": args.precision, "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, cores, sample = linear_cpu_sample(systems, args.cpu_sample_systems)
+        print(json.dumps({"impl": "reference", "metric": LIN_METRIC, "value": v,
+                          "unit": "systems/s", "n_gpus": args.gpus, "steps": args.steps,
+                          "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "config": config,
+                          "cpu_baseline": {"value": v, "unit": "systems/s", "cores": cores,
+                                           "kind": "reference", "sample": sample},
+                          "e2e": {"value": v, "unit": "systems/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+    import torch
+    import rans_uq_b200.replicas as rp
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.perf_counter()
+    batch = lin.LinearBatch(systems, kind="AMG", precision=args.precision)
+    setup_s = time.perf_counter() - t0
+    info = batch.info()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        batch.solve_device(LIN_MAX_ITER, LIN_TOL, stream.cuda_stream)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.solve_device(LIN_MAX_ITER, LIN_TOL, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    res, _ = batch.results()
+    iters = np.array([r.iterations for r in res])
+    conv = int(sum(r.converged for r in res))
+    ms, total_conv, _ = rp.reduce_step(float(np.median(times)), conv, device=dev)
+    batch.destroy()
+    # end to end through the one-shot public call: host arrays in and out, host set-up included
+    t0 = time.perf_counter()
+    res_e2e, xs = lin.solve_batch(systems, kind="AMG", precision=args.precision,
+                                  max_iter=LIN_MAX_ITER, tol=LIN_TOL)
+    e2e_s = time.perf_counter() - t0
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    nnz = np.array([s.n_cells + 2 * s.n_if for s in systems])
+    rows = np.array([s.n_cells for s in systems])
+    alg = float(np.sum(iters * lin_bytes_per_iteration(rows, nnz, args.precision)))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if \
+        (ROOT / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg / (ms / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+        v, cores, sample = linear_cpu_sample(systems, args.cpu_sample_systems)
+        cpu = {"value": v, "unit": "systems/s", "cores": cores, "kind": "reference",
+               "sample": sample}
+    h2d = int(sum(8 * (2 * s.n_cells + 2 * s.n_if) + 8 * s.n_if for s in systems))
+    print(json.dumps({
+        "metric": LIN_METRIC, "value": total_conv / (ms / 1e3), "unit": "systems/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": dict(config, l2="flushed between timed steps; working set above L2"),
+        "converged": conv, "iterations": {"mean": float(iters.mean()), "max": int(iters.max()),
+                                          "by_n": {int(n): float(iters[rows == n * n].mean())
+                                                   for n in wl.LINEAR_SIZES if np.any(rows == n * n)}},
+        "setup_s": setup_s, "rows": info["rows"], "nnz_all_levels": info["nnz"],
+        "e2e": {"value": sum(r.converged for r in res_e2e) / e2e_s, "unit": "systems/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(8 * rows.sum() + 24 * len(systems)),
+                "note": "one-shot rq_linear_solve_batch: host set-up, upload, solve, download"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None, "kernel": "linKernel<512>",
+                     "note": "algorithmic level-0 bytes per AMG-PCG iteration (5 CSR passes + 32 "
+                             "vector passes) x iterations; coarse levels not counted"},
+        "cpu_baseline": cpu,
+    }))
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload == "linear":
+        linear_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

@@ -365,12 +365,15 @@ struct Amg {
     // AMGSolver applies to its aggregation (LinearSolver.hpp:924-941)
     bool needRefresh = true;
     int itersAfterRefresh = -1;
+    // smoother weight and coarse-correction scale: the pressure hierarchy uses
+    // 0.6 and 1; the standalone linear solves 0.75 and 1.7 (over-correction of
+    // the piecewise-constant prolongation)
+    double w = 0.6, alpha = 1.0;
     int levels() const { return static_cast<int>(lev.size()); }
 };
 
 static const int AMG_MIN_COARSE = 32;  // the reference stops at 50 (LinearSolver.hpp:664); 32 = one warp
 static const int AMG_MAX_LEVELS = 20;  // :663
-static const double AMG_JACOBI_W = 0.6;
 static const int AMG_SWEEPS = 2;
 
 static Csr lduCsr(int n, const std::vector<int> &own, const std::vector<int> &nbr, int nf,
@@ -459,6 +462,57 @@ static void aggregate(const Csr &A, std::vector<int> &map, int &nc) {
             }
         }
         map[i] = bestAgg;
+    }
+}
+
+// Aggregation of the standalone linear systems on the device (the product's
+// rq_linsys.cpp): the reference's greedy pass (LinearSolver.hpp:535-575) with
+// row-relative strength |a_ij| >= 0.25 max_k |a_ik|, singleton seeds merged
+// into their strongest neighbour's aggregate, ids renumbered by first use.
+static void aggregateLinear(const Csr &A, std::vector<int> &map, int &nc) {
+    const int n = A.n;
+    map.assign(n, -1);
+    int groups = 0;
+    for (int i = 0; i < n; ++i) {
+        if (map[i] >= 0)
+            continue;
+        const int g = groups++;
+        map[i] = g;
+        double rowMax = 0.0;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+            if (A.col[k] != i)
+                rowMax = std::max(rowMax, std::abs(A.val[k]));
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            const int c = A.col[k];
+            if (c != i && map[c] < 0 && rowMax > 0.0 && std::abs(A.val[k]) >= 0.25 * rowMax)
+                map[c] = g;
+        }
+    }
+    std::vector<int> count(groups, 0);
+    for (int i = 0; i < n; ++i)
+        ++count[map[i]];
+    for (int i = 0; i < n; ++i) {
+        if (count[map[i]] != 1)
+            continue;
+        double best = 0.0;
+        int j = -1;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+            if (A.col[k] != i && std::abs(A.val[k]) > best) {
+                best = std::abs(A.val[k]);
+                j = A.col[k];
+            }
+        if (j < 0)
+            continue;
+        --count[map[i]];
+        map[i] = map[j];
+        ++count[map[j]];
+    }
+    std::vector<int> id(groups, -1);
+    nc = 0;
+    for (int i = 0; i < n; ++i) {
+        if (id[map[i]] < 0)
+            id[map[i]] = nc++;
+        map[i] = id[map[i]];
     }
 }
 
@@ -606,11 +660,11 @@ static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
     }
     Vec r(n);
     for (int i = 0; i < n; ++i)
-        x[i] = AMG_JACOBI_W * b[i] / A.dg[i];
+        x[i] = h.w * b[i] / A.dg[i];
     for (int s = 1; s < AMG_SWEEPS; ++s) {
         csrResidual(A, x, b, r);
         for (int i = 0; i < n; ++i)
-            x[i] += AMG_JACOBI_W * r[i] / A.dg[i];
+            x[i] += h.w * r[i] / A.dg[i];
     }
     csrResidual(A, x, b, r);
     const AmgLevel &fl = h.lev[l];
@@ -619,11 +673,11 @@ static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
         bc[fl.agg[i]] += r[i];
     vcycle(h, l + 1, bc, xc);
     for (int i = 0; i < n; ++i)
-        x[i] += xc[fl.agg[i]];
+        x[i] += h.alpha * xc[fl.agg[i]];
     for (int s = 0; s < AMG_SWEEPS; ++s) {
         csrResidual(A, x, b, r);
         for (int i = 0; i < n; ++i)
-            x[i] += AMG_JACOBI_W * r[i] / A.dg[i];
+            x[i] += h.w * r[i] / A.dg[i];
     }
 }
 
@@ -1757,6 +1811,8 @@ int orc_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,
             r = bicgstab(A, xv, max_iter, tol);
         } else if (kind == 10) {
             Amg h;
+            h.w = 0.75;
+            h.alpha = 1.7;
             AmgLevel l0;
             l0.A = lduCsr(n, ow, nb, nif, A.d, A.up, A.lo, &h.upPos, &h.loPos);
             l0.dpos.resize(n);
@@ -1769,7 +1825,7 @@ int orc_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,
                     break;
                 std::vector<int> map;
                 int nc = 0;
-                aggregate(fine.A, map, nc);
+                aggregateLinear(fine.A, map, nc);
                 if (nc == 0 || nc >= fine.A.n)
                     break;
                 AmgLevel coarse;
