@@ -544,7 +544,7 @@ class ServedResult:
     converged: failed requests are flagged (status, loglik sentinel), not returned."""
     ticket: int
     status: EvaluationStatus
-    loglik: float
+    log_lik: float
     iterations: int
     predictions: np.ndarray | None
     start_ns: int       # GPU global timer at the start / end of the solve

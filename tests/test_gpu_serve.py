@@ -44,10 +44,10 @@ def check_same(served, ref):
     assert served.iterations == ref.simple_iters
     if ref.status.name == "Converged":
         np.testing.assert_allclose(served.predictions, ref.predictions, rtol=RTOL, atol=0)
-        assert abs(served.loglik - ref.loglik) <= RTOL * abs(ref.loglik)
+        assert abs(served.log_lik - ref.log_lik) <= RTOL * abs(ref.log_lik)
     else:
         assert served.flagged and served.predictions is None
-        assert served.loglik == ref.loglik  # the reference's sentinels
+        assert served.log_lik == ref.log_lik  # the reference's sentinels
 
 
 def test_served_results_equal_alone_results(rq):
@@ -66,7 +66,7 @@ def test_served_results_equal_alone_results(rq):
     ref = alone(batches, cls, theta)
     for s, r in zip(served, ref):
         check_same(s, r)
-    assert served[5].status.name == "InvalidParameters" and served[5].loglik == -1e30
+    assert served[5].status.name == "InvalidParameters" and served[5].log_lik == -1e30
     assert served[17].status.name == "InvalidParameters"
     assert all(s.status.name == "Unconverged" for s, c in zip(served, cls) if c == 2)
     assert info["completed"] == len(cls) and info["slots"] >= 1
