@@ -24,5 +24,8 @@ cudaError_t launchServe(const ServeQueue &q, double *ws, long wsStride, int grid
                         int arenaDoubles, cudaStream_t stream);
 int serveBlocksPerSM(int block, int arenaDoubles);
 int normalizeBlock(int block);
+// Posterior weights (rq_stats.cu): one CTA; out = {max, sum of exp, non-finite count}.
+cudaError_t launchWeights(const double *ll, const double *lq, int64_t n, double *w, double *out,
+                          cudaStream_t stream);
 
 } // namespace rq

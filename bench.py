@@ -278,7 +278,8 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
     plain = None
     if per_it is not None:
         plain_s = float(sum(iters[i] * per_it[cls[i]] for i in range(n)))
-        plain = {"solves_per_s": conv / plain_s, "per_iteration_ms": [1e3 * x for x in per_it],
+        plain = {"solves_per_s": conv / plain_s if plain_s > 0 else 0.0,
+                 "per_iteration_ms": [1e3 * x for x in per_it],
                  "method": "capped 3000-iteration single-solve launches x each draw's iterations"}
     hbm = peaks.get("hbm_gbs", 6650.0)
     return {
@@ -300,7 +301,7 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
                        "by_class": [int(np.median(iters[cls == c])) for c in range(3)
                                     if np.any(cls == c)]},
         "plain_fp64": plain,
-        "batched_vs_plain": value / plain["solves_per_s"] if plain else None,
+        "batched_vs_plain": value / plain["solves_per_s"] if plain and plain["solves_per_s"] else None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": len(per_class) * args.steps,

@@ -208,6 +208,20 @@ int rq_linsys_info(const rq_linsys *L, int32_t *n_systems, int64_t *total_rows, 
                    int32_t *max_levels);
 int rq_linsys_destroy(rq_linsys *L);
 
+/* Normalised importance weights of a finite posterior, in FP64 on the GPU
+   (cfdr.statistics.posterior_weights, rans-uq/python/cfdr/statistics.py:217-232):
+   w_i = exp(l_i - log_q_i - m) / sum_j exp(l_j - log_q_j - m), m the maximum;
+   log_q may be NULL (an independent prior design). A non-finite log-likelihood
+   is RQ_E_INVALID, as the reference raises. log_evidence (optional) receives
+   m + log(sum), the log-sum-exp. */
+int rq_posterior_weights(const double *loglik, const double *log_q, int64_t n, double *weights,
+                         double *log_evidence);
+/* The same on device buffers on a stream, queued without waiting; out3_dev
+   receives {m, sum, number of non-finite terms} (weights are unset when the count
+   is nonzero). */
+int rq_posterior_weights_device(const double *loglik_dev, const double *log_q_dev, int64_t n,
+                                double *weights_dev, double *out3_dev, void *stream);
+
 /* ---- serving loop (no reference counterpart: the reference evaluates fixed
    batches only, ForwardBatch.hpp:52-124). A server owns a persistent kernel whose
    CTAs claim requests as they are submitted, in submission order, each on its own

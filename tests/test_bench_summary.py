@@ -55,3 +55,14 @@ def test_summary_has_contract_keys():
     assert out["roofline"]["peak"] == 6552.3
     assert abs(out["latency_ms"]["max"] - 4.0) < 1e-12
     assert out["plain_fp64"]["solves_per_s"] > 0 and out["batched_vs_plain"] > 0
+
+
+def test_summary_when_nothing_converges():
+    raw, clock, cls, cells = fake_step()
+    rec = rq.rows_from_device_bytes(raw).copy()
+    rec["status"][:] = 1
+    args = argparse.Namespace(steps=1, warmup=3, precision="fp64")
+    out = bench.summarize(rec, clock, cls, cells, 4.0, 0, 1, args, 2000, 0.0, 100, 200,
+                          [1e-4, 2e-4, 4e-4], {"hbm_gbs": 6552.3}, {}, None)
+    assert out["value"] == 0.0 and out["batched_vs_plain"] is None
+    assert out["roofline"]["peak_source"] == "fallback"
