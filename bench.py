@@ -274,6 +274,18 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
         dur = (clock[sel, 1].max() - clock[sel, 0].min()) / 1e9
         per_class.append((dur, float(np.sum(work[sel])), c))
     dom_s, dom_bytes, dom_c = max(per_class)
+    names = ["setup", "closure", "momentum", "p_assembly", "p_solve", "amg_refresh", "turbulence",
+             "bookkeeping"]
+    stages = {}
+    for c in sorted(set(int(x) for x in cls)):
+        sel = (cls == c) & (iters > 0)
+        if not np.any(sel):
+            continue
+        cyc = clock[sel, 4:12].astype(np.float64).sum(0)
+        stages[str(c)] = {"share": {k: round(float(v / max(cyc.sum(), 1.0)), 4)
+                                    for k, v in zip(names, cyc)},
+                          "krylov_per_outer": float(clock[sel, 2].sum() / iters[sel].sum()),
+                          "pressure_per_outer": float(clock[sel, 3].sum() / iters[sel].sum())}
     achieved = dom_bytes / dom_s / 1e9
     plain = None
     if per_it is not None:
@@ -300,6 +312,7 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
         "iterations": {"mean": float(iters.mean()),
                        "by_class": [int(np.median(iters[cls == c])) for c in range(3)
                                     if np.any(cls == c)]},
+        "stages_by_class": stages,
         "plain_fp64": plain,
         "batched_vs_plain": value / plain["solves_per_s"] if plain and plain["solves_per_s"] else None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
