@@ -97,6 +97,8 @@ SIGNATURES = {
     "rq_linsys_info": ([C.c_void_p, IP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), IP],
                        C.c_int),
     "rq_linsys_destroy": ([C.c_void_p], C.c_int),
+    "rq_evaluate_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+                            C.c_int),
     "rq_posterior_weights": ([DP, DP, C.c_int64, DP, DP], C.c_int),
     "rq_posterior_weights_device": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                      C.c_void_p], C.c_int),

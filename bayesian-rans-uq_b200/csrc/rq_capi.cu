@@ -1314,6 +1314,36 @@ int rq_server_destroy(rq_server *s) {
     return guarded([&] { delete s; });
 }
 
+int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_dev,
+                        double *predictions_dev, void *stream) {
+    return guarded([&] {
+        if (!p || !theta_dev || !row_dev || (p->nObs > 0 && !predictions_dev))
+            throw std::invalid_argument("null argument");
+        const long need = static_cast<long>(p->cls.wsDoubles);
+        if (need > rq::noAllocScratchDoubles())
+            throw std::invalid_argument(
+                "this mesh class needs " + std::to_string(need) +
+                " doubles of solve scratch; the allocation-free entry point holds at most " +
+                std::to_string(rq::noAllocScratchDoubles()) +
+                " (8 MiB, about 17000 cells): use rq_evaluate_batch for larger meshes");
+        rq::DevJob job{};
+        job.cls = p->dCls.as<rq::DevClass>();
+        job.theta = theta_dev;
+        job.row = reinterpret_cast<rq::RowOut *>(row_dev);
+        job.pred = predictions_dev;
+        // shared-memory arena as the batch path sizes it for one class (no containers)
+        const long shared = static_cast<long>(rq::solveSharedBytes());
+        const long optin = maxSmemOptin();
+        long bytes = p->arenaKb > 0 ? std::min<long>(p->arenaKb * 1024L, optin - shared)
+                     : p->mesh.n <= 768 ? (optin / 2 - 1024) - shared
+                                        : optin - shared;
+        bytes = std::max<long>(0, std::min(bytes, need * 8));
+        const int arena = static_cast<int>(bytes / 8 / 32 * 32);
+        check(rq::launchSolveNoAlloc(job, p->block, arena, static_cast<cudaStream_t>(stream)),
+              "allocation-free solve launch");
+    });
+}
+
 int rq_posterior_weights(const double *loglik, const double *log_q, int64_t n, double *weights,
                          double *log_evidence) {
     return guarded([&] {

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <mutex>
+
 #include <type_traits>
 
 namespace rq {
@@ -2339,6 +2341,26 @@ __global__ void __launch_bounds__(NT) serveKernel(ServeQueue q, double *wsBase, 
     }
 }
 
+// ---------------------------------------------------------------- allocation-free single solve
+// Workspace of rq_evaluate_noalloc: one solve's scratch in a fixed device array
+// that the module owns, so that the call itself needs no device allocation. It
+// lives on every GPU that loads this library until the process exits.
+constexpr long kNoAllocScratchDoubles = 1L << 20; // 8 MiB
+static __device__ __align__(256) double g_noallocScratch[kNoAllocScratchDoubles];
+
+// One job passed by value (no job array, no queue counter), solved by one CTA in
+// the scratch array.
+template <int NT>
+__global__ void __launch_bounds__(NT) solveOneKernel(DevJob job, double *ws, int arenaDoubles) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    Shared &S = *reinterpret_cast<Shared *>(smemRaw);
+    double *arena = reinterpret_cast<double *>(smemRaw + ((sizeof(Shared) + 15) / 16) * 16);
+    if (threadIdx.x == 0)
+        S.jd = job;
+    __syncthreads();
+    runJob(S, S.jd, ws, arena, arenaDoubles);
+}
+
 size_t solveSharedBytes() { return ((sizeof(Shared) + 15) / 16) * 16; }
 
 namespace {
@@ -2433,6 +2455,68 @@ int serveBlocksPerSM(int block, int arenaDoubles) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, block, smem) != cudaSuccess)
         return 0;
     return blocks;
+}
+
+long noAllocScratchDoubles() { return kNoAllocScratchDoubles; }
+
+namespace {
+template <int NT> void *oneFor() { return reinterpret_cast<void *>(&solveOneKernel<NT>); }
+void *pickOne(int block) {
+    switch (block) {
+    case 64: return oneFor<64>();
+    case 128: return oneFor<128>();
+    case 256: return oneFor<256>();
+    case 512: return oneFor<512>();
+    case 1024: return oneFor<1024>();
+    default: return nullptr;
+    }
+}
+constexpr int kMaxDevices = 64;
+std::mutex g_scratchMu;
+double *g_scratchAddr[kMaxDevices] = {};
+} // namespace
+
+// The device address of the scratch array on the current device, looked up once
+// per device with cudaGetSymbolAddress (the host-side name of a __device__
+// array is only a stand-in, not an address a kernel may use).
+cudaError_t noAllocScratch(double **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    if (dev < 0 || dev >= kMaxDevices)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_scratchMu);
+    if (!g_scratchAddr[dev]) {
+        double *p = nullptr;
+        e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noallocScratch);
+        if (e != cudaSuccess)
+            return e;
+        g_scratchAddr[dev] = p;
+    }
+    *out = g_scratchAddr[dev];
+    return cudaSuccess;
+}
+
+cudaError_t launchSolveNoAlloc(const DevJob &job, int block, int arenaDoubles,
+                               cudaStream_t stream) {
+    double *ws = nullptr;
+    cudaError_t e = noAllocScratch(&ws);
+    if (e != cudaSuccess)
+        return e;
+    void *fn = pickOne(block);
+    if (!fn)
+        return cudaErrorInvalidConfiguration;
+    const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess)
+        return e;
+    DevJob j = job;
+    void *args[] = {&j, &ws, &arenaDoubles};
+    e = cudaLaunchKernel(fn, dim3(1), dim3(block), args, smem, stream);
+    if (e != cudaSuccess)
+        return e;
+    return cudaGetLastError();
 }
 
 } // namespace rq

@@ -208,6 +208,23 @@ int rq_linsys_info(const rq_linsys *L, int32_t *n_systems, int64_t *total_rows, 
                    int32_t *max_levels);
 int rq_linsys_destroy(rq_linsys *L);
 
+/* One draw without any device allocation (no counterpart in the reference). For
+   callers that must not allocate GPU memory once they are running: a sampler
+   embedded in a host application whose memory budget was fixed at start-up, or
+   a latency-bound loop where cudaMalloc would stall the device to synchronise.
+   theta_dev (n_active doubles), row_dev (one rq_row_out) and predictions_dev
+   (n_obs doubles) are the caller's device buffers; the solve's scratch is a fixed
+   8 MiB array in the library (held on every GPU that loads it until exit), so
+   mesh classes needing more (above about 17000 cells) are rejected with
+   RQ_E_INVALID. The problem must come from rq_problem_create (which does
+   allocate). Queued on `stream` (cudaStream_t as void*) without waiting. The
+   first call on a device looks the scratch address up; make that first call
+   before any stream capture. Nothing in the scratch needs to start at zero (a
+   solve writes every array before reading it), but every call shares it:
+   calls whose solves overlap on the GPU race and corrupt each other. */
+int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_dev,
+                        double *predictions_dev, void *stream);
+
 /* Normalised importance weights of a finite posterior, in FP64 on the GPU
    (cfdr.statistics.posterior_weights, rans-uq/python/cfdr/statistics.py:217-232):
    w_i = exp(l_i - log_q_i - m) / sum_j exp(l_j - log_q_j - m), m the maximum;
