@@ -48,9 +48,12 @@ def parse():
                     help="cap on outer iterations per draw (profiling runs only; the "
                          "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "linear"],
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "linear", "serve"],
                     help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
-                         "variable-coefficient Poisson systems by AMG-PCG")
+                         "variable-coefficient Poisson systems by AMG-PCG; serve: open-loop "
+                         "Poisson arrivals of channel requests to the serving loop")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--requests", type=int, default=96, help="serve: requests in the stream")
     ap.add_argument("--systems", type=int, default=512)
     ap.add_argument("--cpu-sample-systems", type=int, default=12)
     return ap.parse_args()
@@ -477,8 +480,101 @@ def linear_arm(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------- serving workload
+SERVE_METRIC = "served converged RANS-SST solves/s with p50/p99 request latency (open-loop arrivals)"
+
+
+def student_t_theta(ids, seed=20261012, center=(0.324, 0.0968), std=(0.004, 0.0012), rho=0.3,
+                    nu=4.0):
+    """Seeded bivariate Student-t draws, the construction of the reference's importance
+    proposal (docs/figures/calibration_coverage.py:165-180) with the serving stream's
+    centre, scales and correlation."""
+    import rans_uq_b200.workloads as wl
+
+    cov = np.array([[std[0] ** 2, rho * std[0] * std[1]], [rho * std[0] * std[1], std[1] ** 2]])
+    chol = np.linalg.cholesky(cov)
+    out = []
+    for i in ids:
+        rng = wl.sample_rng(seed, int(i), "student-t-proposal")
+        z, chi2 = rng.standard_normal(2), rng.chisquare(nu)
+        out.append(np.asarray(center) + chol @ z * np.sqrt(nu / chi2))
+    return np.array(out)
+
+
+def serve_arm(args):
+    import torch
+    import rans_uq_b200 as rq
+    import rans_uq_b200.workloads as wl
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    ens = wl.channel_ensemble(3)
+    R = args.requests
+    rng = np.random.default_rng(20261013)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, R))
+    cls = rng.integers(0, 3, R)
+    theta = student_t_theta(range(R))
+    poisoned = rng.random(R) < 0.05
+    theta[poisoned, 0] = 0.95  # a1 above its bound: must come back flagged, not returned
+    srv = rq.ForwardServer(ens.batches, capacity=R, idle_timeout=10.0)
+    done_at = np.full(R, np.nan)
+    results = [None] * R
+    tickets = []
+    t0 = time.perf_counter()
+
+    def poll_all():
+        for k, t in enumerate(tickets):
+            if results[k] is None:
+                r = srv.poll(t)
+                if r is not None:
+                    results[k] = r
+                    done_at[k] = time.perf_counter() - t0
+
+    with Clocks(0) as clk:
+        for i in range(R):
+            while time.perf_counter() - t0 < arrivals[i]:
+                poll_all()
+                time.sleep(2e-4)
+            tickets.append(srv.submit(int(cls[i]), theta[i]))
+        while any(r is None for r in results):
+            poll_all()
+            time.sleep(1e-3)
+            if time.perf_counter() - t0 > 3600:
+                break
+    span = float(np.nanmax(done_at))
+    info = srv.info()
+    srv.destroy()
+    lat = done_at - arrivals
+    status = np.array([int(r.status) for r in results])
+    conv = int(np.sum(status == 0))
+    flagged_poison = int(sum(1 for k in range(R) if poisoned[k] and results[k].flagged))
+    service = np.array([(r.end_ns - r.start_ns) / 1e9 for r in results])
+    print(json.dumps({
+        "metric": SERVE_METRIC, "value": conv / span, "unit": "solves/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{R} channel requests (Re_tau 182/550/1000 equally), Student-t "
+                               "theta (nu 4, centre 0.324/0.0968), 5% out of bounds",
+                   "rate_per_s": args.rate, "slots": info["slots"]},
+        "requests": R, "converged": conv, "poisoned": int(poisoned.sum()),
+        "poisoned_flagged": flagged_poison,
+        "statuses": {s: int(np.sum(status == k)) for k, s in
+                     enumerate(["converged", "unconverged", "diverged", "invalid", "unknown"])},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max()),
+                      "note": "host clock: scheduled arrival to result seen by poll"},
+        "service_s": {"p50": float(np.percentile(service, 50)),
+                      "p99": float(np.percentile(service, 99))},
+        "span_s": span, "kernel_launches": info["launches"], "clocks": clk.summary(),
+    }))
+
+
 def main():
     args = parse()
+    if args.workload == "serve":
+        serve_arm(args)
+        return
     if args.workload == "linear":
         linear_arm(args)
     elif args.impl == "reference":
