@@ -312,19 +312,41 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     if (h.coarseN() > rq::kMaxCoarse)
         throw RqError(RQ_E_UNSUPPORTED, "coarsest AMG level above 64 rows");
     C.nlev = L;
+    // ELL slots of levels >= 1: CSR entry k of row i -> (k - ptr[i]) * n + i
+    std::vector<std::vector<int>> slotOf(L), entryOf(L);
+    std::vector<int> width(L, 0);
+    for (int l = 1; l < L; ++l) {
+        const auto &Lv = h.lev[l];
+        for (int i = 0; i < Lv.n; ++i)
+            width[l] = std::max(width[l], Lv.ptr[i + 1] - Lv.ptr[i]);
+        slotOf[l].resize(Lv.col.size());
+        entryOf[l].assign(static_cast<size_t>(width[l]) * Lv.n, -1);
+        for (int i = 0; i < Lv.n; ++i)
+            for (int k = Lv.ptr[i]; k < Lv.ptr[i + 1]; ++k) {
+                const int slot = (k - Lv.ptr[i]) * Lv.n + i;
+                slotOf[l][k] = slot;
+                entryOf[l][slot] = k;
+            }
+    }
     int valOff = 0, vecOff = 0;
     for (int l = 0; l < L; ++l) {
         const auto &Lv = h.lev[l];
         rq::DevAmgLevel &dl = C.lev[l];
         dl.n = Lv.n;
-        dl.nnz = l > 0 ? static_cast<int>(Lv.col.size()) : 0;
+        dl.width = l > 0 ? width[l] : 0;
+        dl.nnz = l > 0 ? width[l] * Lv.n : 0;
         dl.valOff = valOff;
         dl.vecOff = vecOff;
         if (l > 0) {
             valOff += static_cast<int>(pad32(dl.nnz));
-            addI(&dl.ptr, Lv.ptr);
-            addI(&dl.col, Lv.col);
-            addI(&dl.diagPos, Lv.diagPos);
+            std::vector<int> ecol(dl.nnz, -1), dpos(Lv.n);
+            for (int slot = 0; slot < dl.nnz; ++slot)
+                if (entryOf[l][slot] >= 0)
+                    ecol[slot] = Lv.col[entryOf[l][slot]];
+            for (int i = 0; i < Lv.n; ++i)
+                dpos[i] = slotOf[l][Lv.diagPos[i]];
+            addI(&dl.ecol, ecol);
+            addI(&dl.diagPos, dpos);
         }
         if (l > 0 || L == 1)
             vecOff += static_cast<int>(pad32(5L * Lv.n)); // b, xa, xb, r, 1/diag
@@ -332,8 +354,18 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
             addI(&dl.agg, Lv.agg);
             addI(&dl.childPtr, Lv.childPtr);
             addI(&dl.childIdx, Lv.childIdx);
-            addI(&dl.gPtr, Lv.gPtr);
-            addI(&dl.gSrc, Lv.gSrc);
+            // gather lists in the next level's slot order; sources of level >= 1 as slots
+            const int ns = width[l + 1] * h.lev[l + 1].n;
+            std::vector<int> gp(ns + 1, 0), gs;
+            for (int slot = 0; slot < ns; ++slot) {
+                const int e = entryOf[l + 1][slot];
+                if (e >= 0)
+                    for (int k = Lv.gPtr[e]; k < Lv.gPtr[e + 1]; ++k)
+                        gs.push_back(l == 0 ? Lv.gSrc[k] : slotOf[l][Lv.gSrc[k]]);
+                gp[slot + 1] = static_cast<int>(gs.size());
+            }
+            addI(&dl.gPtr, gp);
+            addI(&dl.gSrc, gs);
         }
     }
     C.amgVals = valOff;

@@ -27,13 +27,17 @@ struct DevSettings {
     double kMin, kMax, wMin;
 };
 
+// Levels >= 1 are stored in ELL form: value slot k*n + i holds the k-th entry of
+// row i in column order (a warp reading slot k of 32 consecutive rows touches
+// consecutive addresses); shorter rows are padded with column -1.
 struct DevAmgLevel {
-    int32_t n, nnz;             // rows; CSR nnz (levels >= 1)
+    int32_t n, nnz;             // rows; value slots (levels >= 1: width x n)
     int32_t valOff, vecOff;     // per-solve value / vector offsets (levels >= 1)
-    const int32_t *ptr, *col, *diagPos;
+    int32_t width, pad;         // ELL width (levels >= 1)
+    const int32_t *ecol, *diagPos;       // ELL columns (-1: padding); slot of the diagonal
     const int32_t *agg;                  // row -> next-level row
     const int32_t *childPtr, *childIdx;  // next-level row -> rows of this level
-    const int32_t *gPtr, *gSrc;          // next-level nnz -> entries of this level
+    const int32_t *gPtr, *gSrc;          // next-level value slot -> entries of this level
 };
 
 struct DevClass {

@@ -457,8 +457,11 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
             }
         } else {
             for (int r = threadIdx.x; r < m; r += blockDim.x)
-                for (int k = __ldg(Q.ptr + r); k < __ldg(Q.ptr + r + 1); ++k)
-                    a[r * m + __ldg(Q.col + k)] = double(qv[k]);
+                for (int k = 0; k < Q.width; ++k) {
+                    const int c = __ldg(Q.ecol + k * m + r);
+                    if (c >= 0)
+                        a[r * m + c] = double(qv[k * m + r]);
+                }
         }
         __syncthreads();
         if (threadIdx.x < 32) {
@@ -509,8 +512,11 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
         }
     } else {
         for (int r = threadIdx.x; r < m; r += blockDim.x)
-            for (int k = __ldg(Q.ptr + r); k < __ldg(Q.ptr + r + 1); ++k)
-                A0[r * m2 + __ldg(Q.col + k)] = double(qv[k]);
+            for (int k = 0; k < Q.width; ++k) {
+                const int c = __ldg(Q.ecol + k * m + r);
+                if (c >= 0)
+                    A0[r * m2 + c] = double(qv[k * m + r]);
+            }
     }
     __syncthreads();
     for (int piv = 0; piv < m; ++piv) {
@@ -532,11 +538,15 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
     }
 }
 
+// row i of an ELL level times x, entries in column order
 template <typename T>
 __device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
     T s = T(0);
-    for (int k = __ldg(L.ptr + i); k < __ldg(L.ptr + i + 1); ++k)
-        s += val[k] * x[__ldg(L.col + k)];
+    for (int k = 0; k < L.width; ++k) {
+        const int c = __ldg(L.ecol + k * L.n + i);
+        if (c >= 0)
+            s += val[k * L.n + i] * x[c];
+    }
     return s;
 }
 
@@ -667,9 +677,10 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
                 ri = Krd[c];
             } else {
                 ax = T(0);
-                for (int k = __ldg(Lv.ptr + i); k < __ldg(Lv.ptr + i + 1); ++k) {
-                    const int jj = __ldg(Lv.col + k);
-                    ax += val[k] * (xprev[jj] + xc[__ldg(agg + jj)]);
+                for (int k = 0; k < Lv.width; ++k) {
+                    const int jj = __ldg(Lv.ecol + k * n + i);
+                    if (jj >= 0)
+                        ax += val[k * n + i] * (xprev[jj] + xc[__ldg(agg + jj)]);
                 }
                 ri = b[4 * n + i];
             }
