@@ -5,8 +5,9 @@ stations (the survey's stand-in for the Lee-Moser DNS profile, which is not
 shipped). Run where oracle/_ref is built:  python bayesian-rans-uq_b200/data/make_channel_truth.py
 """
 import json
+import multiprocessing
 import sys
-import threading
+from concurrent.futures import ProcessPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -16,9 +17,6 @@ sys.path.insert(0, str(ROOT))
 from oracle import checker as ck  # noqa: E402
 import rans_uq_b200.workloads as wl  # noqa: E402
 
-out = {}
-
-
 def run(c):
     re_tau, ny = wl.CLASSES[c]
     x, y = wl.channel_probes(re_tau)
@@ -26,14 +24,15 @@ def run(c):
                    max_iter=wl.MAX_ITER, obs_x=x, obs_y=y, obs_value=np.zeros(30),
                    obs_sigma=np.ones(30)).with_theta(0.31, 0.09)
     o = ck.solve(case, "ref")
-    out[str(c)] = {"re_tau": re_tau, "ny": ny, "status": o.status, "iterations": o.iterations,
-                   "profile": [float(v) for v in o.predictions]}
     print(c, o.status, o.iterations, flush=True)
+    return {"re_tau": re_tau, "ny": ny, "status": o.status, "iterations": o.iterations,
+            "profile": [float(v) for v in o.predictions]}
 
 
-th = [threading.Thread(target=run, args=(c,)) for c in range(3)]
-for t in th:
-    t.start()
-for t in th:
-    t.join()
-(Path(__file__).parent / "channel_truth.json").write_text(json.dumps(out, indent=1))
+if __name__ == "__main__":
+    # one process per class: the reference solver is not safe to run from several
+    # threads of one process
+    with ProcessPoolExecutor(3, mp_context=multiprocessing.get_context("spawn")) as ex:
+        recs = list(ex.map(run, range(3)))
+    out = {str(c): r for c, r in enumerate(recs)}
+    (Path(__file__).parent / "channel_truth.json").write_text(json.dumps(out, indent=1))

@@ -144,3 +144,32 @@ def linear_workload(count: int = 512, seed: int = LINEAR_SEED, sizes=None):
     """The batch of `count` systems; system k uses seed + 1 + k."""
     sizes = linear_batch_sizes(count, seed) if sizes is None else sizes
     return [poisson_system(int(n), seed + 1 + k) for k, n in enumerate(sizes)]
+
+
+# ---------------------------------------------------------------- bump-wall channel
+def bump_geometry(nx: int = 200, h: float = 1.0, length: float = 9.0, width: float = 4.0):
+    """Streamwise nodes and lower-wall heights of the periodic bump channel:
+    y_w(x) = 0.5 h (1 + cos(2 pi (x - L/2) / W)) for |x - L/2| < W/2, else 0."""
+    xn = np.linspace(0.0, length, nx + 1)
+    yb = np.where(np.abs(xn - length / 2) < width / 2,
+                  0.5 * h * (1 + np.cos(2 * np.pi * (xn - length / 2) / width)), 0.0)
+    yb[0] = yb[-1] = 0.0
+    return xn, yb
+
+
+def bump_batch(nx: int = 200, ny: int = 100, max_iter: int = 200, tol: float = 1e-8,
+               body_force: float = 4e-3, re: float = 5600.0) -> core.ForwardBatch:
+    """The bump-wall channel (top 3.04 h, Re 5600 on h, y+ 1) as a ForwardBatch with
+    6 velocity probes at x = 2; the body force drives a bulk velocity of order one."""
+    xn, yb = bump_geometry(nx)
+    mesh = core.Mesh.make_curved_channel_periodic_2d(xn, yb, 3.04, ny, re, 1.0)
+    mesh.compute_wall_distance()
+    obs = core.ObservationOperator()
+    for yi in np.linspace(0.2, 2.8, 6):
+        obs.add_velocity_profile(core.Vec3(2.0, float(yi), 0.0), 0, 0.0, 1e-2)
+    st = core.SolverSettings(max_iterations=max_iter, convergence_tol=tol, alpha_u=0.4,
+                             alpha_p=0.25, body_force=core.Vec3(body_force, 0.0, 0.0),
+                             verbose=False)
+    bcs = core.FlowBoundaryConditions.channel_defaults(mesh, 1.0, 1e-4, 10.0)
+    return core.ForwardBatch(mesh, core.InferenceParameterSet.a1_betaStar(), obs, bcs,
+                             1.0 / re, st, core.Vec3(0.3, 0.0, 0.0), 0.0, 1e-4, 10.0)

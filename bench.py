@@ -18,7 +18,6 @@ import os
 import statistics
 import subprocess
 import sys
-import threading
 import time
 from pathlib import Path
 
@@ -48,7 +47,8 @@ def parse():
                     help="cap on outer iterations per draw (profiling runs only; the "
                          "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "linear", "serve"],
+    ap.add_argument("--workload", default="ensemble",
+                    choices=["ensemble", "linear", "serve", "bump"],
                     help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
                          "variable-coefficient Poisson systems by AMG-PCG; serve: open-loop "
                          "Poisson arrivals of channel requests to the serving loop")
@@ -60,30 +60,35 @@ def parse():
 
 
 # ---------------------------------------------------------------- CPU arm (reference)
-def cpu_iteration_times(sample_iters: int):
-    """Per-outer-iteration wall time of the reference's own solver (oracle/_ref) for
-    each Re_tau class: one capped cold solve per class, all classes concurrently."""
+def _ref_pool(workers: int):
+    """Processes (spawned, so no GPU state is inherited) for the reference's CPU
+    solver, which is not safe to run from several threads of one process."""
+    import multiprocessing
+    from concurrent.futures import ProcessPoolExecutor
+
+    return ProcessPoolExecutor(max_workers=workers, mp_context=multiprocessing.get_context("spawn"))
+
+
+def _ref_channel_seconds_per_iteration(c: int, sample_iters: int) -> float:
+    sys.path.insert(0, str(ROOT))
     from oracle import checker as ck
     import rans_uq_b200.workloads as wl
 
-    out = [None] * 3
+    re_tau, ny = wl.CLASSES[c]
+    x, y = wl.channel_probes(re_tau)
+    case = ck.Case(ny=ny, re_tau=re_tau, nu=1 / re_tau, yplus=0.5, alpha_u=wl.ALPHA_U,
+                   tol=wl.TOL, max_iter=sample_iters, obs_x=x, obs_y=y,
+                   obs_value=np.zeros(30), obs_sigma=np.ones(30)).with_theta(0.31, 0.09)
+    t = time.perf_counter()
+    o = ck.solve(case, "ref")
+    return (time.perf_counter() - t) / max(o.iterations, 1)
 
-    def run(c):
-        re_tau, ny = wl.CLASSES[c]
-        x, y = wl.channel_probes(re_tau)
-        case = ck.Case(ny=ny, re_tau=re_tau, nu=1 / re_tau, yplus=0.5, alpha_u=wl.ALPHA_U,
-                       tol=wl.TOL, max_iter=sample_iters, obs_x=x, obs_y=y,
-                       obs_value=np.zeros(30), obs_sigma=np.ones(30)).with_theta(0.31, 0.09)
-        t = time.perf_counter()
-        o = ck.solve(case, "ref")
-        out[c] = (time.perf_counter() - t) / max(o.iterations, 1)
 
-    th = [threading.Thread(target=run, args=(c,)) for c in range(3)]
-    for t in th:
-        t.start()
-    for t in th:
-        t.join()
-    return out
+def cpu_iteration_times(sample_iters: int):
+    """Per-outer-iteration wall time of the reference's own solver (oracle/_ref) for
+    each Re_tau class: one capped cold solve per class, the classes concurrently."""
+    with _ref_pool(3) as ex:
+        return list(ex.map(_ref_channel_seconds_per_iteration, range(3), [sample_iters] * 3))
 
 
 def cpu_baseline(iters_per_draw, cls, sample_iters):
@@ -346,33 +351,35 @@ def lin_bytes_per_iteration(n_rows, nnz, precision):
     return 5 * (cb * nnz + 4 * n_rows) + 32 * vb * n_rows
 
 
-def linear_cpu_sample(systems, sample):
-    """The reference's AMGSolver::solve (oracle/_ref) on a seeded sample of the
-    systems, one thread per system on all host cores; returns (solves/s for the
-    whole batch extrapolated by rows x iterations, description)."""
-    from concurrent.futures import ThreadPoolExecutor
+def _ref_linear_seconds(arrays):
+    sys.path.insert(0, str(ROOT))
     from oracle import checker as ck
 
+    diag, upper, lower, source, own, nbr = arrays
+    t = time.perf_counter()
+    _, info = ck.linear_solve(0, diag, upper, lower, source, own, nbr, np.zeros(len(diag)),
+                              LIN_MAX_ITER, LIN_TOL, lib_kind="ref")
+    return time.perf_counter() - t, info["iterations"]
+
+
+def linear_cpu_sample(systems, sample):
+    """The reference's AMGSolver::solve (oracle/_ref) on a seeded sample of the
+    systems, one process per host core; returns (solves/s for the whole batch
+    extrapolated by rows, cores, description)."""
     rng = np.random.default_rng(7)
     idx = sorted(rng.choice(len(systems), size=min(sample, len(systems)), replace=False))
     cores = os.cpu_count() or 1
-
-    def run(k):
-        s = systems[k]
-        t = time.perf_counter()
-        _, info = ck.linear_solve(0, s.diag, s.upper, s.lower, s.source, s.own, s.nbr,
-                                  np.zeros(s.n_cells), LIN_MAX_ITER, LIN_TOL, lib_kind="ref")
-        return time.perf_counter() - t, info["iterations"]
-
+    args = [(systems[k].diag, systems[k].upper, systems[k].lower, systems[k].source,
+             systems[k].own, systems[k].nbr) for k in idx]
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=cores) as ex:
-        out = list(ex.map(run, idx))
+    with _ref_pool(min(cores, len(idx))) as ex:
+        out = list(ex.map(_ref_linear_seconds, args))
     wall = time.perf_counter() - t0
     per_row = sum(t for t, _ in out) / sum(systems[k].n_cells for k in idx)
     total_cpu = per_row * sum(s.n_cells for s in systems)
     value = len(systems) / (total_cpu / cores)
     return value, cores, (f"reference AMGSolver::solve (oracle/_ref, g++ -O2) on {len(idx)} of "
-                          f"{len(systems)} systems ({wall:.1f} s wall on {cores} threads); "
+                          f"{len(systems)} systems ({wall:.1f} s wall, one process per core); "
                           f"seconds per row x all rows / {cores} cores (extrapolated)")
 
 
@@ -570,8 +577,110 @@ def serve_arm(args):
     }))
 
 
+# ---------------------------------------------------------------- bump-wall workload
+BUMP_METRIC = "bump-wall RANS-SST outer iterations/s, 32 draws on 200x100 cells (capped solves)"
+
+
+def _ref_bump_seconds_per_iteration(theta, iters: int) -> float:
+    sys.path.insert(0, str(ROOT))
+    from oracle import checker as ck
+    import rans_uq_b200.workloads as wl
+
+    xn, yb = wl.bump_geometry(200)
+    case = ck.Case(nx=200, ny=100, curved=True, x_nodes=xn, y_bottom=yb, y_top=3.04,
+                   re_mesh=5600.0, yplus=1.0, nu=1 / 5600.0, bc=(1.0, 1e-4, 10.0),
+                   init_u=(0.3, 0.0, 0.0), init_k=1e-4, init_w=10.0, alpha_u=0.4,
+                   alpha_p=0.25, body_force=(4e-3, 0.0, 0.0), tol=1e-8, max_iter=iters,
+                   obs_x=np.full(6, 2.0), obs_y=np.linspace(0.2, 2.8, 6),
+                   obs_value=np.zeros(6), obs_sigma=np.full(6, 1e-2)).with_theta(*theta)
+    t = time.perf_counter()
+    o = ck.solve(case, "ref")
+    return (time.perf_counter() - t) / max(o.iterations, 1)
+
+
+def bump_cpu_sample(iters: int = 10, draws: int = 16):
+    """The reference's solver (oracle/_ref) on the same mesh and settings: `draws`
+    solves capped at `iters` outer iterations, one process per host core; returns
+    the median seconds per outer iteration per solve and the process count."""
+    import rans_uq_b200.workloads as wl
+
+    cores = os.cpu_count() or 1
+    theta = [tuple(t) for t in wl.uniform_design(range(draws))]
+    with _ref_pool(min(cores, draws)) as ex:
+        per = list(ex.map(_ref_bump_seconds_per_iteration, theta, [iters] * draws))
+    return float(np.median(per)), min(cores, draws)
+
+
+def bump_arm(args):
+    import torch
+    import rans_uq_b200 as rq
+    import rans_uq_b200.workloads as wl
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    cap = args.max_iter or 200
+    batch = wl.bump_batch(200, 100, max_iter=cap)
+    theta = wl.uniform_design(range(32))
+    n = len(theta)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    th = torch.tensor(theta, dtype=torch.float64, device=dev)
+    rows = torch.zeros(n * 40, dtype=torch.uint8, device=dev)
+    pred = torch.zeros((n, 6), dtype=torch.float64, device=dev)
+    clock = torch.zeros((n, 12), dtype=torch.int64, device=dev)
+    cls = np.zeros(n, np.int32)
+
+    def step():
+        rq.evaluate_multi_device([batch], cls, th.data_ptr(), rows.data_ptr(), pred.data_ptr(),
+                                 stream.cuda_stream, clock.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    recs = rq.rows_from_device_bytes(rows.cpu().numpy())
+    iters = recs["iterations"].astype(np.int64)
+    ck_ = clock.cpu().numpy()
+    per_solve_ms = float(np.median((ck_[:, 1] - ck_[:, 0]) / 1e6 / np.maximum(iters, 1)))
+    value = float(iters.sum()) / (ms / 1e3)
+    cpu = None
+    if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+        sec, cores = bump_cpu_sample()
+        cpu = {"value": cores / sec, "unit": "outer iterations/s", "cores": cores,
+               "kind": "reference",
+               "sample": f"16 reference solves capped at 10 outer iterations on {cores} threads: "
+                         f"{1e3 * sec:.1f} ms per outer iteration per solve; value = threads / that"}
+    print(json.dumps({
+        "metric": BUMP_METRIC, "value": value, "unit": "outer iterations/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "bump-wall channel 200 x 100 (h 1, L 9h, W 4h, top 3.04h, Re 5600), "
+                               "32 draws of the prior box", "max_iter": cap},
+        "per_solve_ms_per_outer_iteration": per_solve_ms,
+        "statuses": {s: int(np.sum(recs["status"] == k)) for k, s in
+                     enumerate(["converged", "unconverged", "diverged", "invalid", "unknown"])},
+        "krylov_per_outer": float(ck_[:, 2].sum() / max(iters.sum(), 1)),
+        "pressure_per_outer": float(ck_[:, 3].sum() / max(iters.sum(), 1)),
+        "gpu_launches": args.steps, "cpu_baseline": cpu,
+    }))
+
+
 def main():
     args = parse()
+    if args.workload == "bump":
+        bump_arm(args)
+        return
     if args.workload == "serve":
         serve_arm(args)
         return
