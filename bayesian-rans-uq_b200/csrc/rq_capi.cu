@@ -410,9 +410,26 @@ int maxSmemOptin() {
     return v;
 }
 
-// Shared-memory arena for a launch: the whole per-solve workspace when it
-// fits beside another CTA on the SM (two CTAs per SM for the small classes),
-// else as much as one CTA per SM can hold; the hottest arrays are placed first.
+// Shared-memory arena of a launch, in doubles. Classes of up to 768 cells run two
+// CTAs per SM and place their whole hot set in half the SM's shared memory each.
+// Larger classes run one CTA per SM and take no arena: their hot set does not fit
+// (14 level-0 Krylov arrays plus the AMG coarse levels), and leaving the unified
+// L1/shared storage to the L1 cache measured faster (1536 cells: 537 us per outer
+// iteration without an arena against 656 us with the largest one).
+int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
+    const long shared = static_cast<long>(rq::solveSharedBytes());
+    const long optin = maxSmemOptin();
+    long bytes;
+    if (knobKb > 0)
+        bytes = std::min<long>(knobKb * 1024L, optin - shared);
+    else if (nmax <= 768)
+        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
+    else
+        bytes = 0;
+    bytes = std::max<long>(0, std::min(bytes, wsDoubles * 8));
+    return static_cast<int>(bytes / 8 / 32 * 32);
+}
+
 int chooseArena(const std::vector<const rq_problem *> &probs) {
     long ws = 0;
     int knob = 0;
@@ -422,17 +439,7 @@ int chooseArena(const std::vector<const rq_problem *> &probs) {
         knob = std::max(knob, p->arenaKb);
         nmax = std::max(nmax, p->mesh.n);
     }
-    const long shared = static_cast<long>(rq::solveSharedBytes());
-    const long optin = maxSmemOptin();
-    long bytes;
-    if (knob > 0)
-        bytes = std::min<long>(knob * 1024L, optin - shared);
-    else if (nmax <= 768)
-        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
-    else
-        bytes = optin - shared;
-    bytes = std::max<long>(0, std::min(bytes, ws * 8));
-    return static_cast<int>(bytes / 8 / 32 * 32);
+    return arenaDoublesFor(ws, knob, nmax);
 }
 
 // One persistent launch of a single mesh class over its rows.
@@ -1363,14 +1370,8 @@ int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_
         job.theta = theta_dev;
         job.row = reinterpret_cast<rq::RowOut *>(row_dev);
         job.pred = predictions_dev;
-        // shared-memory arena as the batch path sizes it for one class (no containers)
-        const long shared = static_cast<long>(rq::solveSharedBytes());
-        const long optin = maxSmemOptin();
-        long bytes = p->arenaKb > 0 ? std::min<long>(p->arenaKb * 1024L, optin - shared)
-                     : p->mesh.n <= 768 ? (optin / 2 - 1024) - shared
-                                        : optin - shared;
-        bytes = std::max<long>(0, std::min(bytes, need * 8));
-        const int arena = static_cast<int>(bytes / 8 / 32 * 32);
+        // shared-memory arena as the batch path sizes it for one class
+        const int arena = arenaDoublesFor(need, p->arenaKb, p->mesh.n);
         check(rq::launchSolveNoAlloc(job, p->block, arena, static_cast<cudaStream_t>(stream)),
               "allocation-free solve launch");
     });

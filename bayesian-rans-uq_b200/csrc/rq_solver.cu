@@ -550,10 +550,16 @@ __device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T
     return s;
 }
 
+// Coarse levels of at most this many rows run their V-cycle phases in warp 0
+// alone, separated by warp barriers instead of CTA barriers: at three rows per
+// lane the work is tiny, and a CTA barrier per phase would cost more than it.
+constexpr int kWarpRows = 96;
+
 // z = M^-1 b at level 0 (b = K.r, z -> K.z): pre-smoothing from zero (two damped
 // Jacobi sweeps), aggregate-sum restriction fused into the next level's first
 // sweep, dense coarsest solve, aggregate-broadcast prolongation fused into the
 // first of two post sweeps (symmetric). Returns (r, z), reduced in the last phase.
+// Levels of at most kWarpRows rows (and the coarsest) run in warp 0 only.
 template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
@@ -563,7 +569,10 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     T *const Krd = K.rd, *const Kr = K.r, *const Kz = K.z, *const Kxa = K.xa, *const Kxb = K.xb,
              *const Krr = K.rr, *const amgVec = K.amgVec, *const amgVal = K.amgVal;
     auto vb = [&](int l) { return amgVec + C.lev[l].vecOff; }; // b, xa, xb, r, 1/diag
-    for (int l = 0; l + 1 < L; ++l) {
+    auto blockSync = [] { __syncthreads(); };
+    auto warpSync = [] { __syncwarp(); };
+    // one level of the down sweep, rows t0, t0 + ts, ...
+    auto down = [&](int l, int t0, int ts, auto sync) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         T *b, *xa, *xb, *rr;
@@ -579,7 +588,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             rr = b + 3 * n;
         }
         const T *val = amgVal + Lv.valOff;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        for (int i = t0; i < n; i += ts) {
             T bi;
             if (l == 0) {
                 bi = b[i];
@@ -594,8 +603,8 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             const T ri = (l == 0) ? Krd[i] : b[4 * n + i];
             xa[i] = om * bi * ri;
         }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sync();
+        for (int i = t0; i < n; i += ts) {
             T ax, ri;
             if (l == 0) {
                 ax = rowDotT(cellOf(C, i), M, xa, nx);
@@ -606,114 +615,126 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             }
             xb[i] = xa[i] + om * (b[i] - ax) * ri;
         }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sync();
+        for (int i = t0; i < n; i += ts) {
             const T ax = (l == 0) ? rowDotT(cellOf(C, i), M, xb, nx) : csrRowT(Lv, val, xb, i);
             rr[i] = b[i] - ax;
         }
-        __syncthreads();
-    }
-    {
+        sync();
+    };
+    // the coarsest level: restriction of the level above, then the dense inverse
+    auto coarsest = [&](int t0, int ts, auto sync) {
         const int l = L - 1;
         const int m = C.lev[l].n, m2 = 2 * m;
         T *b = vb(l), *xb = b + 2 * m;
         if (L == 1) {
-            for (int i = threadIdx.x; i < m; i += blockDim.x)
+            for (int i = t0; i < m; i += ts)
                 b[i] = Kr[i];
         } else {
             const DevAmgLevel &F = C.lev[l - 1];
             const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
-            for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            for (int i = t0; i < m; i += ts) {
                 T bi = T(0);
                 for (int k = __ldg(F.childPtr + i); k < __ldg(F.childPtr + i + 1); ++k)
                     bi += fr[__ldg(F.childIdx + k)];
                 b[i] = bi;
             }
         }
-        __syncthreads();
+        sync();
         // the coarsest solve stays FP64 in both forms: the coarsest level of the
         // pinned all-Neumann pressure system is nearly singular, and an FP32
         // copy of its inverse loses the coarse correction
-        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        for (int i = t0; i < m; i += ts) {
             double s = 0.0;
             const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
             for (int j = 0; j < m; ++j)
                 s += row[j] * double(b[j]);
             xb[i] = T(s);
         }
-        __syncthreads();
-    }
-    double rz = 0.0;
-    for (int l = L - 2; l >= 0; --l) {
+        sync();
+    };
+    // one level of the up sweep (levels >= 1; level 0 ends in the reduction below)
+    auto up = [&](int l, int t0, int ts, auto sync) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         const T *xc = vb(l + 1) + 2 * C.lev[l + 1].n;
-        T *b, *xa, *xb;
-        if (l == 0) {
-            b = Kr;
-            xa = Kxa;
-            xb = Kz;
-        } else {
-            b = vb(l);
-            xa = b + n;
-            xb = b + 2 * n;
-        }
-        const T *xprev = (l == 0) ? Kxb : xb;
+        T *b = vb(l), *xa = b + n, *xb = b + 2 * n;
         const T *val = amgVal + Lv.valOff;
         const int *agg = Lv.agg;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const T xi = xprev[i] + xc[__ldg(agg + i)];
-            T ax, ri;
-            if (l == 0) {
-                const Cell q = cellOf(C, i);
-                const int c = i;
-                auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + jj)]; };
-                const T tW = M.aW[c] * X(q.W), tE = M.aE[c] * X(q.E);
-                const T tS = q.south ? M.aS[c] * X(c - nx) : T(0);
-                const T tN = q.north ? M.aN[c] * X(c + nx) : T(0);
-                const T x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
-                const T y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
-                ax = (((M.d[c] * xi + x1) + x2) + y1) + y2;
-                ri = Krd[c];
-            } else {
-                ax = T(0);
-                for (int k = 0; k < Lv.width; ++k) {
-                    const int jj = __ldg(Lv.ecol + k * n + i);
-                    if (jj >= 0)
-                        ax += val[k * n + i] * (xprev[jj] + xc[__ldg(agg + jj)]);
-                }
-                ri = b[4 * n + i];
+        for (int i = t0; i < n; i += ts) {
+            const T xi = xb[i] + xc[__ldg(agg + i)];
+            T ax = T(0);
+            for (int k = 0; k < Lv.width; ++k) {
+                const int jj = __ldg(Lv.ecol + k * n + i);
+                if (jj >= 0)
+                    ax += val[k * n + i] * (xb[jj] + xc[__ldg(agg + jj)]);
             }
-            xa[i] = xi + om * (b[i] - ax) * ri;
+            xa[i] = xi + om * (b[i] - ax) * b[4 * n + i];
+        }
+        sync();
+        for (int i = t0; i < n; i += ts)
+            xb[i] = xa[i] + om * (b[i] - csrRowT(Lv, val, xa, i)) * b[4 * n + i];
+        sync();
+    };
+    // first level handled by warp 0 alone (L: none)
+    int lw = L;
+    for (int l = 1; l < L; ++l)
+        if (C.lev[l].n <= kWarpRows) {
+            lw = l;
+            break;
+        }
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int l = 0; l + 1 < L && l < lw; ++l)
+        down(l, tid, nt, blockSync);
+    if (lw < L) {
+        if (tid < 32) {
+            for (int l = lw; l + 1 < L; ++l)
+                down(l, tid, 32, warpSync);
+            coarsest(tid, 32, warpSync);
+            for (int l = L - 2; l >= lw; --l)
+                up(l, tid, 32, warpSync);
+        }
+        __syncthreads();
+    } else {
+        coarsest(tid, nt, blockSync);
+    }
+    for (int l = (lw < L ? lw : L - 1) - 1; l >= 1; --l)
+        up(l, tid, nt, blockSync);
+    double rz = 0.0;
+    if (L > 1) { // level 0: prolongation fused into the first post sweep, then the second
+        const DevAmgLevel &Lv = C.lev[0];
+        const int n = Lv.n;
+        const T *xc = vb(1) + 2 * C.lev[1].n;
+        const int *agg = Lv.agg;
+        const T *xprev = Kxb;
+        for (int i = tid; i < n; i += nt) {
+            const T xi = xprev[i] + xc[__ldg(agg + i)];
+            const Cell q = cellOf(C, i);
+            const int c = i;
+            auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + jj)]; };
+            const T tW = M.aW[c] * X(q.W), tE = M.aE[c] * X(q.E);
+            const T tS = q.south ? M.aS[c] * X(c - nx) : T(0);
+            const T tN = q.north ? M.aN[c] * X(c + nx) : T(0);
+            const T x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
+            const T y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
+            const T ax = (((M.d[c] * xi + x1) + x2) + y1) + y2;
+            Kxa[i] = xi + om * (Kr[i] - ax) * Krd[c];
         }
         __syncthreads();
         double part = 0.0;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            T ax, ri;
-            if (l == 0) {
-                ax = rowDotT(cellOf(C, i), M, xa, nx);
-                ri = Krd[i];
-            } else {
-                ax = csrRowT(Lv, val, xa, i);
-                ri = b[4 * n + i];
-            }
-            const T zi = xa[i] + om * (b[i] - ax) * ri;
-            xb[i] = zi;
-            if (l == 0)
-                part += double(b[i]) * double(zi);
+        for (int i = tid; i < n; i += nt) {
+            const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
+            const T zi = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
+            Kz[i] = zi;
+            part += double(Kr[i]) * double(zi);
         }
-        if (l == 0) {
-            double a[1] = {part};
-            blockSum<1>(a, S, rp);
-            rz = a[0];
-        } else {
-            __syncthreads();
-        }
-    }
-    if (L == 1) {
+        double a[1] = {part};
+        blockSum<1>(a, S, rp);
+        rz = a[0];
+    } else {
         const T *xb = vb(0) + 2 * C.lev[0].n;
         double part = 0.0;
-        for (int i = threadIdx.x; i < n0; i += blockDim.x) {
+        for (int i = tid; i < n0; i += nt) {
             Kz[i] = xb[i];
             part += double(Kr[i]) * double(xb[i]);
         }
