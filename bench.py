@@ -32,6 +32,10 @@ UNIT = "solves/s"
 # (CPU pilot of the compiled reference); used only by the CPU arm's extrapolation
 REF_ITERS = (12460, 58690, 258900)
 BYTES_OUTER, BYTES_KRYLOV, BYTES_PRESSURE = 1600, 360, 400  # algorithmic B/cell (FP64)
+# DRAM bytes (read + write) of one 1536-cell draw as ncu counted them over a
+# 600-iteration solve: the first touch of the mesh class and the workspace; later
+# iterations hit L2, so the figure does not grow with iterations
+DRAM_BYTES_PER_DRAW_1536 = 848_384 + 256
 
 
 def parse():
@@ -327,7 +331,11 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": len(per_class) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm,
+                     "traffic": (DRAM_BYTES_PER_DRAW_1536 * int(np.sum(cls == dom_c))
+                                 if int(np.max(cells[cls == dom_c])) == 1536 else None),
+                     "traffic_note": "ncu DRAM read+write of one 1536-cell draw (first touch; "
+                                     "constant in the iteration count) x draws in the launch",
                      "peak_source": "measured" if "gpu_name" in peaks else "fallback",
                      "kernel": f"solveKernel, Re_tau class {dom_c} ({int(np.sum(cls == dom_c))} rows)",
                      "kernel_ms": dom_s * 1e3, "step_bytes_per_s": alg_bytes / (ms / 1e3),
