@@ -550,16 +550,13 @@ __device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T
     return s;
 }
 
-// Coarse levels of at most this many rows run their V-cycle phases in warp 0
-// alone, separated by warp barriers instead of CTA barriers: at three rows per
-// lane the work is tiny, and a CTA barrier per phase would cost more than it.
-constexpr int kWarpRows = 96;
-
 // z = M^-1 b at level 0 (b = K.r, z -> K.z): pre-smoothing from zero (two damped
 // Jacobi sweeps), aggregate-sum restriction fused into the next level's first
 // sweep, dense coarsest solve, aggregate-broadcast prolongation fused into the
 // first of two post sweeps (symmetric). Returns (r, z), reduced in the last phase.
-// Levels of at most kWarpRows rows (and the coarsest) run in warp 0 only.
+// (Running the small coarse levels in one warp with warp barriers measured 15 %
+// slower per outer iteration: one warp exposes the latency of its dependent loads
+// that a CTA's many warps hide.)
 template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
@@ -569,10 +566,10 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     T *const Krd = K.rd, *const Kr = K.r, *const Kz = K.z, *const Kxa = K.xa, *const Kxb = K.xb,
              *const Krr = K.rr, *const amgVec = K.amgVec, *const amgVal = K.amgVal;
     auto vb = [&](int l) { return amgVec + C.lev[l].vecOff; }; // b, xa, xb, r, 1/diag
-    auto blockSync = [] { __syncthreads(); };
-    auto warpSync = [] { __syncwarp(); };
-    // one level of the down sweep, rows t0, t0 + ts, ...
-    auto down = [&](int l, int t0, int ts, auto sync) {
+    auto sync = [] { __syncthreads(); };
+    const int t0 = threadIdx.x, ts = blockDim.x;
+    // one level of the down sweep
+    auto down = [&](int l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         T *b, *xa, *xb, *rr;
@@ -623,7 +620,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         sync();
     };
     // the coarsest level: restriction of the level above, then the dense inverse
-    auto coarsest = [&](int t0, int ts, auto sync) {
+    auto coarsest = [&]() {
         const int l = L - 1;
         const int m = C.lev[l].n, m2 = 2 * m;
         T *b = vb(l), *xb = b + 2 * m;
@@ -654,7 +651,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         sync();
     };
     // one level of the up sweep (levels >= 1; level 0 ends in the reduction below)
-    auto up = [&](int l, int t0, int ts, auto sync) {
+    auto up = [&](int l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         const T *xc = vb(l + 1) + 2 * C.lev[l + 1].n;
@@ -676,30 +673,12 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             xb[i] = xa[i] + om * (b[i] - csrRowT(Lv, val, xa, i)) * b[4 * n + i];
         sync();
     };
-    // first level handled by warp 0 alone (L: none)
-    int lw = L;
-    for (int l = 1; l < L; ++l)
-        if (C.lev[l].n <= kWarpRows) {
-            lw = l;
-            break;
-        }
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int l = 0; l + 1 < L && l < lw; ++l)
-        down(l, tid, nt, blockSync);
-    if (lw < L) {
-        if (tid < 32) {
-            for (int l = lw; l + 1 < L; ++l)
-                down(l, tid, 32, warpSync);
-            coarsest(tid, 32, warpSync);
-            for (int l = L - 2; l >= lw; --l)
-                up(l, tid, 32, warpSync);
-        }
-        __syncthreads();
-    } else {
-        coarsest(tid, nt, blockSync);
-    }
-    for (int l = (lw < L ? lw : L - 1) - 1; l >= 1; --l)
-        up(l, tid, nt, blockSync);
+    for (int l = 0; l + 1 < L; ++l)
+        down(l);
+    coarsest();
+    for (int l = L - 2; l >= 1; --l)
+        up(l);
+    const int tid = t0, nt = ts;
     double rz = 0.0;
     if (L > 1) { // level 0: prolongation fused into the first post sweep, then the second
         const DevAmgLevel &Lv = C.lev[0];
