@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import hashlib
 import json
+import math
 from dataclasses import dataclass
 from pathlib import Path
 
@@ -173,3 +174,47 @@ def bump_batch(nx: int = 200, ny: int = 100, max_iter: int = 200, tol: float = 1
     bcs = core.FlowBoundaryConditions.channel_defaults(mesh, 1.0, 1e-4, 10.0)
     return core.ForwardBatch(mesh, core.InferenceParameterSet.a1_betaStar(), obs, bcs,
                              1.0 / re, st, core.Vec3(0.3, 0.0, 0.0), 0.0, 1e-4, 10.0)
+
+
+# ---------------------------------------------------------------- calibration study
+CAL_HALF_CELLS = 64
+CAL_TRUE_THETA = (0.3137, 0.0912)
+
+
+def calibration_batch(observed=None, sigma=None) -> core.ForwardBatch:
+    """The calibration study's channel (docs/figures/calibration_coverage.py:81-113):
+    Re_tau 182.088 on 3 x 128 cells whose first cell matches a uniform 64-cell
+    half-height tanh stretching, alpha_U 0.5, tol 1e-8, cap 150000, 30 stations;
+    sigma[i] = inf drops station i from the likelihood (sigma 1e6)."""
+    first_height = 1 + math.tanh(2 * (1 / CAL_HALF_CELLS - 1)) / math.tanh(2)
+    mesh = core.Mesh.make_periodic_channel_2d(3, 2 * CAL_HALF_CELLS, 1.0, 1.0, 182.088,
+                                              first_height * 182.088)
+    mesh.compute_wall_distance()
+    x, y = channel_probes(182.088)
+    observed = np.zeros(len(x)) if observed is None else observed
+    sigma = np.ones(len(x)) if sigma is None else sigma
+    obs = core.ObservationOperator()
+    for xi, yi, ui, si in zip(x, y, observed, sigma):
+        obs.add_velocity_profile(core.Vec3(float(xi), float(yi), 0.0), 0, float(ui),
+                                 float(si) if np.isfinite(si) else 1e6)
+    st = core.SolverSettings(max_iterations=150000, convergence_tol=1e-8, alpha_u=0.5,
+                             body_force=core.Vec3(1.0, 0.0, 0.0), verbose=False)
+    bcs = core.FlowBoundaryConditions.channel_defaults(mesh, 1.0, 1.0, 10.0)
+    return core.ForwardBatch(mesh, core.InferenceParameterSet.a1_betaStar(), obs, bcs,
+                             1.0 / 182.088, st, core.Vec3(15.0, 0.0, 0.0), 0.0, 1.0, 10.0)
+
+
+def calibration_study_batch():
+    """The study's batch with a synthetic observed profile (the DNS profile is not
+    shipped): this solver's own profile at CAL_TRUE_THETA times (1 + 0.0014 eps), and
+    sigma_i = 0.0014 |u_i| on every third station (the likelihood third), the rest
+    dropped."""
+    probe = calibration_batch()
+    res = probe.evaluate(np.array([CAL_TRUE_THETA]))
+    if res.rows[0].result.status != core.EvaluationStatus.Converged:
+        raise RuntimeError("the synthetic truth solve did not converge")
+    u = np.asarray(res.rows[0].result.predictions)
+    eps = sample_rng(SEED, 99, "synthetic-observation-noise").standard_normal(len(u))
+    group = np.arange(len(u)) % 3
+    sigma = np.where(group == 0, NOISE * np.abs(u), np.inf)
+    return calibration_batch(u * (1 + NOISE * eps), sigma), u

@@ -52,7 +52,7 @@ def parse():
                          "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ensemble",
-                    choices=["ensemble", "linear", "serve", "bump"],
+                    choices=["ensemble", "linear", "serve", "bump", "calibrate"],
                     help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
                          "variable-coefficient Poisson systems by AMG-PCG; serve: open-loop "
                          "Poisson arrivals of channel requests to the serving loop")
@@ -684,8 +684,53 @@ def bump_arm(args):
     }))
 
 
+# ---------------------------------------------------------------- calibration workload
+CAL_METRIC = "calibration study wall time: uniform design, pattern search, Laplace grid, 2 x 64 importance draws"
+
+
+def calibrate_arm(args):
+    import torch
+    import rans_uq_b200.calibration as cal
+    import rans_uq_b200.workloads as wl
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    batch, truth = wl.calibration_study_batch()
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    out = cal.calibrate(cal.batch_evaluator(batch))
+    wall = time.perf_counter() - t0
+    main, rep = out.importance
+    sd = np.sqrt(np.diag(out.scale))
+    print(json.dumps({
+        "metric": CAL_METRIC, "value": wall, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "Re_tau 182.088, 3 x 128 cells, 30 stations (likelihood third), "
+                               "synthetic observed profile at (0.3137, 0.0912) x (1 + 0.0014 eps)",
+                   "alpha_u": 0.5, "tol": 1e-8},
+        "solves": out.solves, "truth_setup_s": setup,
+        "stages": [{"name": s.name, "solves": s.solves, "seconds": s.seconds} for s in out.stages],
+        "search_path_steps": len(out.path) - 1,
+        "laplace": {"center": out.center.tolist(), "sd": sd.tolist(),
+                    "correlation": float(out.scale[0, 1] / (sd[0] * sd[1])),
+                    "fit_residual_rms": out.laplace["residual_rms"]},
+        "importance": {k: main[k] for k in ("effective_sample_size", "max_weight",
+                                             "distinct_draws", "theta_mean", "theta_sd")},
+        "replicate": {k: rep[k] for k in ("effective_sample_size", "theta_mean", "theta_sd")},
+        "true_theta": list(wl.CAL_TRUE_THETA),
+        "reference_published": "241 solves in about 50 minutes on 4 threads "
+                               "(docs/figures/README.md of the reference)",
+    }))
+
+
 def main():
     args = parse()
+    if args.workload == "calibrate":
+        calibrate_arm(args)
+        return
     if args.workload == "bump":
         bump_arm(args)
         return
