@@ -159,12 +159,15 @@ def importance_stage(evaluator, center, scale, ids, seed, weights=None):
             "weights": w, "theta": theta, "log_q": log_q, "log_lik": ll}
 
 
-def calibrate(evaluator, clock=None, weights=None) -> Calibration:
+def calibrate(evaluator, clock=None, weights=None, trace=None) -> Calibration:
     """All stages, each one batch of solves (pattern-search steps one batch each).
-    weights: the importance-weight function (default: FP64 on the GPU)."""
+    weights: the importance-weight function (default: FP64 on the GPU); trace (a
+    dict, optional) receives each stage's intermediate results as they appear, so
+    a stage that raises leaves the earlier ones behind."""
     import time
 
     clock = clock or time.perf_counter
+    trace = {} if trace is None else trace
     stages = []
     t = clock()
     lower, upper = STAGE1_BOX
@@ -172,13 +175,16 @@ def calibrate(evaluator, clock=None, weights=None) -> Calibration:
     ll1 = _evaluate(evaluator, range(24), th1)
     k = int(np.argmax(ll1))
     stages.append(Stage("uniform design", 24, clock() - t))
+    trace["stage1"] = {"best": th1[k].tolist(), "best_loglik": float(ll1[k])}
     t = clock()
     optimum, step, path, n_search = pattern_search(evaluator, th1[k], ll1[k])
     stages.append(Stage("pattern search", n_search, clock() - t))
+    trace["pattern_search"] = {"path": path, "step": step.tolist()}
     t = clock()
     offsets = np.array([(i, j) for i in range(-2, 3) for j in range(-2, 3)], dtype=float)
     grid = np.array([optimum + step * o for o in offsets])
     llg = _evaluate(evaluator, range(200, 225), grid)
+    trace["laplace_grid"] = {"theta": grid.tolist(), "loglik": llg.tolist()}
     fit = laplace_fit(llg, (grid - optimum) / step)
     center = optimum + step * fit["peak"]
     scale = np.diag(step) @ fit["covariance"] @ np.diag(step)

@@ -344,6 +344,56 @@ void greedyAggregate(const Csr &A, std::vector<int> &map, int &nc) {
         map[i] = bestAgg;
     }
 }
+// Row-relative aggregation, for matrices on which the symmetric strength rule
+// stalls (strongly varying cell aspect ratios: the bump-wall meshes keep ~1000
+// rows after 20 levels): j is strong for i when |a_ij| >= 0.25 max_k |a_ik|; seeds
+// claim their unaggregated strong neighbours, a seed left alone joins its
+// strongest neighbour's aggregate, and ids are renumbered in order of first use.
+void rowRelativeAggregate(const Csr &A, std::vector<int> &map, int &nc) {
+    map.assign(A.n, -1);
+    int groups = 0;
+    for (int i = 0; i < A.n; ++i) {
+        if (map[i] >= 0)
+            continue;
+        const int g = groups++;
+        map[i] = g;
+        double rowMax = 0.0;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+            if (A.col[k] != i)
+                rowMax = std::max(rowMax, std::abs(A.val[k]));
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            const int c = A.col[k];
+            if (c != i && map[c] < 0 && rowMax > 0.0 && std::abs(A.val[k]) >= 0.25 * rowMax)
+                map[c] = g;
+        }
+    }
+    std::vector<int> count(groups, 0);
+    for (int i = 0; i < A.n; ++i)
+        ++count[map[i]];
+    for (int i = 0; i < A.n; ++i) {
+        if (count[map[i]] != 1)
+            continue;
+        double best = 0.0;
+        int j = -1;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+            if (A.col[k] != i && std::abs(A.val[k]) > best) {
+                best = std::abs(A.val[k]);
+                j = A.col[k];
+            }
+        if (j < 0)
+            continue;
+        --count[map[i]];
+        map[i] = map[j];
+        ++count[map[j]];
+    }
+    std::vector<int> id(groups, -1);
+    nc = 0;
+    for (int i = 0; i < A.n; ++i) {
+        if (id[map[i]] < 0)
+            id[map[i]] = nc++;
+        map[i] = id[map[i]];
+    }
+}
 } // namespace
 
 AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
@@ -392,7 +442,11 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
         A.dg[c] = d;
         A.ptr[c + 1] = static_cast<int>(A.col.size());
     }
+    // the reference's aggregation first; if it stalls above minCoarse rows, the
+    // row-relative rule instead
     AmgHost h;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+    h = AmgHost{};
     std::vector<Csr> mats{A};
     for (int l = 0; l < maxLevels; ++l) {
         const Csr &F = mats.back();
@@ -400,7 +454,10 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
             break;
         std::vector<int> map;
         int nc = 0;
-        greedyAggregate(F, map, nc);
+        if (attempt == 0)
+            greedyAggregate(F, map, nc);
+        else
+            rowRelativeAggregate(F, map, nc);
         if (nc == 0 || nc >= F.n)
             break;
         // coarse pattern and Galerkin values
@@ -472,6 +529,9 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
             last.diagPos[i] = Cl.find(i, i);
     }
     h.lev.push_back(std::move(last));
+    if (h.coarseN() <= minCoarse)
+        break;
+    }
     return h;
 }
 

@@ -700,7 +700,13 @@ def calibrate_arm(args):
     batch, truth = wl.calibration_study_batch()
     setup = time.perf_counter() - t0
     t0 = time.perf_counter()
-    out = cal.calibrate(cal.batch_evaluator(batch))
+    trace = {}
+    try:
+        out = cal.calibrate(cal.batch_evaluator(batch), trace=trace)
+    except RuntimeError as e:
+        print(json.dumps({"metric": CAL_METRIC, "failed": str(e),
+                          "seconds": time.perf_counter() - t0, "trace": trace}))
+        return
     wall = time.perf_counter() - t0
     main, rep = out.importance
     sd = np.sqrt(np.diag(out.scale))

@@ -585,6 +585,10 @@ static Amg buildAmg(const Mesh &m) {
         up[f] = lo[f] = -c;
     }
     d[0] += d[0];
+    // the reference's aggregation first; if it stalls above AMG_MIN_COARSE rows
+    // (strongly varying aspect ratios), the row-relative rule of aggregateLinear
+    for (int attempt = 0; attempt < 2; ++attempt) {
+    h = Amg{};
     AmgLevel l0;
     l0.A = lduCsr(m.nC, m.own, m.nbr, m.nI, d, up, lo, &h.upPos, &h.loPos);
     l0.dpos.resize(m.nC);
@@ -597,7 +601,10 @@ static Amg buildAmg(const Mesh &m) {
             break;
         std::vector<int> map;
         int nc = 0;
-        aggregate(fine.A, map, nc);
+        if (attempt == 0)
+            aggregate(fine.A, map, nc);
+        else
+            aggregateLinear(fine.A, map, nc);
         if (nc == 0 || nc >= fine.A.n)
             break;
         AmgLevel coarse;
@@ -613,6 +620,9 @@ static Amg buildAmg(const Mesh &m) {
                 fine.gIdx[k] = csrFind(coarse.A, fine.agg[i], fine.agg[fine.A.col[k]]);
         sumCoarse(fine, coarse);
         h.lev.push_back(std::move(coarse));
+    }
+    if (h.lev.back().A.n <= AMG_MIN_COARSE)
+        break;
     }
     return h;
 }
