@@ -100,8 +100,7 @@ struct rq_problem {
     std::vector<int32_t> active;
     double base[11];
     int32_t nObs = 0;
-    int block = 256;
-    int cpt = 0;     // cells per thread of the register-blocked solvers (0 = generic kernel)
+    int block = 512; // CTA size of this class's launches
     int arenaKb = 0; // shared-memory arena per CTA, 0 = automatic
     cudaStream_t stream = nullptr; // for concurrent per-class launches of a multi-class batch
     cudaEvent_t done = nullptr;
@@ -395,13 +394,9 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     check(cudaMemcpy(P.dCls.p, &C, sizeof(rq::DevClass), cudaMemcpyHostToDevice), "upload");
 }
 
-// Default kernel variant for a class of n cells: the register-blocked solvers
-// when one CTA's registers can own every cell, the generic kernel otherwise.
-void defaultVariant(int n, int &block, int &cpt) {
-    (void)n;
-    block = 512; // fastest measured for 384-1536 cells
-    cpt = 0;
-}
+// CTA size of a class: 512 threads measured fastest for 384-1536 cells (256 and
+// 1024 were slower at every size).
+constexpr int kDefaultBlock = 512;
 
 int maxSmemOptin() {
     int dev = 0, v = 0;
@@ -466,7 +461,7 @@ void launchClass(rq_problem &P, const std::vector<int> &rows, const double *thet
     int dev = 0, sms = 1;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    const int perSM = rq::solveBlocksPerSM(P.block, P.cpt, arena);
+    const int perSM = rq::solveBlocksPerSM(P.block, arena);
     if (perSM < 1)
         throw RqError(RQ_E_CUDA, "solve kernel does not fit on an SM with this arena");
     const int grid = std::max(1, std::min(n, sms * perSM));
@@ -477,7 +472,7 @@ void launchClass(rq_problem &P, const std::vector<int> &rows, const double *thet
                           stream), "jobs");
     check(cudaMemsetAsync(P.dCounter.p, 0, sizeof(int), stream), "counter");
     check(rq::launchSolve(P.dJobs.as<rq::DevJob>(), n, P.dCounter.as<int>(), P.dWs.as<double>(),
-                          wsStride, grid, P.block, P.cpt, arena, stream),
+                          wsStride, grid, P.block, arena, stream),
           "solve launch");
 }
 
@@ -924,11 +919,8 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
         P->active.assign(active, active + n_active);
         std::memcpy(P->base, base, sizeof(P->base));
         P->nObs = obs ? obs->n_obs : 0;
-        defaultVariant(P->mesh.n, P->block, P->cpt);
-        if (settings->block_threads) { // an explicit CTA size selects the generic kernel
-            P->block = rq::normalizeBlock(settings->block_threads);
-            P->cpt = 0;
-        }
+        P->block = settings->block_threads ? rq::normalizeBlock(settings->block_threads)
+                                           : kDefaultBlock;
         upload(*P, obs, nu, *settings, init);
         *out = P.release();
     });
@@ -1131,7 +1123,7 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
         check(cudaMemcpy(p->dJobs.p, jobs.data(), sizeof(rq::DevJob), cudaMemcpyHostToDevice), "jobs");
         check(cudaMemset(p->dCounter.p, 0, sizeof(int)), "counter");
         check(rq::launchSolve(p->dJobs.as<rq::DevJob>(), 1, p->dCounter.as<int>(),
-                              p->dWs.as<double>(), p->cls.wsDoubles, 1, p->block, p->cpt, arena,
+                              p->dWs.as<double>(), p->cls.wsDoubles, 1, p->block, arena,
                               nullptr),
               "solve launch");
         rq::RowOut o;

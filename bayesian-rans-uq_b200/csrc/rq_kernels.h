@@ -10,13 +10,12 @@ size_t solveSharedBytes();
 // Persistent CTAs: each pulls job indices from *nextJob (zeroed by the caller)
 // until njobs are taken; ws is grid x wsStride doubles of per-CTA workspace.
 // arenaDoubles: shared-memory arena per CTA for the hot arrays (0 = all global).
-// cpt: cells per thread of the register-blocked solvers (0 = generic); (block, cpt) must be
-// a compiled variant and block * cpt must cover the class's cells when cpt > 0.
+// block: a compiled CTA size (64, 128, 256, 512 or 1024).
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
-                        int grid, int block, int cpt, int arenaDoubles, cudaStream_t stream);
+                        int grid, int block, int arenaDoubles, cudaStream_t stream);
 // CTAs of the variant with the given arena that fit on one SM at once (0: does not fit).
-int solveBlocksPerSM(int block, int cpt, int arenaDoubles);
-bool launchVariantExists(int block, int cpt);
+int solveBlocksPerSM(int block, int arenaDoubles);
+bool launchVariantExists(int block);
 // The serving loop (serveKernel): grid persistent CTAs of `block` threads (256, 512
 // or 1024) serving q until it is closed and drained, or until q.idleNs passes
 // without a request.

@@ -2377,9 +2377,7 @@ size_t solveSharedBytes() { return ((sizeof(Shared) + 15) / 16) * 16; }
 namespace {
 template <int NT> void *kernelFor() { return reinterpret_cast<void *>(&solveKernel<NT>); }
 template <int NT> void *serveFor() { return reinterpret_cast<void *>(&serveKernel<NT>); }
-void *pick(int block, int cpt) {
-    if (cpt != 0)
-        return nullptr;
+void *pick(int block) {
     switch (block) {
     case 64: return kernelFor<64>();
     case 128: return kernelFor<128>();
@@ -2399,16 +2397,16 @@ void *pickServe(int block) {
 }
 } // namespace
 
-bool launchVariantExists(int block, int cpt) { return pick(block, cpt) != nullptr; }
+bool launchVariantExists(int block) { return pick(block) != nullptr; }
 
 int normalizeBlock(int block) {
     return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : block <= 512 ? 512 : 1024;
 }
 
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
-                        int grid, int block, int cpt, int arenaDoubles, cudaStream_t stream) {
+                        int grid, int block, int arenaDoubles, cudaStream_t stream) {
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
-    void *fn = pick(block, cpt);
+    void *fn = pick(block);
     if (!fn)
         return cudaErrorInvalidConfiguration;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2422,9 +2420,9 @@ cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws,
     return cudaGetLastError();
 }
 
-int solveBlocksPerSM(int block, int cpt, int arenaDoubles) {
+int solveBlocksPerSM(int block, int arenaDoubles) {
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
-    void *fn = pick(block, cpt);
+    void *fn = pick(block);
     if (!fn)
         return 0;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
