@@ -367,6 +367,8 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
             addI(&dl.gSrc, gs);
         }
     }
+    C.amgW = h.w;
+    C.amgAlpha = h.alpha;
     C.amgVals = valOff;
     C.amgVecs = vecOff;
     C.nActive = static_cast<int32_t>(P.active.size());

@@ -59,6 +59,7 @@ struct DevClass {
     const double *pox, *poy, *paxx, *paxy, *payy, *pdet, *pdx, *pdy, *pwt;
     const double *obsVal, *obsVar, *obsFloor;
     DevAmgLevel lev[kMaxLevels];
+    double amgW, amgAlpha;     // V-cycle smoother weight, coarse-correction scale
     int32_t amgVals, amgVecs;  // per-solve doubles for coarse values / vectors
     int64_t wsDoubles;         // per-solve workspace
     // InferenceParameterSet: active indices, the coefficients filling the rest,

@@ -529,6 +529,10 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
             last.diagPos[i] = Cl.find(i, i);
     }
     h.lev.push_back(std::move(last));
+    if (attempt == 1) {
+        h.w = 0.75;
+        h.alpha = 1.7;
+    }
     if (h.coarseN() <= minCoarse)
         break;
     }

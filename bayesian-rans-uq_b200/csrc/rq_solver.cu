@@ -32,7 +32,6 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int kRedSlots = 8;             // values per block reduction
-constexpr double kJacobiW = 0.6;         // AMG smoother damping
 
 struct Work {
     double *Ux, *Uy, *p, *k, *w, *nuT, *F1, *F2, *Pk, *CD, *S;
@@ -561,7 +560,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev, n0 = C.n, nx = C.nx;
-    const T om = T(kJacobiW);
+    const T om = T(C.amgW), al = T(C.amgAlpha);
     const Mat<T> M = matOf(K);
     T *const Krd = K.rd, *const Kr = K.r, *const Kz = K.z, *const Kxa = K.xa, *const Kxb = K.xb,
              *const Krr = K.rr, *const amgVec = K.amgVec, *const amgVal = K.amgVal;
@@ -659,12 +658,12 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const T *val = amgVal + Lv.valOff;
         const int *agg = Lv.agg;
         for (int i = t0; i < n; i += ts) {
-            const T xi = xb[i] + xc[__ldg(agg + i)];
+            const T xi = xb[i] + al * xc[__ldg(agg + i)];
             T ax = T(0);
             for (int k = 0; k < Lv.width; ++k) {
                 const int jj = __ldg(Lv.ecol + k * n + i);
                 if (jj >= 0)
-                    ax += val[k * n + i] * (xb[jj] + xc[__ldg(agg + jj)]);
+                    ax += val[k * n + i] * (xb[jj] + al * xc[__ldg(agg + jj)]);
             }
             xa[i] = xi + om * (b[i] - ax) * b[4 * n + i];
         }
@@ -687,10 +686,10 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const int *agg = Lv.agg;
         const T *xprev = Kxb;
         for (int i = tid; i < n; i += nt) {
-            const T xi = xprev[i] + xc[__ldg(agg + i)];
+            const T xi = xprev[i] + al * xc[__ldg(agg + i)];
             const Cell q = cellOf(C, i);
             const int c = i;
-            auto X = [&](int jj) { return xprev[jj] + xc[__ldg(agg + jj)]; };
+            auto X = [&](int jj) { return xprev[jj] + al * xc[__ldg(agg + jj)]; };
             const T tW = M.aW[c] * X(q.W), tE = M.aE[c] * X(q.E);
             const T tS = q.south ? M.aS[c] * X(c - nx) : T(0);
             const T tN = q.north ? M.aN[c] * X(c + nx) : T(0);

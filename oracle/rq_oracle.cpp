@@ -621,6 +621,10 @@ static Amg buildAmg(const Mesh &m) {
         sumCoarse(fine, coarse);
         h.lev.push_back(std::move(coarse));
     }
+    if (attempt == 1) { // the fallback hierarchy over-corrects (as the linear solves)
+        h.w = 0.75;
+        h.alpha = 1.7;
+    }
     if (h.lev.back().A.n <= AMG_MIN_COARSE)
         break;
     }
