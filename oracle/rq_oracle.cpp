@@ -372,7 +372,11 @@ struct Amg {
     int levels() const { return static_cast<int>(lev.size()); }
 };
 
-static const int AMG_MIN_COARSE = 32;  // the reference stops at 50 (LinearSolver.hpp:664); 32 = one warp
+// coarsening stops at this many rows: the reference stops at 50 (LinearSolver.hpp:664);
+// the pressure hierarchy at 64 (a dense inverse of up to 64 rows is cheaper than two
+// more levels), the standalone linear solves at 32
+static const int AMG_MIN_COARSE = 64;
+static const int AMG_MIN_COARSE_LINEAR = 32;
 static const int AMG_MAX_LEVELS = 20;  // :663
 static const int AMG_SWEEPS = 2;
 
@@ -1835,7 +1839,7 @@ int orc_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,
             h.lev.push_back(std::move(l0));
             for (int l = 0; l < AMG_MAX_LEVELS; ++l) {
                 AmgLevel &fine = h.lev[l];
-                if (fine.A.n <= AMG_MIN_COARSE)
+                if (fine.A.n <= AMG_MIN_COARSE_LINEAR)
                     break;
                 std::vector<int> map;
                 int nc = 0;
