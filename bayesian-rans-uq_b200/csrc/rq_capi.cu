@@ -673,35 +673,28 @@ void buildLinsys(rq_linsys &L, const rq_ldu *systems, int n, int kind, int preci
         if (!err[s].empty())
             throw RqError(unsupported[s] ? RQ_E_UNSUPPORTED : RQ_E_INVALID,
                           "system " + std::to_string(s) + ": " + err[s]);
-    // pack every array into three device buffers (int32, FP64, FP32)
-    std::vector<int32_t> I;
-    std::vector<double> D;
-    std::vector<float> F;
-    struct Patch {
+    // Layout pass: every array of every system gets an offset in one of three
+    // device buffers (int32, FP64, FP32); the copies then run on all host threads.
+    enum { P_PTR, P_COL, P_VAL, P_RDG, P_VAL32, P_RDG32, P_AGG, P_CPTR, P_CIDX, P_INV, P_INV32 };
+    struct Piece {
         int s, l, what;
         size_t off;
+        const void *src; // std::vector<int> or std::vector<double> of the host set-up
     };
-    std::vector<Patch> patches;
+    std::vector<Piece> pieces;
+    size_t nI = 0, nD = 0, nF = 0;
     auto addI = [&](int s, int l, int what, const std::vector<int> &v) {
-        patches.push_back({s, l, what, I.size()});
-        I.insert(I.end(), v.begin(), v.end());
-        while (I.size() % 8)
-            I.push_back(0);
+        pieces.push_back({s, l, what, nI, &v});
+        nI += (v.size() + 7) / 8 * 8;
     };
     auto addD = [&](int s, int l, int what, const std::vector<double> &v) {
-        patches.push_back({s, l, what, D.size()});
-        D.insert(D.end(), v.begin(), v.end());
-        while (D.size() % 4)
-            D.push_back(0.0);
+        pieces.push_back({s, l, what, nD, &v});
+        nD += (v.size() + 3) / 4 * 4;
     };
     auto addF = [&](int s, int l, int what, const std::vector<double> &v) {
-        patches.push_back({s, l, what, F.size()});
-        for (double x : v)
-            F.push_back(static_cast<float>(x));
-        while (F.size() % 8)
-            F.push_back(0.0f);
+        pieces.push_back({s, l, what, nF, &v});
+        nF += (v.size() + 7) / 8 * 8;
     };
-    enum { P_PTR, P_COL, P_VAL, P_RDG, P_VAL32, P_RDG32, P_AGG, P_CPTR, P_CIDX, P_INV, P_INV32 };
     const bool mixed = precision == RQ_PREC_MIXED;
     L.rows.resize(n);
     L.xOff.resize(n);
@@ -759,14 +752,57 @@ void buildLinsys(rq_linsys &L, const rq_ldu *systems, int n, int kind, int preci
         L.totalRows += h.n;
         L.maxLevels = std::max(L.maxLevels, nl);
     }
-    L.dI.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));
-    L.dD.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
-    L.dF.ensure(std::max<size_t>(F.size(), 1) * sizeof(float));
-    check(cudaMemcpy(L.dI.p, I.data(), I.size() * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-    check(cudaMemcpy(L.dD.p, D.data(), D.size() * sizeof(double), cudaMemcpyHostToDevice), "upload");
-    if (!F.empty())
-        check(cudaMemcpy(L.dF.p, F.data(), F.size() * sizeof(float), cudaMemcpyHostToDevice), "upload");
-    for (const Patch &p : patches) {
+    std::unique_ptr<int32_t[]> I(new int32_t[std::max<size_t>(nI, 1)]);
+    std::unique_ptr<double[]> D(new double[std::max<size_t>(nD, 1)]);
+    std::unique_ptr<float[]> F(new float[std::max<size_t>(nF, 1)]);
+    std::unique_ptr<double[]> hb(new double[std::max<int64_t>(L.totalRows, 1)]);
+    {
+        const int nt = std::max(1, std::min<int>(static_cast<int>(pieces.size()),
+                                                 static_cast<int>(std::thread::hardware_concurrency())));
+        std::atomic<size_t> next{0};
+        std::atomic<int> nextRhs{0};
+        auto work = [&] {
+            for (size_t k = next++; k < pieces.size(); k = next++) {
+                const Piece &p = pieces[k];
+                switch (p.what) {
+                case P_PTR: case P_COL: case P_AGG: case P_CPTR: case P_CIDX: {
+                    const auto &v = *static_cast<const std::vector<int> *>(p.src);
+                    std::copy(v.begin(), v.end(), I.get() + p.off);
+                    std::fill(I.get() + p.off + v.size(), I.get() + p.off + (v.size() + 7) / 8 * 8, 0);
+                    break;
+                }
+                case P_VAL: case P_RDG: case P_INV: {
+                    const auto &v = *static_cast<const std::vector<double> *>(p.src);
+                    std::copy(v.begin(), v.end(), D.get() + p.off);
+                    std::fill(D.get() + p.off + v.size(), D.get() + p.off + (v.size() + 3) / 4 * 4, 0.0);
+                    break;
+                }
+                default: {
+                    const auto &v = *static_cast<const std::vector<double> *>(p.src);
+                    for (size_t e = 0; e < v.size(); ++e)
+                        F[p.off + e] = static_cast<float>(v[e]);
+                    std::fill(F.get() + p.off + v.size(), F.get() + p.off + (v.size() + 7) / 8 * 8, 0.0f);
+                }
+                }
+            }
+            for (int s = nextRhs++; s < n; s = nextRhs++)
+                std::memcpy(hb.get() + L.xOff[s], systems[s].source, sizeof(double) * L.rows[s]);
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nt; ++t)
+            pool.emplace_back(work);
+        work();
+        for (auto &t : pool)
+            t.join();
+    }
+    L.dI.ensure(std::max<size_t>(nI, 1) * sizeof(int32_t));
+    L.dD.ensure(std::max<size_t>(nD, 1) * sizeof(double));
+    L.dF.ensure(std::max<size_t>(nF, 1) * sizeof(float));
+    check(cudaMemcpy(L.dI.p, I.get(), nI * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
+    check(cudaMemcpy(L.dD.p, D.get(), nD * sizeof(double), cudaMemcpyHostToDevice), "upload");
+    if (nF)
+        check(cudaMemcpy(L.dF.p, F.get(), nF * sizeof(float), cudaMemcpyHostToDevice), "upload");
+    for (const Piece &p : pieces) {
         rq::DevLinSys &d = byIndex[p.s];
         rq::DevLinLevel &dl = d.lev[p.l];
         const int32_t *ip = L.dI.as<int32_t>() + p.off;
@@ -786,14 +822,11 @@ void buildLinsys(rq_linsys &L, const rq_ldu *systems, int n, int kind, int preci
         case P_INV32: d.inv32 = fp; break;
         }
     }
-    // right-hand sides, solutions and results
-    std::vector<double> hb(L.totalRows);
-    for (int s = 0; s < n; ++s)
-        std::memcpy(hb.data() + L.xOff[s], systems[s].source, sizeof(double) * L.rows[s]);
+    // right-hand sides (gathered above), solutions and results
     L.dB.ensure(sizeof(double) * L.totalRows);
     L.dX.ensure(sizeof(double) * L.totalRows);
     L.dOut.ensure(sizeof(rq::LinOut) * n);
-    check(cudaMemcpy(L.dB.p, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice), "rhs");
+    check(cudaMemcpy(L.dB.p, hb.get(), sizeof(double) * L.totalRows, cudaMemcpyHostToDevice), "rhs");
     for (int s = 0; s < n; ++s) {
         byIndex[s].b = L.dB.as<double>() + L.xOff[s];
         byIndex[s].x = L.dX.as<double>() + L.xOff[s];
