@@ -2,118 +2,54 @@
 // per-mesh-class set-up (rq_setup.cpp), admission of inputs with the
 // reference's rules, and the launch of persistent solve CTAs; all per-draw
 // numerics run in rq_solver.cu.
-#include "../../include/rq_b200.h"
-#include "rq_device.cuh"
-#include "rq_kernels.h"
-#include "rq_lin.cuh"
-#include "rq_linsys.h"
-#include "rq_setup.h"
+#include "rq_capi_common.h"
 
-#include <cuda_runtime.h>
+using namespace rqc;
 
-#include <algorithm>
-#include <atomic>
-#include <chrono>
-#include <cmath>
-#include <cstring>
-#include <limits>
-#include <memory>
-#include <mutex>
-#include <numeric>
-#include <stdexcept>
-#include <string>
-#include <thread>
-#include <vector>
-
-namespace {
+namespace rqc {
 
 thread_local std::string g_error;
 
-struct RqError : std::runtime_error {
-    int code;
-    RqError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
-};
-
-void check(cudaError_t e, const char *what) {
-    if (e == cudaErrorMemoryAllocation)
-        throw RqError(RQ_E_OOM, std::string(what) + ": " + cudaGetErrorString(e));
-    if (e != cudaSuccess)
-        throw RqError(RQ_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+int maxSmemOptin() {
+    int dev = 0, v = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attribute");
+    return v;
 }
 
-template <class F> int guarded(F &&f) {
-    try {
-        f();
-        return RQ_OK;
-    } catch (const RqError &e) {
-        g_error = e.what();
-        return e.code;
-    } catch (const std::invalid_argument &e) {
-        g_error = e.what();
-        return RQ_E_INVALID;
-    } catch (const std::bad_alloc &e) {
-        g_error = "host allocation failed";
-        return RQ_E_OOM;
-    } catch (const std::exception &e) {
-        g_error = e.what();
-        return RQ_E_CUDA;
-    }
-}
-
-// device allocation that frees itself
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p)
-            cudaFree(p);
-        p = nullptr;
+// Shared-memory arena of a launch, in doubles. Classes of up to 768 cells run two
+// CTAs per SM and place their whole hot set in half the SM's shared memory each.
+// Larger classes run one CTA per SM and take no arena: their hot set does not fit
+// (14 level-0 Krylov arrays plus the AMG coarse levels), and leaving the unified
+// L1/shared storage to the L1 cache measured faster (1536 cells: 537 us per outer
+// iteration without an arena against 656 us with the largest one).
+int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
+    const long shared = static_cast<long>(rq::solveSharedBytes());
+    const long optin = maxSmemOptin();
+    long bytes;
+    if (knobKb > 0)
+        bytes = std::min<long>(knobKb * 1024L, optin - shared);
+    else if (nmax <= 768)
+        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
+    else
         bytes = 0;
+    bytes = std::max<long>(0, std::min(bytes, wsDoubles * 8));
+    return static_cast<int>(bytes / 8 / 32 * 32);
+}
+
+int chooseArena(const std::vector<const rq_problem *> &probs) {
+    long ws = 0;
+    int knob = 0;
+    int nmax = 0;
+    for (const auto *p : probs) {
+        ws = std::max(ws, static_cast<long>(p->cls.wsDoubles));
+        knob = std::max(knob, p->arenaKb);
+        nmax = std::max(nmax, p->mesh.n);
     }
-    void ensure(size_t b) {
-        if (b <= bytes)
-            return;
-        release();
-        check(cudaMalloc(&p, b), "cudaMalloc");
-        bytes = b;
-    }
-    template <class T> T *as() const { return static_cast<T *>(p); }
-};
+    return arenaDoublesFor(ws, knob, nmax);
+}
 
-// The reference's parameter bounds (core/include/InferenceParameters.hpp:147-165).
-const double kLower[11] = {0.1, 0.1, 0.01, 0.1, 0.1, 0.1, 0.01, 0.1, 0.01, 0.1, 0.35};
-const double kUpper[11] = {2.0, 2.0, 0.2, 1.5, 2.0, 2.0, 0.2, 1.5, 0.2, 0.8, 0.50};
-
-long pad32(long n) { return (n + 31) / 32 * 32; }
-
-} // namespace
-
-struct rq_problem {
-    rq::StructMesh mesh;
-    rq::AmgHost amg;
-    rq::DevClass cls{};      // host copy with device pointers
-    DevBuf dCls, dDoubles, dInts;
-    std::vector<int32_t> active;
-    double base[11];
-    int32_t nObs = 0;
-    int block = 512; // CTA size of this class's launches
-    int arenaKb = 0; // shared-memory arena per CTA, 0 = automatic
-    cudaStream_t stream = nullptr; // for concurrent per-class launches of a multi-class batch
-    cudaEvent_t done = nullptr;
-    ~rq_problem() {
-        if (done)
-            cudaEventDestroy(done);
-        if (stream)
-            cudaStreamDestroy(stream);
-    }
-    // launch scratch, reused across calls
-    DevBuf dWs, dJobs, dRows, dPred, dFields, dHist, dTheta, dCounter, dClock;
-    std::mutex mu;
-};
+} // namespace rqc
 
 namespace {
 
@@ -400,44 +336,8 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
 // 1024 were slower at every size).
 constexpr int kDefaultBlock = 512;
 
-int maxSmemOptin() {
-    int dev = 0, v = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    check(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "attribute");
-    return v;
-}
 
-// Shared-memory arena of a launch, in doubles. Classes of up to 768 cells run two
-// CTAs per SM and place their whole hot set in half the SM's shared memory each.
-// Larger classes run one CTA per SM and take no arena: their hot set does not fit
-// (14 level-0 Krylov arrays plus the AMG coarse levels), and leaving the unified
-// L1/shared storage to the L1 cache measured faster (1536 cells: 537 us per outer
-// iteration without an arena against 656 us with the largest one).
-int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
-    const long shared = static_cast<long>(rq::solveSharedBytes());
-    const long optin = maxSmemOptin();
-    long bytes;
-    if (knobKb > 0)
-        bytes = std::min<long>(knobKb * 1024L, optin - shared);
-    else if (nmax <= 768)
-        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
-    else
-        bytes = 0;
-    bytes = std::max<long>(0, std::min(bytes, wsDoubles * 8));
-    return static_cast<int>(bytes / 8 / 32 * 32);
-}
 
-int chooseArena(const std::vector<const rq_problem *> &probs) {
-    long ws = 0;
-    int knob = 0;
-    int nmax = 0;
-    for (const auto *p : probs) {
-        ws = std::max(ws, static_cast<long>(p->cls.wsDoubles));
-        knob = std::max(knob, p->arenaKb);
-        nmax = std::max(nmax, p->mesh.n);
-    }
-    return arenaDoublesFor(ws, knob, nmax);
-}
 
 // One persistent launch of a single mesh class over its rows.
 void launchClass(rq_problem &P, const std::vector<int> &rows, const double *thetaDev,
@@ -527,352 +427,6 @@ void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOf
     for (int g : order)
         check(cudaStreamWaitEvent(stream, classes[g]->done, 0), "stream wait");
     cudaEventDestroy(fork);
-}
-
-rq_row_out toRow(const rq::RowOut &o) {
-    return rq_row_out{o.status, o.iterations, o.stalled, o.converged, o.loglik, o.finalWorst,
-                      o.contractionRate};
-}
-
-// pinned, device-mapped host allocation that frees itself
-struct MappedBuf {
-    void *p = nullptr;
-    MappedBuf() = default;
-    MappedBuf(const MappedBuf &) = delete;
-    MappedBuf &operator=(const MappedBuf &) = delete;
-    ~MappedBuf() {
-        if (p)
-            cudaFreeHost(p);
-    }
-    void alloc(size_t b) {
-        check(cudaHostAlloc(&p, b, cudaHostAllocMapped | cudaHostAllocPortable), "cudaHostAlloc");
-        std::memset(p, 0, b);
-    }
-};
-
-} // namespace
-
-// The serving loop's host half: a request queue in host-mapped memory that a
-// persistent kernel drains while the host keeps appending to it.
-struct rq_server {
-    std::vector<rq_problem *> problems;
-    int capacity = 0, thetaStride = 1, predStride = 1, block = 512, grid = 1, arena = 0;
-    long wsStride = 0;
-    long long idleNs = 0;
-    MappedBuf host; // jobs | theta | rows | predictions | clocks | done | published | closed
-    rq::DevJob *jobs = nullptr;
-    double *theta = nullptr, *pred = nullptr;
-    rq::RowOut *rows = nullptr;
-    long long *clock = nullptr;
-    int *done = nullptr, *published = nullptr, *closed = nullptr;
-    DevBuf dWs, dCtl; // per-slot workspace; head and idle-exit counters
-    cudaStream_t stream = nullptr;
-    int submitted = 0, launches = 0;
-    std::mutex mu;
-    ~rq_server() {
-        if (closed)
-            __atomic_store_n(closed, 2, __ATOMIC_RELEASE); // cancel what is not yet claimed
-        if (stream) {
-            cudaStreamSynchronize(stream); // in-flight solves finish first
-            cudaStreamDestroy(stream);
-        }
-    }
-    rq::ServeQueue queue() const {
-        rq::ServeQueue q{};
-        q.jobs = jobs;
-        q.published = published;
-        q.closed = closed;
-        q.done = done;
-        q.head = dCtl.as<int>();
-        q.idleExits = dCtl.as<int>() + 1;
-        q.capacity = capacity;
-        q.idleNs = idleNs;
-        return q;
-    }
-    void launch() {
-        check(rq::launchServe(queue(), dWs.as<double>(), wsStride, grid, block, arena, stream),
-              "serve launch");
-        ++launches;
-    }
-    // The kernel's CTAs leave after idleNs without work; relaunch while requests
-    // remain unclaimed (a relaunch never repeats a request: CTAs claim by head).
-    void ensureRunning() {
-        const cudaError_t e = cudaStreamQuery(stream);
-        if (e == cudaErrorNotReady)
-            return;
-        check(e, "serve loop");
-        for (int i = 0; i < submitted; ++i)
-            if (!__atomic_load_n(done + i, __ATOMIC_ACQUIRE)) {
-                launch();
-                return;
-            }
-    }
-};
-
-
-// Standalone LDU systems resident on the device (rq_linsys_*).
-struct rq_linsys {
-    int nsys = 0, kind = 0, precision = 0, maxLevels = 0, grid = 1;
-    long wsStride = 0;
-    int64_t totalRows = 0, totalNnz = 0;
-    std::vector<int> rows;
-    std::vector<int64_t> xOff;
-    std::vector<rq::DevLinSys> sys; // queue order (largest first), device pointers
-    DevBuf dI, dD, dF, dB, dX, dSys, dOut, dWs, dNext;
-    std::mutex mu;
-};
-
-namespace {
-
-void checkSolveArgs(int maxIter, double tol) {
-    if (maxIter < 0 || !std::isfinite(tol) || tol <= 0.)
-        throw std::invalid_argument("linear solve requires matching x, nonnegative iteration "
-                                    "cap and positive finite tolerance");
-}
-
-void buildLinsys(rq_linsys &L, const rq_ldu *systems, int n, int kind, int precision) {
-    L.nsys = n;
-    L.kind = kind;
-    L.precision = precision;
-    for (int s = 0; s < n; ++s) {
-        const rq_ldu &A = systems[s];
-        rq::validateLdu(A.n_cells, A.n_faces, A.diag, A.upper, A.lower, A.source, A.owner,
-                        A.neighbour);
-        if (A.n_cells < 1)
-            throw std::invalid_argument("linear system needs at least one cell");
-    }
-    // host set-up of every system, on all host threads
-    std::vector<rq::LinSysHost> H(n);
-    std::vector<std::string> err(n);
-    std::vector<int> unsupported(n, 0);
-    {
-        const int nt = std::max(1, std::min<int>(n, static_cast<int>(std::thread::hardware_concurrency())));
-        std::atomic<int> next{0};
-        auto work = [&] {
-            for (int s = next++; s < n; s = next++) {
-                const rq_ldu &A = systems[s];
-                try {
-                    H[s] = rq::buildLinSys(A.n_cells, A.n_faces, A.diag, A.upper, A.lower, A.owner,
-                                           A.neighbour, kind == rq::kLinAmg);
-                } catch (const rq::LinUnsupported &e) {
-                    err[s] = e.what();
-                    unsupported[s] = 1;
-                } catch (const std::exception &e) {
-                    err[s] = e.what();
-                }
-            }
-        };
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nt; ++t)
-            pool.emplace_back(work);
-        work();
-        for (auto &t : pool)
-            t.join();
-    }
-    for (int s = 0; s < n; ++s)
-        if (!err[s].empty())
-            throw RqError(unsupported[s] ? RQ_E_UNSUPPORTED : RQ_E_INVALID,
-                          "system " + std::to_string(s) + ": " + err[s]);
-    // Layout pass: every array of every system gets an offset in one of three
-    // device buffers (int32, FP64, FP32); the copies then run on all host threads.
-    enum { P_PTR, P_COL, P_VAL, P_RDG, P_VAL32, P_RDG32, P_AGG, P_CPTR, P_CIDX, P_INV, P_INV32 };
-    struct Piece {
-        int s, l, what;
-        size_t off;
-        const void *src; // std::vector<int> or std::vector<double> of the host set-up
-    };
-    std::vector<Piece> pieces;
-    size_t nI = 0, nD = 0, nF = 0;
-    auto addI = [&](int s, int l, int what, const std::vector<int> &v) {
-        pieces.push_back({s, l, what, nI, &v});
-        nI += (v.size() + 7) / 8 * 8;
-    };
-    auto addD = [&](int s, int l, int what, const std::vector<double> &v) {
-        pieces.push_back({s, l, what, nD, &v});
-        nD += (v.size() + 3) / 4 * 4;
-    };
-    auto addF = [&](int s, int l, int what, const std::vector<double> &v) {
-        pieces.push_back({s, l, what, nF, &v});
-        nF += (v.size() + 7) / 8 * 8;
-    };
-    const bool mixed = precision == RQ_PREC_MIXED;
-    L.rows.resize(n);
-    L.xOff.resize(n);
-    std::vector<rq::DevLinSys> byIndex(n);
-    long wsMax = 0;
-    for (int s = 0; s < n; ++s) {
-        const rq::LinSysHost &h = H[s];
-        rq::DevLinSys &d = byIndex[s];
-        std::memset(&d, 0, sizeof(d));
-        const int nl = static_cast<int>(h.lev.size());
-        if (nl > rq::kLinMaxLevels)
-            throw RqError(RQ_E_UNSUPPORTED, "AMG hierarchy deeper than 16 levels");
-        d.n = h.n;
-        d.nlev = nl;
-        d.kind = kind;
-        d.precision = mixed && kind != rq::kLinBicgstab ? 1 : 0;
-        d.m = h.m;
-        long lvecs = 0;
-        for (int l = 0; l < nl; ++l) {
-            const rq::LinLevelHost &lv = h.lev[l];
-            rq::DevLinLevel &dl = d.lev[l];
-            dl.n = lv.n;
-            dl.nc = lv.nc;
-            dl.vecOff = l > 0 ? lvecs : 0;
-            if (l > 0)
-                lvecs += 3L * lv.n;
-            addI(s, l, P_PTR, lv.ptr);
-            addI(s, l, P_COL, lv.col);
-            addD(s, l, P_VAL, lv.val);
-            addD(s, l, P_RDG, lv.rdg);
-            if (d.precision) {
-                addF(s, l, P_VAL32, lv.val);
-                addF(s, l, P_RDG32, lv.rdg);
-            }
-            if (l + 1 < nl) {
-                addI(s, l, P_AGG, lv.agg);
-                addI(s, l, P_CPTR, lv.childPtr);
-                addI(s, l, P_CIDX, lv.childIdx);
-            }
-            L.totalNnz += static_cast<int64_t>(lv.col.size());
-        }
-        if (kind == rq::kLinAmg) {
-            addD(s, 0, P_INV, h.inv);
-            if (d.precision)
-                addF(s, 0, P_INV32, h.inv);
-        }
-        const long nn = h.n;
-        d.lvOff = pad32(8 * nn);
-        d.f32Off = d.lvOff + pad32(lvecs);
-        d.lvOff32 = 2 * pad32((6 * nn + 1) / 2);
-        const long ws = d.f32Off + (d.precision ? (d.lvOff32 / 2 + pad32((lvecs + 1) / 2)) : 0);
-        wsMax = std::max(wsMax, ws);
-        L.rows[s] = h.n;
-        L.xOff[s] = L.totalRows;
-        L.totalRows += h.n;
-        L.maxLevels = std::max(L.maxLevels, nl);
-    }
-    std::unique_ptr<int32_t[]> I(new int32_t[std::max<size_t>(nI, 1)]);
-    std::unique_ptr<double[]> D(new double[std::max<size_t>(nD, 1)]);
-    std::unique_ptr<float[]> F(new float[std::max<size_t>(nF, 1)]);
-    std::unique_ptr<double[]> hb(new double[std::max<int64_t>(L.totalRows, 1)]);
-    {
-        const int nt = std::max(1, std::min<int>(static_cast<int>(pieces.size()),
-                                                 static_cast<int>(std::thread::hardware_concurrency())));
-        std::atomic<size_t> next{0};
-        std::atomic<int> nextRhs{0};
-        auto work = [&] {
-            for (size_t k = next++; k < pieces.size(); k = next++) {
-                const Piece &p = pieces[k];
-                switch (p.what) {
-                case P_PTR: case P_COL: case P_AGG: case P_CPTR: case P_CIDX: {
-                    const auto &v = *static_cast<const std::vector<int> *>(p.src);
-                    std::copy(v.begin(), v.end(), I.get() + p.off);
-                    std::fill(I.get() + p.off + v.size(), I.get() + p.off + (v.size() + 7) / 8 * 8, 0);
-                    break;
-                }
-                case P_VAL: case P_RDG: case P_INV: {
-                    const auto &v = *static_cast<const std::vector<double> *>(p.src);
-                    std::copy(v.begin(), v.end(), D.get() + p.off);
-                    std::fill(D.get() + p.off + v.size(), D.get() + p.off + (v.size() + 3) / 4 * 4, 0.0);
-                    break;
-                }
-                default: {
-                    const auto &v = *static_cast<const std::vector<double> *>(p.src);
-                    for (size_t e = 0; e < v.size(); ++e)
-                        F[p.off + e] = static_cast<float>(v[e]);
-                    std::fill(F.get() + p.off + v.size(), F.get() + p.off + (v.size() + 7) / 8 * 8, 0.0f);
-                }
-                }
-            }
-            for (int s = nextRhs++; s < n; s = nextRhs++)
-                std::memcpy(hb.get() + L.xOff[s], systems[s].source, sizeof(double) * L.rows[s]);
-        };
-        std::vector<std::thread> pool;
-        for (int t = 1; t < nt; ++t)
-            pool.emplace_back(work);
-        work();
-        for (auto &t : pool)
-            t.join();
-    }
-    L.dI.ensure(std::max<size_t>(nI, 1) * sizeof(int32_t));
-    L.dD.ensure(std::max<size_t>(nD, 1) * sizeof(double));
-    L.dF.ensure(std::max<size_t>(nF, 1) * sizeof(float));
-    check(cudaMemcpy(L.dI.p, I.get(), nI * sizeof(int32_t), cudaMemcpyHostToDevice), "upload");
-    check(cudaMemcpy(L.dD.p, D.get(), nD * sizeof(double), cudaMemcpyHostToDevice), "upload");
-    if (nF)
-        check(cudaMemcpy(L.dF.p, F.get(), nF * sizeof(float), cudaMemcpyHostToDevice), "upload");
-    for (const Piece &p : pieces) {
-        rq::DevLinSys &d = byIndex[p.s];
-        rq::DevLinLevel &dl = d.lev[p.l];
-        const int32_t *ip = L.dI.as<int32_t>() + p.off;
-        const double *dp = L.dD.as<double>() + p.off;
-        const float *fp = L.dF.as<float>() + p.off;
-        switch (p.what) {
-        case P_PTR: dl.ptr = ip; break;
-        case P_COL: dl.col = ip; break;
-        case P_VAL: dl.val = dp; break;
-        case P_RDG: dl.rdg = dp; break;
-        case P_VAL32: dl.val32 = fp; break;
-        case P_RDG32: dl.rdg32 = fp; break;
-        case P_AGG: dl.agg = ip; break;
-        case P_CPTR: dl.childPtr = ip; break;
-        case P_CIDX: dl.childIdx = ip; break;
-        case P_INV: d.inv = dp; break;
-        case P_INV32: d.inv32 = fp; break;
-        }
-    }
-    // right-hand sides (gathered above), solutions and results
-    L.dB.ensure(sizeof(double) * L.totalRows);
-    L.dX.ensure(sizeof(double) * L.totalRows);
-    L.dOut.ensure(sizeof(rq::LinOut) * n);
-    check(cudaMemcpy(L.dB.p, hb.get(), sizeof(double) * L.totalRows, cudaMemcpyHostToDevice), "rhs");
-    for (int s = 0; s < n; ++s) {
-        byIndex[s].b = L.dB.as<double>() + L.xOff[s];
-        byIndex[s].x = L.dX.as<double>() + L.xOff[s];
-        byIndex[s].out = L.dOut.as<rq::LinOut>() + s;
-    }
-    // queue order: largest systems first (longest-processing-time)
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return L.rows[a] > L.rows[b]; });
-    L.sys.clear();
-    for (int s : order)
-        L.sys.push_back(byIndex[s]);
-    int dev = 0, sms = 1;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-    const int perSM = std::max(1, rq::linBlocksPerSM());
-    L.grid = std::max(1, std::min(n, sms * perSM));
-    L.wsStride = wsMax;
-    L.dWs.ensure(sizeof(double) * wsMax * L.grid);
-    L.dSys.ensure(sizeof(rq::DevLinSys) * n);
-    L.dNext.ensure(sizeof(int));
-}
-
-void launchLinsys(rq_linsys &L, int maxIter, double tol, cudaStream_t stream) {
-    for (auto &d : L.sys) {
-        d.maxIter = maxIter;
-        d.tol = tol;
-    }
-    check(cudaMemcpyAsync(L.dSys.p, L.sys.data(), sizeof(rq::DevLinSys) * L.nsys,
-                          cudaMemcpyHostToDevice, stream), "systems");
-    check(cudaMemsetAsync(L.dNext.p, 0, sizeof(int), stream), "counter");
-    check(rq::launchLinear(L.dSys.as<rq::DevLinSys>(), L.nsys, L.dNext.as<int>(),
-                           L.dWs.as<double>(), L.wsStride, L.grid, stream), "linear solve launch");
-}
-
-void fetchLinsys(rq_linsys &L, double *const *x, rq_solver_result *results) {
-    static_assert(sizeof(rq::LinOut) == sizeof(rq_solver_result), "result layout");
-    if (results)
-        check(cudaMemcpy(results, L.dOut.p, sizeof(rq::LinOut) * L.nsys, cudaMemcpyDeviceToHost),
-              "results");
-    if (x) {
-        std::vector<double> hx(L.totalRows);
-        check(cudaMemcpy(hx.data(), L.dX.p, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost), "x");
-        for (int s = 0; s < L.nsys; ++s)
-            std::memcpy(x[s], hx.data() + L.xOff[s], sizeof(double) * L.rows[s]);
-    }
 }
 
 } // namespace
@@ -1189,197 +743,6 @@ int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells) 
     });
 }
 
-int rq_server_create(rq_problem *const *problems, int32_t n_problems, int32_t capacity,
-                     double idle_timeout_s, int32_t max_slots, rq_server **out) {
-    return guarded([&] {
-        if (!problems || n_problems < 1 || !out)
-            throw std::invalid_argument("null argument");
-        *out = nullptr;
-        if (capacity < 1)
-            throw std::invalid_argument("server capacity must be positive");
-        if (!std::isfinite(idle_timeout_s) || idle_timeout_s <= 0 || idle_timeout_s > 600)
-            throw std::invalid_argument("idle timeout must be in (0, 600] seconds");
-        if (max_slots < 0)
-            throw std::invalid_argument("max_slots must be nonnegative");
-        auto S = std::make_unique<rq_server>();
-        std::vector<const rq_problem *> cp;
-        long ws = 0;
-        for (int i = 0; i < n_problems; ++i) {
-            if (!problems[i])
-                throw std::invalid_argument("null problem");
-            S->problems.push_back(problems[i]);
-            cp.push_back(problems[i]);
-            S->thetaStride = std::max<int>(S->thetaStride, static_cast<int>(problems[i]->active.size()));
-            S->predStride = std::max(S->predStride, problems[i]->nObs);
-            ws = std::max(ws, static_cast<long>(problems[i]->cls.wsDoubles));
-        }
-        S->capacity = capacity;
-        S->wsStride = ws;
-        S->idleNs = static_cast<long long>(idle_timeout_s * 1e9);
-        S->arena = chooseArena(cp);
-        int dev = 0, sms = 1;
-        check(cudaGetDevice(&dev), "cudaGetDevice");
-        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attribute");
-        const int perSM = rq::serveBlocksPerSM(S->block, S->arena);
-        if (perSM < 1)
-            throw RqError(RQ_E_CUDA, "serve kernel does not fit on an SM with this arena");
-        // admission by free HBM: as many solve slots as the SMs hold and free memory allows
-        size_t freeB = 0, totalB = 0;
-        check(cudaMemGetInfo(&freeB, &totalB), "cudaMemGetInfo");
-        const long byMem = static_cast<long>(0.8 * static_cast<double>(freeB) / (8.0 * ws));
-        long slots = std::min<long>(static_cast<long>(sms) * perSM, byMem);
-        if (max_slots > 0)
-            slots = std::min<long>(slots, max_slots);
-        if (slots < 1)
-            throw RqError(RQ_E_OOM, "free device memory holds no solve slot");
-        S->grid = static_cast<int>(slots);
-        S->dWs.ensure(sizeof(double) * ws * S->grid);
-        S->dCtl.ensure(2 * sizeof(int));
-        check(cudaMemset(S->dCtl.p, 0, 2 * sizeof(int)), "server counters");
-        const size_t c = static_cast<size_t>(capacity);
-        auto up = [](size_t b) { return (b + 255) / 256 * 256; };
-        const size_t oJobs = 0, oTheta = oJobs + up(c * sizeof(rq::DevJob)),
-                     oRows = oTheta + up(c * S->thetaStride * sizeof(double)),
-                     oPred = oRows + up(c * sizeof(rq::RowOut)),
-                     oClock = oPred + up(c * S->predStride * sizeof(double)),
-                     oDone = oClock + up(c * 12 * sizeof(long long)),
-                     oCtl = oDone + up(c * sizeof(int)), total = oCtl + 256;
-        S->host.alloc(total);
-        char *base = static_cast<char *>(S->host.p);
-        S->jobs = reinterpret_cast<rq::DevJob *>(base + oJobs);
-        S->theta = reinterpret_cast<double *>(base + oTheta);
-        S->rows = reinterpret_cast<rq::RowOut *>(base + oRows);
-        S->pred = reinterpret_cast<double *>(base + oPred);
-        S->clock = reinterpret_cast<long long *>(base + oClock);
-        S->done = reinterpret_cast<int *>(base + oDone);
-        S->published = reinterpret_cast<int *>(base + oCtl);
-        S->closed = S->published + 1;
-        // unified addressing: the mapped host pointers are also the device pointers
-        void *dp = nullptr;
-        check(cudaHostGetDevicePointer(&dp, S->host.p, 0), "mapped pointer");
-        if (dp != S->host.p)
-            throw RqError(RQ_E_UNSUPPORTED, "serving needs unified virtual addressing");
-        check(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking), "stream");
-        check(cudaDeviceSynchronize(), "server set-up");
-        S->launch();
-        *out = S.release();
-    });
-}
-
-int rq_server_submit(rq_server *s, int32_t problem, const double *theta, int64_t *ticket) {
-    return guarded([&] {
-        if (!s || !theta || !ticket)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(s->mu);
-        if (__atomic_load_n(s->closed, __ATOMIC_ACQUIRE))
-            throw std::invalid_argument("server is closed");
-        if (problem < 0 || problem >= static_cast<int>(s->problems.size()))
-            throw std::invalid_argument("problem index out of range");
-        if (s->submitted >= s->capacity)
-            throw std::invalid_argument("server capacity reached");
-        const int t = s->submitted;
-        const rq_problem &P = *s->problems[problem];
-        double *th = s->theta + static_cast<long>(t) * s->thetaStride;
-        for (size_t a = 0; a < P.active.size(); ++a)
-            th[a] = theta[a];
-        rq::DevJob &j = s->jobs[t];
-        j.cls = P.dCls.as<rq::DevClass>();
-        j.theta = th;
-        j.row = s->rows + t;
-        j.pred = s->pred + static_cast<long>(t) * s->predStride;
-        j.fields = nullptr;
-        j.hist = nullptr;
-        j.clock = s->clock + 12L * t;
-        j.histCap = 0;
-        s->submitted = t + 1;
-        __atomic_store_n(s->published, t + 1, __ATOMIC_RELEASE);
-        s->ensureRunning();
-        *ticket = t;
-    });
-}
-
-int rq_server_poll(rq_server *s, int64_t ticket, int32_t *done, rq_row_out *row,
-                   double *predictions, int64_t *clock12) {
-    return guarded([&] {
-        if (!s || !done)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(s->mu);
-        if (ticket < 0 || ticket >= s->submitted)
-            throw std::invalid_argument("unknown ticket");
-        *done = __atomic_load_n(s->done + ticket, __ATOMIC_ACQUIRE) ? 1 : 0;
-        if (!*done) {
-            s->ensureRunning();
-            return;
-        }
-        if (row)
-            *row = toRow(s->rows[ticket]);
-        if (predictions)
-            std::memcpy(predictions, s->pred + ticket * s->predStride,
-                        sizeof(double) * s->predStride);
-        if (clock12)
-            std::memcpy(clock12, s->clock + 12 * ticket, sizeof(long long) * 12);
-    });
-}
-
-int rq_server_wait(rq_server *s, double timeout_s, int64_t *completed) {
-    return guarded([&] {
-        if (!s)
-            throw std::invalid_argument("null argument");
-        const auto t0 = std::chrono::steady_clock::now();
-        for (;;) {
-            {
-                std::lock_guard<std::mutex> lock(s->mu);
-                int64_t n = 0;
-                for (int i = 0; i < s->submitted; ++i)
-                    n += __atomic_load_n(s->done + i, __ATOMIC_ACQUIRE) ? 1 : 0;
-                if (completed)
-                    *completed = n;
-                if (n == s->submitted)
-                    return;
-                s->ensureRunning();
-            }
-            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            if (el >= timeout_s)
-                return;
-            std::this_thread::sleep_for(std::chrono::microseconds(200));
-        }
-    });
-}
-
-int rq_server_close(rq_server *s) {
-    return guarded([&] {
-        if (!s)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(s->mu);
-        __atomic_store_n(s->closed, 1, __ATOMIC_RELEASE);
-    });
-}
-
-int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *completed,
-                   int32_t *launches) {
-    return guarded([&] {
-        if (!s)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(s->mu);
-        if (slots)
-            *slots = s->grid;
-        if (submitted)
-            *submitted = s->submitted;
-        if (completed) {
-            int64_t n = 0;
-            for (int i = 0; i < s->submitted; ++i)
-                n += __atomic_load_n(s->done + i, __ATOMIC_ACQUIRE) ? 1 : 0;
-            *completed = n;
-        }
-        if (launches)
-            *launches = s->launches;
-    });
-}
-
-int rq_server_destroy(rq_server *s) {
-    return guarded([&] { delete s; });
-}
-
 int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_dev,
                         double *predictions_dev, void *stream) {
     return guarded([&] {
@@ -1438,117 +801,6 @@ int rq_posterior_weights_device(const double *loglik_dev, const double *log_q_de
         check(rq::launchWeights(loglik_dev, log_q_dev, n, weights_dev, out3_dev,
                                 static_cast<cudaStream_t>(stream)), "weights launch");
     });
-}
-
-int rq_linsys_create(const rq_ldu *systems, int32_t n_systems, int32_t kind, int32_t precision,
-                     rq_linsys **out) {
-    return guarded([&] {
-        if (!systems || n_systems < 1 || !out)
-            throw std::invalid_argument("null argument");
-        *out = nullptr;
-        if (kind == 3)
-            throw RqError(RQ_E_UNSUPPORTED, "the Gauss-Seidel solver is not on the GPU path");
-        if (kind < 0 || kind > 2)
-            throw std::invalid_argument("unknown linear solver kind");
-        if (precision != RQ_PREC_FP64 && precision != RQ_PREC_MIXED)
-            throw std::invalid_argument("unknown precision");
-        auto L = std::make_unique<rq_linsys>();
-        buildLinsys(*L, systems, n_systems, kind, precision);
-        *out = L.release();
-    });
-}
-
-int rq_linsys_solve(rq_linsys *L, int32_t max_iter, double tol, double *const *x,
-                    rq_solver_result *results) {
-    return guarded([&] {
-        if (!L)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(L->mu);
-        checkSolveArgs(max_iter, tol);
-        if (x)
-            for (int s = 0; s < L->nsys; ++s) {
-                if (!x[s])
-                    throw std::invalid_argument("null initial guess");
-                for (int i = 0; i < L->rows[s]; ++i)
-                    if (!std::isfinite(x[s][i]))
-                        throw std::invalid_argument("linear solve initial values must be finite");
-            }
-        if (x) {
-            std::vector<double> hx(L->totalRows);
-            for (int s = 0; s < L->nsys; ++s)
-                std::memcpy(hx.data() + L->xOff[s], x[s], sizeof(double) * L->rows[s]);
-            check(cudaMemcpy(L->dX.p, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice), "x");
-        } else {
-            check(cudaMemset(L->dX.p, 0, sizeof(double) * L->totalRows), "x");
-        }
-        launchLinsys(*L, max_iter, tol, nullptr);
-        check(cudaStreamSynchronize(nullptr), "linear solve");
-        fetchLinsys(*L, x, results);
-    });
-}
-
-int rq_linsys_solve_device(rq_linsys *L, int32_t max_iter, double tol, void *stream) {
-    return guarded([&] {
-        if (!L)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(L->mu);
-        checkSolveArgs(max_iter, tol);
-        const cudaStream_t st = static_cast<cudaStream_t>(stream);
-        check(cudaMemsetAsync(L->dX.p, 0, sizeof(double) * L->totalRows, st), "x");
-        launchLinsys(*L, max_iter, tol, st);
-    });
-}
-
-int rq_linsys_results(rq_linsys *L, rq_solver_result *results, double *const *x) {
-    return guarded([&] {
-        if (!L)
-            throw std::invalid_argument("null argument");
-        std::lock_guard<std::mutex> lock(L->mu);
-        check(cudaDeviceSynchronize(), "linear solve");
-        fetchLinsys(*L, x, results);
-    });
-}
-
-int rq_linsys_info(const rq_linsys *L, int32_t *n_systems, int64_t *total_rows, int64_t *total_nnz,
-                   int32_t *max_levels) {
-    return guarded([&] {
-        if (!L)
-            throw std::invalid_argument("null argument");
-        if (n_systems)
-            *n_systems = L->nsys;
-        if (total_rows)
-            *total_rows = L->totalRows;
-        if (total_nnz)
-            *total_nnz = L->totalNnz;
-        if (max_levels)
-            *max_levels = L->maxLevels;
-    });
-}
-
-int rq_linsys_destroy(rq_linsys *L) {
-    return guarded([&] { delete L; });
-}
-
-int rq_linear_solve_batch(const rq_ldu *systems, int32_t n_systems, double *const *x,
-                          int32_t max_iter, double tol, int32_t kind, int32_t precision,
-                          rq_solver_result *results) {
-    rq_linsys *L = nullptr;
-    int rc = rq_linsys_create(systems, n_systems, kind, precision, &L);
-    if (rc != RQ_OK)
-        return rc;
-    rc = rq_linsys_solve(L, max_iter, tol, x, results);
-    rq_linsys_destroy(L);
-    return rc;
-}
-
-int rq_linear_solve(const rq_ldu *A, double *x, int32_t max_iter, double tol, int32_t kind,
-                    rq_solver_result *result) {
-    if (!x) {
-        g_error = "null argument";
-        return RQ_E_INVALID;
-    }
-    double *xs[1] = {x};
-    return rq_linear_solve_batch(A, 1, xs, max_iter, tol, kind, RQ_PREC_FP64, result);
 }
 
 } // extern "C"
