@@ -42,7 +42,7 @@ struct Work {
     double *r, *rh, *pv, *v, *s, *t, *ph, *sh;
     double *z, *xa, *xb, *rr;                // PCG / level-0 V-cycle
     double *rd;                              // reciprocal diagonal of the system being solved
-    double *amgVal, *amgVec, *dense0, *dense1;
+    double *amgVal, *amgVec, *dense0;
 };
 
 // Krylov / AMG storage of one value type (see "inner linear solvers").
@@ -52,7 +52,6 @@ template <typename T> struct KW {
     T *z, *xa, *xb, *rr;                  // PCG / level-0 V-cycle (share BiCGSTAB-only storage)
     T *x;                                 // FP32 correction of the mixed form
     T *amgVal, *amgVec;                   // coarse levels: values; b, xa, xb, r, 1/diag
-    T *coarse;                            // inverse of a coarsest level of <= 32 rows
 };
 
 struct Shared {
@@ -74,7 +73,6 @@ struct Shared {
     long long tmark;
     int wallBetaInit; // the wall-face omega still carries applyAllBCs' beta1
     double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
-    float coarse32[32 * 32];              // its FP32 copy (mixed form)
 };
 
 // stage timers, as the reference's momentum / pressure / turbulence timers
@@ -405,9 +403,9 @@ template <typename T> __device__ __forceinline__ T level0EntryT(const KW<T> &K, 
 
 // Galerkin values of every coarse level from the current pressure system, the
 // reciprocal diagonals of the smoothed levels, then the inverse of the coarsest
-// level: in place by one warp (Gauss-Jordan, SPD: no pivoting) when it has at
-// most 32 rows, else by the whole CTA with ping-pong buffers. The inversion
-// itself is always FP64; the mixed form stores the result in FP32.
+// level (at most 64 rows) in place by one warp (Gauss-Jordan, SPD: no pivoting),
+// in shared memory up to 32 rows and in the workspace above. The inverse is FP64
+// in both forms.
 template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
@@ -436,108 +434,67 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
             rdl[i] = T(1) / val[__ldg(Lv.diagPos + i)];
     }
     const DevAmgLevel &Q = C.lev[L - 1];
-    const int m = Q.n;
+    const int m = Q.n; // at most kMaxCoarse = 64 rows (the set-up rejects more)
     const T *qv = K.amgVal + Q.valOff;
-    if (m <= 32) {
-        double *a = S.coarse;
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x)
-            a[e] = 0.0;
-        __syncthreads();
-        if (L == 1) {
-            for (int r = threadIdx.x; r < m; r += blockDim.x) {
-                const Cell q = cellOf(C, r);
-                a[r * m + r] += double(K.d[r]);
-                a[r * m + q.W] += double(K.aW[r]);
-                a[r * m + q.E] += double(K.aE[r]);
-                if (q.south)
-                    a[r * m + r - C.nx] += double(K.aS[r]);
-                if (q.north)
-                    a[r * m + r + C.nx] += double(K.aN[r]);
-            }
-        } else {
-            for (int r = threadIdx.x; r < m; r += blockDim.x)
-                for (int k = 0; k < Q.width; ++k) {
-                    const int c = __ldg(Q.ecol + k * m + r);
-                    if (c >= 0)
-                        a[r * m + c] = double(qv[k * m + r]);
-                }
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const int r = threadIdx.x;
-            for (int k = 0; k < m; ++k) {
-                const double p = 1.0 / a[k * m + k];
-                const double f = (r < m) ? a[r * m + k] : 0.0;
-                __syncwarp();
-                if (r < m && r != k) {
-                    for (int j = 0; j < m; ++j)
-                        if (j != k)
-                            a[r * m + j] -= f * a[k * m + j] * p;
-                    a[r * m + k] = -f * p;
-                }
-                __syncwarp();
-                if (r == k) {
-                    for (int j = 0; j < m; ++j)
-                        if (j != k)
-                            a[k * m + j] *= p;
-                    a[k * m + k] = p;
-                }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        if (!std::is_same<T, double>::value) {
-            for (int e = threadIdx.x; e < m * m; e += blockDim.x)
-                K.coarse[e] = T(a[e]);
-            __syncthreads();
-        }
-        return;
-    }
-    const int m2 = 2 * m;
-    double *A0 = W.dense0, *A1 = W.dense1;
-    for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
-        A0[e] = ((e % m2) == m + e / m2) ? 1.0 : 0.0;
+    // row-major m x m: shared memory up to 32 rows, the workspace's dense0 above
+    double *a = (m <= 32) ? S.coarse : W.dense0;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x)
+        a[e] = 0.0;
     __syncthreads();
     if (L == 1) {
         for (int r = threadIdx.x; r < m; r += blockDim.x) {
             const Cell q = cellOf(C, r);
-            A0[r * m2 + r] += double(K.d[r]);
-            A0[r * m2 + q.W] += double(K.aW[r]);
-            A0[r * m2 + q.E] += double(K.aE[r]);
+            a[r * m + r] += double(K.d[r]);
+            a[r * m + q.W] += double(K.aW[r]);
+            a[r * m + q.E] += double(K.aE[r]);
             if (q.south)
-                A0[r * m2 + r - C.nx] += double(K.aS[r]);
+                a[r * m + r - C.nx] += double(K.aS[r]);
             if (q.north)
-                A0[r * m2 + r + C.nx] += double(K.aN[r]);
+                a[r * m + r + C.nx] += double(K.aN[r]);
         }
     } else {
         for (int r = threadIdx.x; r < m; r += blockDim.x)
             for (int k = 0; k < Q.width; ++k) {
                 const int c = __ldg(Q.ecol + k * m + r);
                 if (c >= 0)
-                    A0[r * m2 + c] = double(qv[k * m + r]);
+                    a[r * m + c] = double(qv[k * m + r]);
             }
     }
     __syncthreads();
-    for (int piv = 0; piv < m; ++piv) {
-        const double inv = 1.0 / A0[piv * m2 + piv];
-        for (int e = threadIdx.x; e < m * m2; e += blockDim.x) {
-            const int r = e / m2, col = e - r * m2;
-            const double pr = A0[piv * m2 + col] * inv;
-            A1[e] = (r == piv) ? pr : A0[e] - A0[r * m2 + piv] * pr;
+    // in-place Gauss-Jordan inverse by one warp (SPD: no pivoting), rows lane and
+    // lane + 32; warp barriers only (a CTA barrier per pivot cost more)
+    if (threadIdx.x < 32) {
+        const int r0 = threadIdx.x, r1 = threadIdx.x + 32;
+        for (int k = 0; k < m; ++k) {
+            const double p = 1.0 / a[k * m + k];
+            const double f0 = (r0 < m) ? a[r0 * m + k] : 0.0;
+            const double f1 = (r1 < m) ? a[r1 * m + k] : 0.0;
+            __syncwarp();
+            if (r0 < m && r0 != k) {
+                for (int j = 0; j < m; ++j)
+                    if (j != k)
+                        a[r0 * m + j] -= f0 * a[k * m + j] * p;
+                a[r0 * m + k] = -f0 * p;
+            }
+            if (r1 < m && r1 != k) {
+                for (int j = 0; j < m; ++j)
+                    if (j != k)
+                        a[r1 * m + j] -= f1 * a[k * m + j] * p;
+                a[r1 * m + k] = -f1 * p;
+            }
+            __syncwarp();
+            if (r0 == k || r1 == k) {
+                for (int j = 0; j < m; ++j)
+                    if (j != k)
+                        a[k * m + j] *= p;
+                a[k * m + k] = p;
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        double *tmp = A0;
-        A0 = A1;
-        A1 = tmp;
     }
-    if (A0 != W.dense0) { // keep the inverse in dense0
-        for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
-            W.dense0[e] = A0[e];
-        __syncthreads();
-    }
+    __syncthreads();
 }
 
-// row i of an ELL level times x, entries in column order
 template <typename T>
 __device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
     T s = T(0);
@@ -621,7 +578,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     // the coarsest level: restriction of the level above, then the dense inverse
     auto coarsest = [&]() {
         const int l = L - 1;
-        const int m = C.lev[l].n, m2 = 2 * m;
+        const int m = C.lev[l].n;
         T *b = vb(l), *xb = b + 2 * m;
         if (L == 1) {
             for (int i = t0; i < m; i += ts)
@@ -642,7 +599,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         // copy of its inverse loses the coarse correction
         for (int i = t0; i < m; i += ts) {
             double s = 0.0;
-            const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
+            const double *row = ((m <= 32) ? S.coarse : W.dense0) + i * m;
             for (int j = 0; j < m; ++j)
                 s += row[j] * double(b[j]);
             xb[i] = T(s);
@@ -1047,7 +1004,6 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
         F.xa = F.t;
         F.xb = F.sh;
         F.rr = F.rh;
-        F.coarse = S.coarse32;
     }
     // tier 1: matrix and Krylov vectors
     W.d = take(n);
@@ -1114,8 +1070,7 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.Uyp = take(n);
     W.kOld = take(n);
     W.wOld = take(n);
-    W.dense0 = take(2L * m * m);
-    W.dense1 = take(2L * m * m);
+    W.dense0 = take(static_cast<long>(m) * m); // coarsest inverse when above 32 rows
     if (mixed) {
         W.ph = W.s = W.sh = W.t = W.rh = nullptr;
         W.xa = W.xb = W.rr = W.amgVec = W.amgVal = nullptr;
@@ -1142,7 +1097,6 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     K.x = nullptr;
     K.amgVal = W.amgVal;
     K.amgVec = W.amgVec;
-    K.coarse = S.coarse;
 }
 
 // Locals shared by the phase functions (read from the CTA's shared state).
