@@ -236,6 +236,44 @@ def solve(case: Case, kind: str = "ref", hist_cap: int = 0) -> SolveOut:
                     pred[: len(case.obs_x)], hist[:nh])
 
 
+@dataclass
+class SequenceOut:
+    """One ForwardModel's calls in order: verdicts, iterations, log-likelihoods,
+    predictions (calls x probes), whether each call started warm, and the warm-start
+    cache's retained bytes after each call."""
+    status: list
+    iterations: np.ndarray
+    loglik: np.ndarray
+    predictions: np.ndarray
+    used_warm: np.ndarray
+    retained: np.ndarray
+
+
+def solve_sequence(case: Case, thetas, kind: str = "ref", max_size: int = 50,
+                   threshold: float = 0.5, byte_budget: int = 64 * 1024 * 1024) -> SequenceOut:
+    """Evaluate theta rows (a1, betaStar) one after another on ONE ForwardModel with its
+    warm-start cache, through the reference ('ref') or the restatement ('oracle')."""
+    L = lib(kind)
+    fn = L.ref_solve_sequence if kind == "ref" else L.orc_solve_sequence
+    th = np.ascontiguousarray(np.asarray(thetas, dtype=np.float64).reshape(-1, 2))
+    m = len(th)
+    s, keep = case.struct()
+    res = (OrcResult * m)()
+    nobs = len(case.obs_x)
+    pred = np.zeros((m, max(nobs, 1)))
+    used = np.zeros(m, dtype=np.int32)
+    kept = np.zeros(m, dtype=np.int64)
+    rc = fn(C.byref(s), _dptr(th), C.c_int32(m), C.c_int32(max_size), C.c_double(threshold),
+            C.c_int64(byte_budget), res, _dptr(pred), used.ctypes.data_as(C.POINTER(C.c_int32)),
+            kept.ctypes.data_as(C.POINTER(C.c_int64)))
+    if rc != 0:
+        err = (L.ref_last_error if kind == "ref" else L.orc_last_error)
+        err.restype = C.c_char_p
+        raise RuntimeError(err().decode())
+    return SequenceOut([STATUS[r.status] for r in res], np.array([r.iterations for r in res]),
+                       np.array([r.loglik for r in res]), pred[:, :nobs], used.astype(bool), kept)
+
+
 def mesh(case: Case, kind: str = "ref"):
     """Cell (cx, cy, vol, wd) and face (owner, nbr, cx, cy, nx, ny, area, delta, dx, dy,
     weight, shift_x, patch) arrays of the mesh as the checker builds it."""
@@ -277,5 +315,5 @@ def rel_err(a, b) -> float:
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-__all__ = ["Case", "config1_case", "channel_probes", "solve", "mesh", "linear_solve", "have",
+__all__ = ["Case", "config1_case", "channel_probes", "solve", "solve_sequence", "mesh", "linear_solve", "have",
            "rel_err", "DEFAULT_COEFFS", "P_AMG", "P_PCG", "P_BICGSTAB", "FIELD_NAMES", "math"]

@@ -187,6 +187,61 @@ int ref_solve(const orc_case *c, orc_result *res, double *fields, double *predic
     }
 }
 
+// A sequence of evaluateWithDiagnostics calls on ONE ForwardModel, whose warm-start
+// cache (ForwardModel.hpp:21-157; the model builds it as cache_(50, 0.5),
+// ForwardModel.cpp:14) seeds each call from the nearest converged state. Only the
+// byte budget can be changed after construction (setByteBudget), so max_size and
+// threshold must be the model's own 50 and 0.5.
+int ref_solve_sequence(const orc_case *c, const double *thetas, int32_t m_calls, int32_t max_size,
+                       double threshold, int64_t byte_budget, orc_result *res,
+                       double *predictions, int32_t *used_warm, int64_t *retained) {
+    try {
+        if (max_size != 50 || threshold != 0.5)
+            throw std::invalid_argument("the reference model's cache is (50, 0.5)");
+        std::streambuf *old = std::cout.rdbuf(nullptr);
+        Mesh mesh = buildMesh(*c);
+        std::cout.rdbuf(old);
+        mesh.computeWallDistance();
+        auto bcs = FlowBoundaryConditions::channelDefaults(mesh, c->bc_u, c->bc_k, c->bc_w);
+        ObservationOperator obs;
+        for (int i = 0; i < c->n_obs; ++i)
+            obs.addVelocityProfile(Vec3(c->obs_x[i], c->obs_y[i], 0.0), c->obs_component,
+                                   c->obs_value[i], c->obs_sigma[i]);
+        auto params = InferenceParameterSet::a1_betaStar();
+        params.base = InferenceParameterSet::fromVector(std::vector<double>(c->coeffs, c->coeffs + 11));
+        ForwardModel model(mesh, params, obs, bcs, c->nu, buildSettings(*c),
+                           Vec3(c->init_u[0], c->init_u[1], c->init_u[2]), c->init_p, c->init_k,
+                           c->init_w);
+        model.cache().setByteBudget(static_cast<size_t>(byte_budget));
+        for (int i = 0; i < m_calls; ++i) {
+            std::vector<double> theta = {thetas[2 * i], thetas[2 * i + 1]};
+            auto ev = model.evaluateWithDiagnostics(theta);
+            if (!ev.error.empty())
+                lastError = ev.error;
+            orc_result &r = res[i];
+            std::memset(&r, 0, sizeof(r));
+            r.status = static_cast<int32_t>(ev.result.status);
+            r.iterations = ev.result.simpleIters;
+            r.converged = ev.convergence.converged;
+            r.diverged = ev.convergence.diverged;
+            r.stalled = ev.convergence.stalled;
+            r.loglik = ev.result.loglik;
+            r.final_worst = ev.convergence.finalWorstMeasure;
+            r.contraction_rate = ev.convergence.contractionRateU;
+            used_warm[i] = ev.usedWarmStart;
+            if (predictions)
+                for (size_t k = 0; k < ev.result.predictions.size(); ++k)
+                    predictions[static_cast<size_t>(i) * c->n_obs + k] = ev.result.predictions[k];
+            if (retained)
+                retained[i] = static_cast<int64_t>(model.cache().retainedBytes());
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return -1;
+    }
+}
+
 // The reference linear solvers on one LDU system: kind 0 AMG, 1 PCG, 2 BiCGSTAB,
 // 3 GaussSeidel. x is the initial guess on input and the solution on output.
 int ref_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,

@@ -1732,76 +1732,197 @@ int orc_mesh(const orc_case *c, int32_t *n_cells, int32_t *n_faces, int32_t *n_i
     }
 }
 
+} // extern "C"
+
+namespace orc {
+
 // ForwardModel::evaluateWithDiagnostics (rans-uq/src/ForwardModel.cpp:35-137) for the
-// a1_betaStar parameter set (InferenceParameters.hpp:103-156): bounds, cold start, solve,
-// classification, probe predictions and the Gaussian log-likelihood (ObservationOperator.hpp:592-609).
+// a1_betaStar parameter set (InferenceParameters.hpp:103-156): bounds, cold or warm start,
+// solve, classification, probe predictions and the Gaussian log-likelihood
+// (ObservationOperator.hpp:592-609). theta = (a1, betaStar) replaces coeffs[9], coeffs[8].
+// warm (optional) is a cached state copied in place of initUniform (ForwardModel.cpp:79-82);
+// out (optional) receives the final state of a solve that ran.
+static void evaluateOne(const orc_case *c, const double theta[2], const State *warm, State *out,
+                        orc_result *res, double *fields, double *predictions, double *history,
+                        int32_t hist_cap) {
+    std::memset(res, 0, sizeof(*res));
+    const double a1 = theta[0], bs = theta[1];
+    auto outOf = [](double v, double lo, double hi) {
+        return v < lo || v > hi || std::isnan(v) || std::isinf(v);
+    };
+    if (outOf(a1, 0.1, 0.8) || outOf(bs, 0.01, 0.2)) {
+        res->status = 3;
+        res->loglik = -1e30;
+        return;
+    }
+    double coeffs[11];
+    std::memcpy(coeffs, c->coeffs, sizeof(coeffs));
+    coeffs[9] = a1;
+    coeffs[8] = bs;
+    Mesh m = buildMesh(*c);
+    Settings st{c->max_iter, c->inner_iter, c->conv_window, c->monitor_interval,
+                c->turb_start, c->nut_floor_iters, c->pressure_solver,
+                c->tol, c->inner_tol, c->alpha_u, c->alpha_p, c->alpha_k, c->alpha_w,
+                c->body_force[0], c->body_force[1], c->div_limit, c->k_min, c->k_max,
+                c->omega_min};
+    Solver sv(m, coeffs, c->nu, st);
+    for (int i = 0; i < c->n_obs; ++i) {
+        sv.probes.push_back(prepareProbe(m, c->obs_x[i], c->obs_y[i]));
+        sv.floors.push_back(std::sqrt(c->obs_sigma[i] * c->obs_sigma[i] + 0.0 * 0.0));
+    }
+    State s;
+    if (warm)
+        s = *warm;
+    else
+        sv.init(s, c->init_u, c->init_p, c->init_k, c->init_w);
+    std::vector<std::array<double, ORC_NHIST>> hist;
+    History H = sv.solve(s, history ? &hist : nullptr);
+    res->iterations = H.finalIter;
+    res->converged = H.converged;
+    res->diverged = H.diverged;
+    res->stalled = H.stalled;
+    res->final_worst = H.worst;
+    res->contraction_rate = H.rate;
+    res->n_hist = static_cast<int32_t>(hist.size());
+    if (history)
+        for (int i = 0; i < static_cast<int>(hist.size()) && i < hist_cap; ++i)
+            std::memcpy(history + ORC_NHIST * i, hist[i].data(), sizeof(double) * ORC_NHIST);
+    if (H.diverged) {
+        res->status = 2;
+        res->loglik = -1e6;
+        return;
+    }
+    res->status = H.converged ? 0 : 1;
+    Vec q = sv.observe(s);
+    double ll = 0.0;
+    for (int i = 0; i < c->n_obs; ++i) {
+        if (predictions)
+            predictions[i] = q[i];
+        const double var = c->obs_sigma[i] * c->obs_sigma[i] + 0.0 * 0.0;
+        const double diff = q[i] - c->obs_value[i];
+        ll += -0.5 * diff * diff / var;
+    }
+    res->loglik = ll;
+    if (fields) {
+        const int n = m.nC;
+        const Vec *src[ORC_NFIELD] = {&s.Ux, &s.Uy, &s.Uz, &s.p, &s.k, &s.w,
+                                      &s.nuT, &s.F1, &s.F2, &s.Pk, &s.CD};
+        for (int b = 0; b < ORC_NFIELD; ++b)
+            std::memcpy(fields + static_cast<size_t>(b) * n, src[b]->data(), sizeof(double) * n);
+    }
+    if (out)
+        *out = std::move(s);
+}
+
+// WarmStartCache (rans-uq/include/ForwardModel.hpp:21-157): converged states keyed by theta,
+// FIFO eviction by count and by the payload byte count of entryBytes (:39-47): theta, the
+// vector field and eight scalar fields, each over cells plus boundary faces.
+struct WarmCache {
+    struct Entry {
+        std::array<double, 2> theta;
+        State s;
+        size_t bytes;
+    };
+    int maxSize;
+    double threshold;
+    size_t budget, retained = 0;
+    std::vector<Entry> q; // front = oldest
+
+    static size_t entryBytes(size_t cellsPlusBoundary) {
+        return 2 * sizeof(double) + cellsPlusBoundary * (3 * sizeof(double)) +
+               8 * cellsPlusBoundary * sizeof(double);
+    }
+    const Entry *nearest(const double theta[2]) const { // nearest (:132-144), strict <
+        const Entry *best = nullptr;
+        double bestDist = threshold;
+        for (const Entry &e : q) {
+            const double d0 = theta[0] - e.theta[0], d1 = theta[1] - e.theta[1];
+            const double d = std::sqrt(d0 * d0 + d1 * d1);
+            if (d < bestDist) {
+                bestDist = d;
+                best = &e;
+            }
+        }
+        return best;
+    }
+    void store(const double theta[2], State &&s, size_t nCB) { // store (:70-92)
+        if (!std::isfinite(theta[0]) || !std::isfinite(theta[1]))
+            return;
+        for (size_t i = 0; i < q.size(); ++i)
+            if (q[i].theta[0] == theta[0] && q[i].theta[1] == theta[1]) {
+                retained -= q[i].bytes;
+                q.erase(q.begin() + static_cast<long>(i));
+                break;
+            }
+        const size_t bytes = entryBytes(nCB);
+        if (maxSize == 0 || bytes > budget)
+            return;
+        while (!q.empty() && (q.size() >= static_cast<size_t>(maxSize) || retained > budget - bytes)) {
+            retained -= q.front().bytes;
+            q.erase(q.begin());
+        }
+        q.push_back({{theta[0], theta[1]}, std::move(s), bytes});
+        retained += bytes;
+    }
+};
+
+} // namespace orc
+
+extern "C" {
+
 int orc_solve(const orc_case *c, orc_result *res, double *fields, double *predictions,
               double *history, int32_t hist_cap) {
     try {
-        std::memset(res, 0, sizeof(*res));
-        const double a1 = c->coeffs[9], bs = c->coeffs[8];
-        auto outOf = [](double v, double lo, double hi) {
-            return v < lo || v > hi || std::isnan(v) || std::isinf(v);
-        };
-        if (outOf(a1, 0.1, 0.8) || outOf(bs, 0.01, 0.2)) {
-            res->status = 3;
-            res->loglik = -1e30;
-            return 0;
-        }
-        Mesh m = buildMesh(*c);
-        Settings st{c->max_iter, c->inner_iter, c->conv_window, c->monitor_interval,
-                    c->turb_start, c->nut_floor_iters, c->pressure_solver,
-                    c->tol, c->inner_tol, c->alpha_u, c->alpha_p, c->alpha_k, c->alpha_w,
-                    c->body_force[0], c->body_force[1], c->div_limit, c->k_min, c->k_max,
-                    c->omega_min};
-        Solver sv(m, c->coeffs, c->nu, st);
-        for (int i = 0; i < c->n_obs; ++i) {
-            sv.probes.push_back(prepareProbe(m, c->obs_x[i], c->obs_y[i]));
-            sv.floors.push_back(std::sqrt(c->obs_sigma[i] * c->obs_sigma[i] + 0.0 * 0.0));
-        }
-        State s;
-        sv.init(s, c->init_u, c->init_p, c->init_k, c->init_w);
-        std::vector<std::array<double, ORC_NHIST>> hist;
-        History H = sv.solve(s, history ? &hist : nullptr);
-        res->iterations = H.finalIter;
-        res->converged = H.converged;
-        res->diverged = H.diverged;
-        res->stalled = H.stalled;
-        res->final_worst = H.worst;
-        res->contraction_rate = H.rate;
-        res->n_hist = static_cast<int32_t>(hist.size());
-        if (history)
-            for (int i = 0; i < static_cast<int>(hist.size()) && i < hist_cap; ++i)
-                std::memcpy(history + ORC_NHIST * i, hist[i].data(), sizeof(double) * ORC_NHIST);
-        if (H.diverged) {
-            res->status = 2;
-            res->loglik = -1e6;
-            return 0;
-        }
-        res->status = H.converged ? 0 : 1;
-        Vec q = sv.observe(s);
-        double ll = 0.0;
-        for (int i = 0; i < c->n_obs; ++i) {
-            if (predictions)
-                predictions[i] = q[i];
-            const double var = c->obs_sigma[i] * c->obs_sigma[i] + 0.0 * 0.0;
-            const double diff = q[i] - c->obs_value[i];
-            ll += -0.5 * diff * diff / var;
-        }
-        res->loglik = ll;
-        if (fields) {
-            const int n = m.nC;
-            const Vec *src[ORC_NFIELD] = {&s.Ux, &s.Uy, &s.Uz, &s.p, &s.k, &s.w,
-                                          &s.nuT, &s.F1, &s.F2, &s.Pk, &s.CD};
-            for (int b = 0; b < ORC_NFIELD; ++b)
-                std::memcpy(fields + static_cast<size_t>(b) * n, src[b]->data(), sizeof(double) * n);
-        }
+        const double theta[2] = {c->coeffs[9], c->coeffs[8]};
+        evaluateOne(c, theta, nullptr, nullptr, res, fields, predictions, history, hist_cap);
         return 0;
     } catch (const std::exception &e) {
         orc::lastError = e.what();
         res->status = 4;
         res->loglik = -1e6;
         return 0;
+    }
+}
+
+// A sequence of ForwardModel::evaluateWithDiagnostics calls on one model, with its
+// warm-start cache (ForwardModel.cpp:79-82 lookup, :116-117 store of converged solves):
+// theta row i is (a1, betaStar); used_warm[i] = ForwardEvaluationResult::usedWarmStart.
+// retained[i] (optional) = the cache's retained bytes after call i.
+int orc_solve_sequence(const orc_case *c, const double *thetas, int32_t m_calls, int32_t max_size,
+                       double threshold, int64_t byte_budget, orc_result *res,
+                       double *predictions, int32_t *used_warm, int64_t *retained) {
+    try {
+        WarmCache cache{max_size, threshold, static_cast<size_t>(byte_budget)};
+        Mesh mesh = buildMesh(*c);
+        const size_t nCB = static_cast<size_t>(mesh.nF - mesh.nI) + mesh.nC;
+        for (int i = 0; i < m_calls; ++i) {
+            const double *th = thetas + 2 * i;
+            orc_result &r = res[i];
+            double *pred = predictions ? predictions + static_cast<size_t>(i) * c->n_obs : nullptr;
+            const bool inBounds = !(th[0] < 0.1 || th[0] > 0.8 || th[1] < 0.01 || th[1] > 0.2 ||
+                                    std::isnan(th[0]) || std::isnan(th[1]));
+            const WarmCache::Entry *hit = inBounds ? cache.nearest(th) : nullptr;
+            State warm, out;
+            if (hit)
+                warm = hit->s; // deep copy, as findNearest does
+            used_warm[i] = hit != nullptr;
+            try {
+                evaluateOne(c, th, hit ? &warm : nullptr, &out, &r, nullptr, pred, nullptr, 0);
+            } catch (const std::exception &e) {
+                orc::lastError = e.what();
+                std::memset(&r, 0, sizeof(r));
+                r.status = 4;
+                r.loglik = -1e6;
+            }
+            if (r.status == 0)
+                cache.store(th, std::move(out), nCB);
+            if (retained)
+                retained[i] = static_cast<int64_t>(cache.retained);
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        orc::lastError = e.what();
+        return -1;
     }
 }
 

@@ -10,8 +10,9 @@ from oracle import checker as ck
 
 
 def product_batch(rq, case: ck.Case, pressure_solver: str = "AMG", precision: str = "fp64",
-                  block_threads: int = 0):
-    """A ForwardBatch on the GPU path with the same inputs as the checker case."""
+                  block_threads: int = 0, model_class=None):
+    """A ForwardBatch (or model_class, e.g. rq.ForwardModel) on the GPU path with the same
+    inputs as the checker case."""
     if case.curved:
         mesh = rq.Mesh.make_curved_channel_periodic_2d(case.x_nodes, case.y_bottom, case.y_top,
                                                       case.ny, case.re_mesh, case.yplus)
@@ -34,8 +35,9 @@ def product_batch(rq, case: ck.Case, pressure_solver: str = "AMG", precision: st
         pressure_solver=pressure_solver, precision=precision, block_threads=block_threads)
     params = rq.InferenceParameterSet("a1_betaStar", (9, 8), base=tuple(case.coeffs))
     bcs = rq.FlowBoundaryConditions.channel_defaults(mesh, *case.bc)
-    return rq.ForwardBatch(mesh, params, obs, bcs, case.nu, st, rq.Vec3(*case.init_u),
-                           case.init_p, case.init_k, case.init_w)
+    return (model_class or rq.ForwardBatch)(mesh, params, obs, bcs, case.nu, st,
+                                            rq.Vec3(*case.init_u), case.init_p, case.init_k,
+                                            case.init_w)
 
 
 def small_channel(**kw) -> ck.Case:
@@ -44,6 +46,24 @@ def small_channel(**kw) -> ck.Case:
     base = ck.Case(ny=24, yplus=1.0, tol=1e-8, max_iter=60000, obs_x=x, obs_y=y,
                    obs_value=np.zeros(8), obs_sigma=np.full(8, 1e-3))
     return dataclasses.replace(base, **kw)
+
+
+# Warm-start sequences on small_channel() (one ForwardModel, calls in order), with what
+# the reference does on each call:
+#   (0.2, 0.05)    cold, Converged, stored
+#   (0.72, 0.12)   0.525 from the entry (>= 0.5): cold, Converged, stored
+#   (0.2, 0.05)    warm from its own state: Converged at the turbulence start, replaces it
+#   (0.21, 0.052)  warm from (0.2, 0.05): the iteration-0 residual norms are round-off
+#                  of a converged state, so the normalised residual blows past the
+#                  divergence limit: Diverged, not stored
+#   (0.95, 0.09)   a1 above its bound: InvalidParameters, no lookup
+#   (0.72, 0.12)   warm from itself again
+WARM_SEQUENCE = [(0.2, 0.05), (0.72, 0.12), (0.2, 0.05), (0.21, 0.052), (0.95, 0.09),
+                 (0.72, 0.12)]
+# A budget of one entry (6880 payload bytes on the 3 x 24 mesh): the second store evicts
+# the first, so the third call starts cold.
+WARM_BUDGET_SEQUENCE = [(0.2, 0.05), (0.72, 0.12), (0.2, 0.05)]
+WARM_BUDGET_BYTES = 6900
 
 
 def bump_case(nx=24, ny=16, **kw) -> ck.Case:

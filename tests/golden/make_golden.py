@@ -31,8 +31,22 @@ def solve_npz(name, case, hist=0):
     print(name, o.status, o.iterations, flush=True)
 
 
+def sequence_npz(name, case, thetas, byte_budget=64 * 1024 * 1024):
+    """One reference ForwardModel evaluating thetas in order with its warm-start cache."""
+    o = ck.solve_sequence(case, thetas, "ref", byte_budget=byte_budget)
+    np.savez_compressed(OUT / f"{name}.npz", thetas=np.asarray(thetas, float),
+                        status=np.array(o.status), iterations=o.iterations, loglik=o.loglik,
+                        predictions=o.predictions, used_warm=o.used_warm, retained=o.retained,
+                        byte_budget=byte_budget)
+    print(name, o.status, o.iterations, o.used_warm, flush=True)
+
+
 def main():
-    which = set(sys.argv[1:]) or {"small", "config1", "goldens"}
+    which = set(sys.argv[1:]) or {"small", "config1", "goldens", "warm"}
+    if "warm" in which:
+        sequence_npz("warm_sequence_ref", cases.small_channel(), cases.WARM_SEQUENCE)
+        sequence_npz("warm_budget_ref", cases.small_channel(), cases.WARM_BUDGET_SEQUENCE,
+                     byte_budget=cases.WARM_BUDGET_BYTES)
     if "small" in which:
         solve_npz("small_channel_ref", cases.small_channel())
         solve_npz("small_channel_pcg_ref", cases.small_channel(pressure_solver=ck.P_PCG))

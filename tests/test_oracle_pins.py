@@ -10,7 +10,8 @@ import pytest
 import cases
 from oracle import checker as ck
 
-GOLD = json.loads((Path(__file__).parent / "golden" / "reference_goldens.json").read_text())
+GOLDEN = Path(__file__).parent / "golden"
+GOLD = json.loads((GOLDEN / "reference_goldens.json").read_text())
 need_ref = pytest.mark.skipif(not ck.have("ref"), reason="oracle/_ref not built here")
 
 
@@ -120,3 +121,41 @@ def test_device_amg_matches_reference_amg_solution(checker):
     xp, rp = checker.linear_solve(1, d, up, up, b, own, nbr, np.zeros(n), 2000, 1e-12, "ref")
     xq, rq_ = checker.linear_solve(1, d, up, up, b, own, nbr, np.zeros(n), 2000, 1e-12, "oracle")
     np.testing.assert_array_equal(xp, xq)
+
+
+def _same_sequence(a, b, rtol=1e-12):
+    """Verdicts, iteration counts, warm/cold and retained bytes exactly; predictions and
+    log-likelihoods to 1e-12 (the fields are bitwise equal; the probe interpolation of the
+    restatement rounds differently, ~1e-14)."""
+    assert a.status == b.status
+    assert np.array_equal(a.iterations, b.iterations)
+    assert np.array_equal(a.used_warm, b.used_warm)
+    assert np.array_equal(a.retained, b.retained)
+    ok = np.array([s in ("Converged", "Unconverged") for s in a.status])
+    np.testing.assert_allclose(a.loglik, b.loglik, rtol=rtol, atol=0)
+    np.testing.assert_allclose(a.predictions[ok], b.predictions[ok], rtol=rtol, atol=0)
+
+
+def test_warm_sequence_oracle_matches_reference_fixture(checker):
+    """The warm-start cache of the sequential model: which calls start warm, the
+    verdicts (a warm start next to a converged state is Diverged after 5 iterations
+    in the reference too), eviction by the byte budget, and bitwise results."""
+    for name, seq, budget in (("warm_sequence_ref", cases.WARM_SEQUENCE, 64 << 20),
+                              ("warm_budget_ref", cases.WARM_BUDGET_SEQUENCE,
+                               cases.WARM_BUDGET_BYTES)):
+        g = np.load(GOLDEN / f"{name}.npz")
+        assert np.array_equal(g["thetas"], np.asarray(seq, float))
+        want = ck.SequenceOut(list(g["status"]), g["iterations"], g["loglik"], g["predictions"],
+                              g["used_warm"], g["retained"])
+        got = ck.solve_sequence(cases.small_channel(), seq, "oracle", byte_budget=budget)
+        _same_sequence(got, want)
+
+
+@need_ref
+def test_warm_sequence_unconverged_not_stored():
+    case = cases.small_channel(max_iter=200)
+    th = [(0.31, 0.09), (0.31, 0.09)]
+    a = ck.solve_sequence(case, th, "oracle")
+    b = ck.solve_sequence(case, th, "ref")
+    _same_sequence(a, b)
+    assert not a.used_warm.any() and a.retained.tolist() == [0, 0]
