@@ -7,13 +7,13 @@ from . import _native
 from .core import (EvaluationResult, EvaluationStatus, FlowBoundaryConditions, ForwardBatch,
                    ForwardBatchResult, ForwardBatchRow, ForwardEvaluationResult, ForwardModel,
                    ForwardServer, InferenceParameterSet, Mesh, ObservationOperator,
-                   SST_DEFAULTS, SST_NAMES, ServedResult, SolverSettings, Vec3, evaluate_multi,
-                   evaluate_multi_device, rows_from_device_bytes)
+                   SST_DEFAULTS, SST_NAMES, ServedResult, SolverSettings, Vec3, WarmStartCache,
+                   evaluate_multi, evaluate_multi_device, rows_from_device_bytes)
 
 __all__ = ["EvaluationResult", "EvaluationStatus", "FlowBoundaryConditions", "ForwardBatch",
            "ForwardBatchResult", "ForwardBatchRow", "ForwardEvaluationResult", "ForwardModel",
            "ForwardServer", "InferenceParameterSet", "ServedResult", "Mesh", "ObservationOperator", "SST_DEFAULTS", "SST_NAMES",
-           "SolverSettings", "Vec3", "evaluate_multi", "evaluate_multi_device",
+           "SolverSettings", "Vec3", "WarmStartCache", "evaluate_multi", "evaluate_multi_device",
            "rows_from_device_bytes", "lib"]
 
 

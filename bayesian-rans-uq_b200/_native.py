@@ -112,6 +112,15 @@ SIGNATURES = {
     "rq_server_info": ([C.c_void_p, IP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), IP],
                        C.c_int),
     "rq_server_destroy": ([C.c_void_p], C.c_int),
+    "rq_warm_cache_create": ([C.c_void_p, C.c_int32, C.c_double, C.c_uint64,
+                              C.POINTER(C.c_void_p)], C.c_int),
+    "rq_warm_cache_destroy": ([C.c_void_p], C.c_int),
+    "rq_warm_cache_info": ([C.c_void_p, IP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)],
+                           C.c_int),
+    "rq_warm_cache_clear": ([C.c_void_p], C.c_int),
+    "rq_warm_cache_set_byte_budget": ([C.c_void_p, C.c_uint64], C.c_int),
+    "rq_evaluate_cached": ([C.c_void_p, DP, C.POINTER(RowOut), DP, DP, DP, DP, IP, IP],
+                           C.c_int),
 }
 
 _lib = None

@@ -418,6 +418,7 @@ class _Problem:
                C.byref(h))
         self.handle = h
         self.n_cells = mesh.n_cells()
+        self.nx = mesh.nx
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -636,31 +637,117 @@ class ForwardEvaluationResult:
     error: str
     fields: np.ndarray | None = None
     history: np.ndarray | None = None
+    used_warm_start: bool = False
+    snapshot: dict | None = None
+
+
+_SNAPSHOT_SCALARS = ("p", "k", "omega", "nuT", "F1", "F2", "Pk", "CDkw")
+
+
+def _snapshot(cells, bnd, flux, established) -> dict:
+    """The reference binding's snapshot dict (ownedSnapshot, rans-uq/python/bindings.cpp:427-447):
+    cell interiors, boundary-face values, face fluxes and the turbulence marker. Blocks of
+    cells / bnd are Ux Uy Uz p k omega nuT F1 F2 Pk CDkw."""
+    data = {"U": np.ascontiguousarray(cells[0:3].T)}
+    boundary = {"U": np.ascontiguousarray(bnd[0:3].T)}
+    for i, name in enumerate(_SNAPSHOT_SCALARS):
+        data[name] = cells[3 + i].copy()
+        boundary[name] = bnd[3 + i].copy()
+    data["boundary"] = boundary
+    data["face_fluxes"] = flux
+    data["turb_established"] = established
+    return data
+
+
+class WarmStartCache:
+    """WarmStartCache (rans-uq/include/ForwardModel.hpp:21-157) of one ForwardModel:
+    converged states kept in device memory, looked up by Euclidean distance in theta
+    (strictly below the threshold) and evicted oldest-first by count and by the
+    reference's payload byte count. Same methods as the reference binding
+    (rans-uq/python/bindings.cpp:823-828)."""
+
+    def __init__(self, problem, max_size: int = 50, threshold: float = 0.5,
+                 byte_budget: int = 64 * 1024 * 1024):
+        self._problem = problem  # keeps the mesh class alive while the cache exists
+        self.handle = C.c_void_p()
+        N.call("rq_warm_cache_create", problem.handle, C.c_int32(max_size),
+               C.c_double(threshold), C.c_uint64(byte_budget), C.byref(self.handle))
+
+    def _info(self):
+        size, kept, budget = C.c_int32(), C.c_uint64(), C.c_uint64()
+        N.call("rq_warm_cache_info", self.handle, C.byref(size), C.byref(kept), C.byref(budget))
+        return size.value, kept.value, budget.value
+
+    def size(self) -> int:
+        return self._info()[0]
+
+    def clear(self) -> None:
+        N.call("rq_warm_cache_clear", self.handle)
+
+    def set_byte_budget(self, byte_budget: int) -> None:
+        N.call("rq_warm_cache_set_byte_budget", self.handle, C.c_uint64(byte_budget))
+
+    def byte_budget(self) -> int:
+        return self._info()[2]
+
+    def retained_bytes(self) -> int:
+        return self._info()[1]
+
+    def __del__(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            try:
+                N.lib().rq_warm_cache_destroy(self.handle)
+            except Exception:
+                pass
+            self.handle = C.c_void_p()
 
 
 class ForwardModel:
-    """ForwardModel (rans-uq/include/ForwardModel.hpp:199-281): one cold GPU solve per call.
-    The warm-start cache is not part of the B200 path (batches disable it too)."""
+    """ForwardModel (rans-uq/include/ForwardModel.hpp:199-281): one GPU solve per call,
+    started from the nearest converged state of its warm-start cache (50 entries, distance
+    0.5, 64 MiB, as ForwardModel.cpp:14 builds it) or cold when none is near; a Converged
+    solve is stored (ForwardModel.cpp:79-82, 114-117). Batches start every row cold."""
 
     def __init__(self, mesh, param_set, obs_op, bcs, nu, settings=None, u_init=Vec3(1, 0, 0),
                  p_init=0.0, k_init=1e-4, omega_init=1.0):
         self._batch = ForwardBatch(mesh, param_set, obs_op, bcs, nu, settings, u_init, p_init,
                                    k_init, omega_init)
+        self._cache = WarmStartCache(self._batch._problem)
         self._last = None
+
+    def cache(self) -> WarmStartCache:
+        return self._cache
 
     def evaluate(self, theta) -> EvaluationResult:
         return self.evaluate_with_diagnostics(theta).result
 
     def evaluate_with_diagnostics(self, theta, snapshot: bool = False,
                                   hist_cap: int = 0) -> ForwardEvaluationResult:
-        res, fields, hist = self._batch.evaluate_fields(np.asarray([theta], dtype=np.float64),
-                                                        hist_cap=hist_cap)
-        row = res.rows[0]
+        theta = np.ascontiguousarray(np.asarray(theta, dtype=np.float64).reshape(-1))
+        if theta.size != self._batch.n_parameters():
+            raise ValueError("theta must have n_parameters values")
+        if hist_cap:
+            raise NotImplementedError("residual histories come from ForwardBatch.evaluate_fields")
+        no, nc = self._batch.n_observations(), self._batch._problem.n_cells
+        nx = self._batch._problem.nx
+        nb, nf = 2 * nx, 2 * nc + nx
+        out = N.RowOut()
+        pred = np.full(max(no, 1), np.nan)
+        fields = np.zeros((11, nc))
+        bnd = np.zeros((11, nb)) if snapshot else None
+        flux = np.zeros(nf) if snapshot else None
+        est = C.c_int32(0)
+        used = C.c_int32(0)
+        N.call("rq_evaluate_cached", self._cache.handle, N.dptr(theta), C.byref(out),
+               N.dptr(pred), N.dptr(fields), N.dptr(bnd), N.dptr(flux),
+               C.byref(est) if snapshot else None, C.byref(used))
+        row = _rows_from_native([out], pred[None, :no], no, self._batch.n_parameters())[0]
         keep = row.result.status in (EvaluationStatus.Converged, EvaluationStatus.Unconverged)
-        self._last = fields[0] if keep else None
+        self._last = fields if keep else None
+        snap = _snapshot(fields, bnd, flux, bool(est.value)) if snapshot and keep else None
         return ForwardEvaluationResult(row.result, row.final_worst_measure, row.contraction_rate_u,
-                                       row.stalled, row.error, fields[0] if keep else None,
-                                       hist[0] if hist_cap else None)
+                                       row.stalled, row.error, fields if keep else None, None,
+                                       bool(used.value), snap)
 
     def penalized_log_likelihood(self, theta) -> float:
         r = self.evaluate(theta)

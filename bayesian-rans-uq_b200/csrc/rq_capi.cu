@@ -318,7 +318,7 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     // FP64 arrays, FP32 inner-solver copies (mixed form), faces, AMG, dense coarse
     C.wsDoubles = 43 * pad32(n) + 15 * pad32((n + 1) / 2) + pad32((valOff + 1) / 2) +
                   pad32((vecOff + 1) / 2) +
-                  4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + pad32(mc * mc);
+                  4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
     // upload and patch pointers
     P.dDoubles.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
     P.dInts.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));
@@ -332,9 +332,11 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     check(cudaMemcpy(P.dCls.p, &C, sizeof(rq::DevClass), cudaMemcpyHostToDevice), "upload");
 }
 
-// CTA size of a class: 512 threads measured fastest for 384-1536 cells (256 and
-// 1024 were slower at every size).
-constexpr int kDefaultBlock = 512;
+// CTA size of a class, measured per outer iteration on a B200 (FP64): 512 threads
+// for up to 1024 cells (384 cells: 153 us at 512, 182 us at 768; 768 cells: equal),
+// 768 threads above (1536 cells: 431 us at 768, 465 us at 512, 567 us at 1024 --
+// two cells per thread; 1024 threads cap registers at 64 and spill).
+int defaultBlock(int nCells) { return nCells > 1024 ? 768 : 512; }
 
 
 
@@ -509,7 +511,7 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
         std::memcpy(P->base, base, sizeof(P->base));
         P->nObs = obs ? obs->n_obs : 0;
         P->block = settings->block_threads ? rq::normalizeBlock(settings->block_threads)
-                                           : kDefaultBlock;
+                                           : defaultBlock(P->mesh.n);
         upload(*P, obs, nu, *settings, init);
         *out = P.release();
     });

@@ -87,6 +87,15 @@ struct DevJob {
                        // Krylov iterations, inner pressure iterations, 8 stage cycle counts
     int32_t histCap;
     int32_t pad;
+    // Warm start (optional): a converged state in the fields layout (11 x n: Ux Uy Uz p k
+    // omega nuT F1 F2 Pk CDkw) copied in place of the uniform initial state, and the beta1
+    // its wall-face omega was last set with (the cached solve's own coefficient).
+    const double *warm;
+    double warmBeta;
+    // Snapshot (optional, written with the fields): the n + nfy face fluxes in the
+    // device face layout (x faces, then y faces), the beta1 of the final wall-face omega,
+    // and the turbulence-established marker (0 or 1).
+    double *snap;
 };
 
 // Request queue of the serving loop. The host appends requests (jobs[i], with

@@ -185,6 +185,9 @@ int rq_server_submit(rq_server *s, int32_t problem, const double *theta, int64_t
         j.hist = nullptr;
         j.clock = s->clock + 12L * t;
         j.histCap = 0;
+        j.warm = nullptr; // served requests start cold, as batch rows do
+        j.warmBeta = 0.0;
+        j.snap = nullptr;
         s->submitted = t + 1;
         __atomic_store_n(s->published, t + 1, __ATOMIC_RELEASE);
         s->ensureRunning();

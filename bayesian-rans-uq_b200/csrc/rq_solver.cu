@@ -42,7 +42,7 @@ struct Work {
     double *r, *rh, *pv, *v, *s, *t, *ph, *sh;
     double *z, *xa, *xb, *rr;                // PCG / level-0 V-cycle
     double *rd;                              // reciprocal diagonal of the system being solved
-    double *amgVal, *amgVec, *dense0;
+    double *amgVal, *amgVec, *dense0, *dense1;
 };
 
 // Krylov / AMG storage of one value type (see "inner linear solvers").
@@ -71,7 +71,8 @@ struct Shared {
     long long innerKrylov, innerPressure; // inner iterations of the solve (work accounting)
     long long stage[8];                   // clock64 cycles per stage (thread 0)
     long long tmark;
-    int wallBetaInit; // the wall-face omega still carries applyAllBCs' beta1
+    double wallBeta;  // beta1 the wall-face omega was last set with (applyAllBCs' default
+                      // on a cold start, the cached solve's on a warm one, then b1)
     double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
 };
 
@@ -403,9 +404,12 @@ template <typename T> __device__ __forceinline__ T level0EntryT(const KW<T> &K, 
 
 // Galerkin values of every coarse level from the current pressure system, the
 // reciprocal diagonals of the smoothed levels, then the inverse of the coarsest
-// level (at most 64 rows) in place by one warp (Gauss-Jordan, SPD: no pivoting),
-// in shared memory up to 32 rows and in the workspace above. The inverse is FP64
-// in both forms.
+// level (Gauss-Jordan, SPD: no pivoting): in place by one warp, one row per lane,
+// when it has at most 32 rows; above that (up to 64) by the whole CTA, one
+// barrier per pivot, ping-ponging [A | I] between two workspace buffers. (One warp
+// with two rows per lane was measured 17 % slower per outer iteration at 1536
+// cells: 128 dependent updates per lane and pivot against 16 per thread.) The
+// inverse is FP64 in both forms.
 template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
@@ -436,65 +440,102 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
     const DevAmgLevel &Q = C.lev[L - 1];
     const int m = Q.n; // at most kMaxCoarse = 64 rows (the set-up rejects more)
     const T *qv = K.amgVal + Q.valOff;
-    // row-major m x m: shared memory up to 32 rows, the workspace's dense0 above
-    double *a = (m <= 32) ? S.coarse : W.dense0;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x)
-        a[e] = 0.0;
+    if (m <= 32) {
+        double *a = S.coarse;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x)
+            a[e] = 0.0;
+        __syncthreads();
+        if (L == 1) {
+            for (int r = threadIdx.x; r < m; r += blockDim.x) {
+                const Cell q = cellOf(C, r);
+                a[r * m + r] += double(K.d[r]);
+                a[r * m + q.W] += double(K.aW[r]);
+                a[r * m + q.E] += double(K.aE[r]);
+                if (q.south)
+                    a[r * m + r - C.nx] += double(K.aS[r]);
+                if (q.north)
+                    a[r * m + r + C.nx] += double(K.aN[r]);
+            }
+        } else {
+            for (int r = threadIdx.x; r < m; r += blockDim.x)
+                for (int k = 0; k < Q.width; ++k) {
+                    const int c = __ldg(Q.ecol + k * m + r);
+                    if (c >= 0)
+                        a[r * m + c] = double(qv[k * m + r]);
+                }
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const int r = threadIdx.x;
+            for (int k = 0; k < m; ++k) {
+                const double p = 1.0 / a[k * m + k];
+                const double f = (r < m) ? a[r * m + k] : 0.0;
+                __syncwarp();
+                if (r < m && r != k) {
+                    for (int j = 0; j < m; ++j)
+                        if (j != k)
+                            a[r * m + j] -= f * a[k * m + j] * p;
+                    a[r * m + k] = -f * p;
+                }
+                __syncwarp();
+                if (r == k) {
+                    for (int j = 0; j < m; ++j)
+                        if (j != k)
+                            a[k * m + j] *= p;
+                    a[k * m + k] = p;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        return;
+    }
+    // m x 2m [A | I], row-major; the inverse ends in the right half of dense0
+    const int m2 = 2 * m;
+    double *A0 = W.dense0, *A1 = W.dense1;
+    for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
+        A0[e] = ((e % m2) == m + e / m2) ? 1.0 : 0.0;
     __syncthreads();
     if (L == 1) {
         for (int r = threadIdx.x; r < m; r += blockDim.x) {
             const Cell q = cellOf(C, r);
-            a[r * m + r] += double(K.d[r]);
-            a[r * m + q.W] += double(K.aW[r]);
-            a[r * m + q.E] += double(K.aE[r]);
+            A0[r * m2 + r] += double(K.d[r]);
+            A0[r * m2 + q.W] += double(K.aW[r]);
+            A0[r * m2 + q.E] += double(K.aE[r]);
             if (q.south)
-                a[r * m + r - C.nx] += double(K.aS[r]);
+                A0[r * m2 + r - C.nx] += double(K.aS[r]);
             if (q.north)
-                a[r * m + r + C.nx] += double(K.aN[r]);
+                A0[r * m2 + r + C.nx] += double(K.aN[r]);
         }
     } else {
         for (int r = threadIdx.x; r < m; r += blockDim.x)
             for (int k = 0; k < Q.width; ++k) {
                 const int c = __ldg(Q.ecol + k * m + r);
                 if (c >= 0)
-                    a[r * m + c] = double(qv[k * m + r]);
+                    A0[r * m2 + c] = double(qv[k * m + r]);
             }
     }
     __syncthreads();
-    // in-place Gauss-Jordan inverse by one warp (SPD: no pivoting), rows lane and
-    // lane + 32; warp barriers only (a CTA barrier per pivot cost more)
-    if (threadIdx.x < 32) {
-        const int r0 = threadIdx.x, r1 = threadIdx.x + 32;
-        for (int k = 0; k < m; ++k) {
-            const double p = 1.0 / a[k * m + k];
-            const double f0 = (r0 < m) ? a[r0 * m + k] : 0.0;
-            const double f1 = (r1 < m) ? a[r1 * m + k] : 0.0;
-            __syncwarp();
-            if (r0 < m && r0 != k) {
-                for (int j = 0; j < m; ++j)
-                    if (j != k)
-                        a[r0 * m + j] -= f0 * a[k * m + j] * p;
-                a[r0 * m + k] = -f0 * p;
-            }
-            if (r1 < m && r1 != k) {
-                for (int j = 0; j < m; ++j)
-                    if (j != k)
-                        a[r1 * m + j] -= f1 * a[k * m + j] * p;
-                a[r1 * m + k] = -f1 * p;
-            }
-            __syncwarp();
-            if (r0 == k || r1 == k) {
-                for (int j = 0; j < m; ++j)
-                    if (j != k)
-                        a[k * m + j] *= p;
-                a[k * m + k] = p;
-            }
-            __syncwarp();
+    for (int piv = 0; piv < m; ++piv) {
+        const double inv = 1.0 / A0[piv * m2 + piv];
+        for (int e = threadIdx.x; e < m * m2; e += blockDim.x) {
+            const int r = e / m2, col = e - r * m2;
+            const double pr = A0[piv * m2 + col] * inv;
+            A1[e] = (r == piv) ? pr : A0[e] - A0[r * m2 + piv] * pr;
         }
+        __syncthreads();
+        double *tmp = A0;
+        A0 = A1;
+        A1 = tmp;
     }
-    __syncthreads();
+    if (A0 != W.dense0) { // keep the inverse in dense0
+        for (int e = threadIdx.x; e < m * m2; e += blockDim.x)
+            W.dense0[e] = A0[e];
+        __syncthreads();
+    }
 }
 
+// row i of an ELL level times x, entries in column order
 template <typename T>
 __device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
     T s = T(0);
@@ -578,7 +619,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     // the coarsest level: restriction of the level above, then the dense inverse
     auto coarsest = [&]() {
         const int l = L - 1;
-        const int m = C.lev[l].n;
+        const int m = C.lev[l].n, m2 = 2 * m;
         T *b = vb(l), *xb = b + 2 * m;
         if (L == 1) {
             for (int i = t0; i < m; i += ts)
@@ -599,7 +640,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         // copy of its inverse loses the coarse correction
         for (int i = t0; i < m; i += ts) {
             double s = 0.0;
-            const double *row = ((m <= 32) ? S.coarse : W.dense0) + i * m;
+            const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
             for (int j = 0; j < m; ++j)
                 s += row[j] * double(b[j]);
             xb[i] = T(s);
@@ -1070,7 +1111,8 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.Uyp = take(n);
     W.kOld = take(n);
     W.wOld = take(n);
-    W.dense0 = take(static_cast<long>(m) * m); // coarsest inverse when above 32 rows
+    W.dense0 = take(2L * m * m); // [A | I] ping-pong of a coarsest level above 32 rows
+    W.dense1 = take(2L * m * m);
     if (mixed) {
         W.ph = W.s = W.sh = W.t = W.rh = nullptr;
         W.xa = W.xb = W.rr = W.amgVec = W.amgVal = nullptr;
@@ -1110,7 +1152,7 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     const double sk2 = S.coeff[4], sw2 = S.coeff[5], b2 = S.coeff[6], al2 = S.coeff[7];         \
     const double bs = S.coeff[8], a1 = S.coeff[9];                                              \
     auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };    \
-    auto bwOf = [&](int f) { return wallFaceOmega(C, S.wallBetaInit ? C.beta1Init : b1, f); }; \
+    auto bwOf = [&](int f) { return wallFaceOmega(C, S.wallBeta, f); };                        \
     (void)st; (void)n; (void)nx; (void)ny; (void)nfy; (void)nu; (void)sk1; (void)sw1;          \
     (void)b1; (void)al1; (void)sk2; (void)sw2; (void)b2; (void)al2; (void)bs; (void)a1;         \
     (void)blend; (void)bwOf;
@@ -1134,6 +1176,25 @@ __device__ __noinline__ void phInitCells(Shared &S) {
         W.Pk[c] = 0.0;
         W.CD[c] = 0.0;
         W.nuT[c] = a1 * K0 / dmax(a1 * om, 1e-20);
+        W.S[c] = 0.0;
+    }
+}
+
+// A cached converged state (fields layout, 11 x n) in place of the uniform one; the
+// strain starts from zero as in solve() (SIMPLESolver.cpp:1205).
+__device__ __noinline__ void phInitWarm(Shared &S, const double *wf) {
+    RQ_PRELUDE
+    FOR_CELLS(c) {
+        W.Ux[c] = wf[c];
+        W.Uy[c] = wf[n + c];
+        W.p[c] = wf[3 * n + c];
+        W.k[c] = wf[4 * n + c];
+        W.w[c] = wf[5 * n + c];
+        W.nuT[c] = wf[6 * n + c];
+        W.F1[c] = wf[7 * n + c];
+        W.F2[c] = wf[8 * n + c];
+        W.Pk[c] = wf[9 * n + c];
+        W.CD[c] = wf[10 * n + c];
         W.S[c] = 0.0;
     }
 }
@@ -1789,7 +1850,7 @@ __device__ __noinline__ void phTurbClamp(Shared &S, int eq) {
                         W.w[c] = v;
                     }
                     if (threadIdx.x == 0)
-                        S.wallBetaInit = 0;
+                        S.wallBeta = b1;
                 }
 }
 
@@ -1845,12 +1906,16 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
     auto blend = [](double p1, double p2, double F1) { return F1 * p1 + (1.0 - F1) * p2; };
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
 
-    // ---- initUniform (SIMPLESolver.cpp:267-298) and applyAllBCs
-    phInitCells(S);
+    // ---- initUniform (SIMPLESolver.cpp:267-298) and applyAllBCs, or the cached state of
+    // a warm start (ForwardModel.cpp:79-82), whose turbulence is established
+    if (job.warm)
+        phInitWarm(S, job.warm);
+    else
+        phInitCells(S);
     if (threadIdx.x < 4)
         S.cnt[threadIdx.x] = 0;
     if (threadIdx.x == 0)
-        S.wallBetaInit = 1;
+        S.wallBeta = job.warm ? job.warmBeta : C.beta1Init;
     if (threadIdx.x == 0) {
         S.haveQPrev = 0;
         S.innerKrylov = 0;
@@ -1864,7 +1929,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
     phInitFlux(S);
     __syncthreads();
 
-    bool established = false;
+    bool established = job.warm != nullptr;
     int amgNeed = 1, amgAfter = -1; // AMG coarse-value refresh state
     double lastK = 1.0, lastW = 1.0;
     const double tol = st.tol, negligible = 0.01 * tol;
@@ -2158,6 +2223,14 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         for (int b = 0; b < 11; ++b)
             FOR_CELLS(c) job.fields[(long)b * n + c] = src[b] ? src[b][c] : 0.0;
     }
+    if (job.snap && status != 2) {
+        for (int f = threadIdx.x; f < n + nfy; f += blockDim.x)
+            job.snap[f] = W.phi[f];
+        if (threadIdx.x == 0) {
+            job.snap[n + nfy] = S.wallBeta;
+            job.snap[n + nfy + 1] = established ? 1.0 : 0.0;
+        }
+    }
     __syncthreads();
 }
 
@@ -2336,6 +2409,7 @@ void *pick(int block) {
     case 128: return kernelFor<128>();
     case 256: return kernelFor<256>();
     case 512: return kernelFor<512>();
+    case 768: return kernelFor<768>();
     case 1024: return kernelFor<1024>();
     default: return nullptr;
     }
@@ -2344,6 +2418,7 @@ void *pickServe(int block) {
     switch (block) {
     case 256: return serveFor<256>();
     case 512: return serveFor<512>();
+    case 768: return serveFor<768>();
     case 1024: return serveFor<1024>();
     default: return nullptr;
     }
@@ -2353,7 +2428,8 @@ void *pickServe(int block) {
 bool launchVariantExists(int block) { return pick(block) != nullptr; }
 
 int normalizeBlock(int block) {
-    return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : block <= 512 ? 512 : 1024;
+    return block <= 64 ? 64 : block <= 128 ? 128 : block <= 256 ? 256 : block <= 512 ? 512
+         : block <= 768 ? 768 : 1024;
 }
 
 cudaError_t launchSolve(const DevJob *jobs, int njobs, int *nextJob, double *ws, long wsStride,
@@ -2429,6 +2505,7 @@ void *pickOne(int block) {
     case 128: return oneFor<128>();
     case 256: return oneFor<256>();
     case 512: return oneFor<512>();
+    case 768: return oneFor<768>();
     case 1024: return oneFor<1024>();
     default: return nullptr;
     }

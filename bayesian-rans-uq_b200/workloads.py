@@ -159,7 +159,8 @@ def bump_geometry(nx: int = 200, h: float = 1.0, length: float = 9.0, width: flo
 
 
 def bump_batch(nx: int = 200, ny: int = 100, max_iter: int = 200, tol: float = 1e-8,
-               body_force: float = 4e-3, re: float = 5600.0) -> core.ForwardBatch:
+               body_force: float = 4e-3, re: float = 5600.0,
+               block_threads: int = 0) -> core.ForwardBatch:
     """The bump-wall channel (top 3.04 h, Re 5600 on h, y+ 1) as a ForwardBatch with
     6 velocity probes at x = 2; the body force drives a bulk velocity of order one."""
     xn, yb = bump_geometry(nx)
@@ -170,7 +171,7 @@ def bump_batch(nx: int = 200, ny: int = 100, max_iter: int = 200, tol: float = 1
         obs.add_velocity_profile(core.Vec3(2.0, float(yi), 0.0), 0, 0.0, 1e-2)
     st = core.SolverSettings(max_iterations=max_iter, convergence_tol=tol, alpha_u=0.4,
                              alpha_p=0.25, body_force=core.Vec3(body_force, 0.0, 0.0),
-                             verbose=False)
+                             verbose=False, block_threads=block_threads)
     bcs = core.FlowBoundaryConditions.channel_defaults(mesh, 1.0, 1e-4, 10.0)
     return core.ForwardBatch(mesh, core.InferenceParameterSet.a1_betaStar(), obs, bcs,
                              1.0 / re, st, core.Vec3(0.3, 0.0, 0.0), 0.0, 1e-4, 10.0)

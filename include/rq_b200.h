@@ -19,6 +19,9 @@
  *       several ForwardBatch::evaluate calls (one per mesh class) fused into one launch
  *   rq_solve
  *       SIMPLESolver::initUniform + solve(FlowFields&, Workspace&) rans-uq/src/SIMPLESolver.cpp:267-298, 1193-1716
+ *   rq_evaluate_cached, rq_warm_cache_*
+ *       ForwardModel::evaluateWithDiagnostics with its WarmStartCache rans-uq/src/ForwardModel.cpp:35-137,
+ *       rans-uq/include/ForwardModel.hpp:21-157 (size, clear, setByteBudget, byteBudget, retainedBytes)
  *   rq_linear_solve
  *       makeSolver(name)->solve(LinearSystem, x, maxIter, tol)  core/include/LinearSolver.hpp:137-153, 988-998
  *   rq_mesh_geometry
@@ -266,6 +269,41 @@ int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *co
                    int32_t *launches);
 /* Cancels requests not yet claimed, waits for the solves in flight, frees. */
 int rq_server_destroy(rq_server *s);
+
+/* ---- warm starts: the sequential model's cache of converged states
+   (WarmStartCache, rans-uq/include/ForwardModel.hpp:21-157; the model's own is
+   (50, 0.5, 64 MiB), ForwardModel.cpp:14). Entries stay in device memory; the byte
+   count is the reference's payload count (entryBytes, :39-47: theta, the vector
+   field and eight scalar fields, each over cells plus boundary faces), so eviction
+   happens after the same calls. */
+typedef struct rq_warm_cache rq_warm_cache;
+/* max_size < 0 or a negative / non-finite threshold: RQ_E_INVALID (the reference throws). */
+int rq_warm_cache_create(rq_problem *p, int32_t max_size, double threshold, uint64_t byte_budget,
+                         rq_warm_cache **out);
+int rq_warm_cache_destroy(rq_warm_cache *c);
+/* size, retainedBytes, byteBudget */
+int rq_warm_cache_info(rq_warm_cache *c, int32_t *size, uint64_t *retained_bytes,
+                       uint64_t *byte_budget);
+int rq_warm_cache_clear(rq_warm_cache *c);
+/* setByteBudget: evicts oldest entries until the retained bytes fit. */
+int rq_warm_cache_set_byte_budget(rq_warm_cache *c, uint64_t byte_budget);
+/* ForwardModel::evaluateWithDiagnostics with the cache (rans-uq/src/ForwardModel.cpp:35-137):
+   an admitted theta (n_active values, host) starts from the nearest cached state closer
+   than the threshold (strictly; ties keep the older entry), else cold; a Converged solve
+   is stored (replacing an entry with the same theta). row, predictions (n_obs) and the
+   optional fields (11 x n_cells) are host buffers; used_warm_start (optional) reports
+   ForwardEvaluationResult::usedWarmStart.
+   Snapshot (evaluateWithDiagnostics(theta, snapshot = true); OwnedFlowSnapshot,
+   ForwardModel.hpp:162-186), optional, written only for a Converged or Unconverged row
+   (the rows the reference snapshots). On these nx x ny periodic meshes there are
+   2 nx ny - nx internal faces and 2 nx wall faces (Mesh.cpp:620-625):
+   boundary = 11 x 2nx values over the wall faces in the mesh's face order (bottom row,
+   then top row), blocks as fields; face_fluxes = 2 nx ny + nx owner-outward fluxes in the
+   mesh's face order; turb_established = FlowFields::turbEstablished. */
+int rq_evaluate_cached(rq_warm_cache *c, const double *theta, rq_row_out *row,
+                       double *predictions, double *fields, double *boundary,
+                       double *face_fluxes, int32_t *turb_established,
+                       int32_t *used_warm_start);
 
 #ifdef __cplusplus
 }

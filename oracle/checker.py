@@ -274,6 +274,33 @@ def solve_sequence(case: Case, thetas, kind: str = "ref", max_size: int = 50,
                        np.array([r.loglik for r in res]), pred[:, :nobs], used.astype(bool), kept)
 
 
+def solve_snapshot(case: Case) -> dict | None:
+    """The reference's evaluateWithDiagnostics(theta, snapshot=True) on a cold model:
+    {'status', 'iterations', 'cells' (11, nC), 'boundary' (11, nB), 'face_fluxes' (nF),
+    'turb_established'}, blocks Ux Uy Uz p k omega nuT F1 F2 Pk CDkw; None without a
+    snapshot. Reference only (the restatement keeps no snapshot)."""
+    L = lib("ref")
+    s, keep = case.struct()
+    cells_, faces_, ni = mesh(case, "ref")
+    nc, nf = len(cells_), len(faces_)
+    nb = nf - ni
+    res = OrcResult()
+    cells = np.zeros((NFIELD, nc))
+    bnd = np.zeros((NFIELD, max(nb, 1)))
+    flux = np.zeros(nf)
+    est, has = C.c_int32(), C.c_int32()
+    rc = L.ref_solve_snapshot(C.byref(s), C.byref(res), _dptr(cells), _dptr(bnd), _dptr(flux),
+                              C.byref(est), C.byref(has))
+    if rc != 0:
+        L.ref_last_error.restype = C.c_char_p
+        raise RuntimeError(L.ref_last_error().decode())
+    if not has.value:
+        return None
+    return dict(status=STATUS[res.status], iterations=res.iterations, loglik=res.loglik,
+                cells=cells, boundary=bnd[:, :nb], face_fluxes=flux,
+                turb_established=bool(est.value))
+
+
 def mesh(case: Case, kind: str = "ref"):
     """Cell (cx, cy, vol, wd) and face (owner, nbr, cx, cy, nx, ny, area, delta, dx, dy,
     weight, shift_x, patch) arrays of the mesh as the checker builds it."""
@@ -315,5 +342,5 @@ def rel_err(a, b) -> float:
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-__all__ = ["Case", "config1_case", "channel_probes", "solve", "solve_sequence", "mesh", "linear_solve", "have",
+__all__ = ["Case", "config1_case", "channel_probes", "solve", "solve_sequence", "solve_snapshot", "mesh", "linear_solve", "have",
            "rel_err", "DEFAULT_COEFFS", "P_AMG", "P_PCG", "P_BICGSTAB", "FIELD_NAMES", "math"]

@@ -242,6 +242,67 @@ int ref_solve_sequence(const orc_case *c, const double *thetas, int32_t m_calls,
     }
 }
 
+// One cold evaluateWithDiagnostics(theta, snapshot = true) (ForwardModel.cpp:118-119,
+// OwnedFlowSnapshot ForwardModel.hpp:162-186): cells (11 x nC blocks Ux Uy Uz p k omega
+// nuT F1 F2 Pk CDkw), boundary faces (the same 11 blocks over nB faces), the face fluxes
+// (nF, owner-outward, the mesh's face order) and the turbulence marker. has_snapshot = 0
+// when the reference returns none (a diverged or invalid evaluation).
+int ref_solve_snapshot(const orc_case *c, orc_result *res, double *cells, double *boundary,
+                       double *fluxes, int32_t *turb_established, int32_t *has_snapshot) {
+    try {
+        std::streambuf *old = std::cout.rdbuf(nullptr);
+        Mesh mesh = buildMesh(*c);
+        std::cout.rdbuf(old);
+        mesh.computeWallDistance();
+        auto bcs = FlowBoundaryConditions::channelDefaults(mesh, c->bc_u, c->bc_k, c->bc_w);
+        ObservationOperator obs;
+        for (int i = 0; i < c->n_obs; ++i)
+            obs.addVelocityProfile(Vec3(c->obs_x[i], c->obs_y[i], 0.0), c->obs_component,
+                                   c->obs_value[i], c->obs_sigma[i]);
+        auto params = InferenceParameterSet::a1_betaStar();
+        params.base = InferenceParameterSet::fromVector(std::vector<double>(c->coeffs, c->coeffs + 11));
+        ForwardModel model(mesh, params, obs, bcs, c->nu, buildSettings(*c),
+                           Vec3(c->init_u[0], c->init_u[1], c->init_u[2]), c->init_p, c->init_k,
+                           c->init_w);
+        std::vector<double> theta = {c->coeffs[9], c->coeffs[8]};
+        auto ev = model.evaluateWithDiagnostics(theta, true);
+        std::memset(res, 0, sizeof(*res));
+        res->status = static_cast<int32_t>(ev.result.status);
+        res->iterations = ev.result.simpleIters;
+        res->loglik = ev.result.loglik;
+        *has_snapshot = ev.snapshot.has_value();
+        if (!ev.snapshot)
+            return 0;
+        const OwnedFlowSnapshot &s = *ev.snapshot;
+        const size_t n = s.p.size(), nb = s.pBoundary.size();
+        auto put = [](double *dst, size_t m, const std::vector<Vec3> &v,
+                      const std::initializer_list<const std::vector<double> *> &scalars) {
+            for (size_t i = 0; i < m; ++i) {
+                dst[i] = v[i].x;
+                dst[m + i] = v[i].y;
+                dst[2 * m + i] = v[i].z;
+            }
+            size_t b = 3;
+            for (const std::vector<double> *f : scalars) {
+                for (size_t i = 0; i < m; ++i)
+                    dst[b * m + i] = (*f)[i];
+                ++b;
+            }
+        };
+        put(cells, n, s.U, {&s.p, &s.k, &s.omega, &s.nuT, &s.F1, &s.F2, &s.Pk, &s.CDkw});
+        put(boundary, nb, s.UBoundary,
+            {&s.pBoundary, &s.kBoundary, &s.omegaBoundary, &s.nuTBoundary, &s.F1Boundary,
+             &s.F2Boundary, &s.PkBoundary, &s.CDkwBoundary});
+        for (size_t f = 0; f < s.faceFluxes.size(); ++f)
+            fluxes[f] = s.faceFluxes[f];
+        *turb_established = s.turbEstablished;
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return -1;
+    }
+}
+
 // The reference linear solvers on one LDU system: kind 0 AMG, 1 PCG, 2 BiCGSTAB,
 // 3 GaussSeidel. x is the initial guess on input and the solution on output.
 int ref_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,

@@ -42,7 +42,16 @@ def sequence_npz(name, case, thetas, byte_budget=64 * 1024 * 1024):
 
 
 def main():
-    which = set(sys.argv[1:]) or {"small", "config1", "goldens", "warm"}
+    which = set(sys.argv[1:]) or {"small", "config1", "goldens", "warm", "snapshot"}
+    if "snapshot" in which:
+        for name, case in (("snapshot_small_channel_ref", cases.small_channel()),
+                           ("snapshot_small_channel_capped_ref", cases.small_channel(max_iter=300))):
+            o = ck.solve_snapshot(case)
+            np.savez_compressed(OUT / f"{name}.npz", status=o["status"],
+                                iterations=o["iterations"], cells=o["cells"],
+                                boundary=o["boundary"], face_fluxes=o["face_fluxes"],
+                                turb_established=o["turb_established"])
+            print(name, o["status"], o["iterations"], o["turb_established"], flush=True)
     if "warm" in which:
         sequence_npz("warm_sequence_ref", cases.small_channel(), cases.WARM_SEQUENCE)
         sequence_npz("warm_budget_ref", cases.small_channel(), cases.WARM_BUDGET_SEQUENCE,
