@@ -84,6 +84,7 @@ SIGNATURES = {
                                   C.c_void_p], C.c_int),
     "rq_solve": ([C.c_void_p, DP, C.POINTER(RowOut), DP, DP, DP, C.c_int32], C.c_int),
     "rq_mesh_geometry": ([C.POINTER(MeshDesc), IP, DP], C.c_int),
+    "rq_mesh_save_binary": ([C.POINTER(MeshDesc), C.c_char_p], C.c_int),
     "rq_linear_solve": ([C.POINTER(Ldu), DP, C.c_int32, C.c_double, C.c_int32,
                          C.POINTER(SolverResult)], C.c_int),
     "rq_linear_solve_batch": ([C.POINTER(Ldu), C.c_int32, C.POINTER(DP), C.c_int32, C.c_double,

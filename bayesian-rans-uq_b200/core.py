@@ -12,6 +12,7 @@ through the C ABI (include/rq_b200.h); nothing here computes a flow field.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import enum
 import math
 from dataclasses import dataclass, field
@@ -104,6 +105,12 @@ class Mesh:
 
     def cell_centers(self) -> np.ndarray:
         return self.cell_geometry()[:, :2]
+
+    def save_binary(self, path) -> None:
+        """Mesh::saveBinary (core/src/Mesh.cpp:751-811): the reference's MSH2 binary mesh
+        file, byte-identical to the reference's for the same generator call."""
+        d = self.desc()
+        N.call("rq_mesh_save_binary", C.byref(d), os.fsencode(path))
 
 
 @dataclass

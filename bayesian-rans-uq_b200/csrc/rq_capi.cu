@@ -4,6 +4,8 @@
 // numerics run in rq_solver.cu.
 #include "rq_capi_common.h"
 
+#include <cstdio>
+
 using namespace rqc;
 
 namespace rqc {
@@ -742,6 +744,21 @@ int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells) 
                 cells[4 * c + 2] = m.vol[c];
                 cells[4 * c + 3] = m.wd[c];
             }
+    });
+}
+
+int rq_mesh_save_binary(const rq_mesh_desc *mesh, const char *path) {
+    return guarded([&] {
+        if (!mesh || !path)
+            throw std::invalid_argument("null argument");
+        const std::vector<char> bytes = rq::meshBinary(buildMesh(*mesh));
+        std::FILE *f = std::fopen(path, "wb");
+        if (!f)
+            throw std::runtime_error(std::string("Cannot open binary mesh for writing: ") + path);
+        const size_t put = std::fwrite(bytes.data(), 1, bytes.size(), f);
+        const bool closed = std::fclose(f) == 0;
+        if (put != bytes.size() || !closed)
+            throw std::runtime_error(std::string("Cannot write binary mesh: ") + path);
     });
 }
 

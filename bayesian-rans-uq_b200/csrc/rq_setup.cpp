@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <limits>
 #include <map>
 #include <stdexcept>
@@ -64,6 +65,11 @@ StructMesh buildPeriodic(const std::vector<double> &xN, const std::vector<double
         eta[j] = 0.5 * (1.0 + std::tanh(stretch * (2.0 * e - 1.0)) / std::tanh(stretch));
     }
     auto Y = [&](int i, int j) { return yB[i] + (yTop - yB[i]) * eta[j]; };
+    m.xNodes = xN;
+    m.yNodes.resize(static_cast<size_t>(nx + 1) * (ny + 1));
+    for (int j = 0; j <= ny; ++j)
+        for (int i = 0; i <= nx; ++i)
+            m.yNodes[static_cast<size_t>(j) * (nx + 1) + i] = Y(i, j);
 
     const int n = m.n;
     m.cx.resize(n);
@@ -195,7 +201,120 @@ StructMesh makeCurvedPeriodic(const std::vector<double> &xN, const std::vector<d
         const double nu = meanH / re;
         y1t = yPlus * nu / uTau;
     }
-    return buildPeriodic(xN, yB, yTop, ny, y1t);
+    StructMesh m = buildPeriodic(xN, yB, yTop, ny, y1t);
+    m.bottomName = "bottom_wall";
+    m.topName = "top_wall";
+    return m;
+}
+
+std::vector<char> meshBinary(const StructMesh &m) {
+    const int nx = m.nx, ny = m.ny, n = m.n, nfy = m.nfy();
+    const double dz = 1.0, zc = 0.5 * dz;
+    std::vector<char> out;
+    auto raw = [&](const void *p, size_t bytes) {
+        const char *c = static_cast<const char *>(p);
+        out.insert(out.end(), c, c + bytes);
+    };
+    auto i32 = [&](int v) { raw(&v, sizeof v); };
+    auto f64 = [&](double v) { raw(&v, sizeof v); };
+    auto vec = [&](double x, double y, double z) {
+        f64(x);
+        f64(y);
+        f64(z);
+    };
+    const int nInternal = 2 * nx * ny - nx, nFaces = nInternal + 2 * nx;
+    const int nNodes = 2 * (nx + 1) * (ny + 1);
+    const uint32_t magic = 0x4D534832; // "MSH2"
+    raw(&magic, sizeof magic);
+    i32(n);
+    i32(nFaces);
+    i32(nNodes);
+    i32(2);
+    i32(nInternal);
+    for (int k = 0; k < 2; ++k) // front plane z = 0, back plane z = dz
+        for (int j = 0; j <= ny; ++j)
+            for (int i = 0; i <= nx; ++i)
+                vec(m.xNodes[i], m.yNodes[static_cast<size_t>(j) * (nx + 1) + i], k * dz);
+    // faces in the generator's order (Mesh.cpp:646-720); fields as Mesh::saveBinary writes
+    // them: owner, neighbour, patch, centre, normal, area, delta, d, weight, shift
+    std::vector<std::vector<int>> cellFaces(n);
+    int fi = 0;
+    auto xFace = [&](int c, int q) {
+        i32(c);
+        i32(q);
+        i32(-1);
+        vec(m.xfx[c], m.xfy[c], zc);
+        vec(m.xnx[c], m.xny[c], 0.0);
+        f64(m.xa[c]);
+        f64(m.xdl[c]);
+        vec(m.xdx[c], m.xdy[c], 0.0);
+        f64(m.xw[c]);
+        vec(m.xsh[c], 0.0, 0.0);
+        cellFaces[c].push_back(fi);
+        cellFaces[q].push_back(fi);
+        ++fi;
+    };
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx - 1; ++i)
+            xFace(j * nx + i, j * nx + i + 1);
+    for (int j = 0; j < ny; ++j)
+        xFace(j * nx + nx - 1, j * nx);
+    for (int jf = 1; jf < ny; ++jf)
+        for (int i = 0; i < nx; ++i) {
+            const int g = jf * nx + i, o = g - nx;
+            i32(o);
+            i32(g);
+            i32(-1);
+            vec(m.yfx[g], m.yfy[g], zc);
+            vec(m.ynx[g], m.yny[g], 0.0);
+            f64(m.ya[g]);
+            f64(m.ydl[g]);
+            vec(m.ydx[g], m.ydy[g], 0.0);
+            f64(m.yw[g]);
+            vec(0.0, 0.0, 0.0);
+            cellFaces[o].push_back(fi);
+            cellFaces[g].push_back(fi);
+            ++fi;
+        }
+    std::vector<int> patchFaces[2];
+    for (int side = 0; side < 2; ++side)
+        for (int i = 0; i < nx; ++i) {
+            const int g = (side == 0 ? 0 : ny) * nx + i;
+            const int o = (side == 0 ? 0 : ny - 1) * nx + i;
+            i32(o);
+            i32(-1);
+            i32(side);
+            vec(m.yfx[g], m.yfy[g], zc);
+            vec(m.ynx[g], m.yny[g], 0.0);
+            f64(m.ya[g]);
+            f64(m.ydl[g]);
+            vec(m.ydx[g], m.ydy[g], 0.0);
+            f64(m.yw[g]);
+            vec(0.0, 0.0, 0.0);
+            cellFaces[o].push_back(fi);
+            patchFaces[side].push_back(fi);
+            ++fi;
+        }
+    for (int c = 0; c < n; ++c) {
+        vec(m.cx[c], m.cy[c], zc);
+        f64(m.vol[c]);
+        i32(static_cast<int>(cellFaces[c].size()));
+        for (int f : cellFaces[c])
+            i32(f);
+    }
+    for (int side = 0; side < 2; ++side) {
+        const std::string &name = side == 0 ? m.bottomName : m.topName;
+        const std::string type = "wall";
+        i32(static_cast<int>(name.size()));
+        raw(name.data(), name.size());
+        i32(static_cast<int>(type.size()));
+        raw(type.data(), type.size());
+        i32(static_cast<int>(patchFaces[side].size()));
+        for (int f : patchFaces[side])
+            i32(f);
+    }
+    (void)nfy;
+    return out;
 }
 
 // Qualifies a mesh bounded by two parallel planar walls with orthogonal faces

@@ -24,6 +24,10 @@ struct StructMesh {
     // planar singular omega balance (empty unless the mesh qualifies)
     bool balance = false;
     std::vector<double> sing, slap, sgx, sgy; // sgx per x-face, sgy per y-face
+    // generator nodes (front plane: x of column i, y of node (i, j) at j * (nx + 1) + i)
+    // and the wall patch names, for the binary mesh export
+    std::vector<double> xNodes, yNodes;
+    std::string bottomName = "bottom", topName = "top";
     int nfy() const { return n + nx; }
 };
 
@@ -34,6 +38,11 @@ StructMesh makePeriodicChannel(int nx, int ny, double lx, double h, double reTau
 StructMesh makeCurvedPeriodic(const std::vector<double> &xNodes,
                               const std::vector<double> &yBottom, double yTop, int ny, double re,
                               double yPlus);
+
+// The reference's binary mesh file (MSH2, Mesh::saveBinary, core/src/Mesh.cpp:751-811):
+// native byte order, int32 indices, IEEE binary64 geometry, the periodic shift after
+// each face's weight. Byte-identical to the reference's file for the same generator call.
+std::vector<char> meshBinary(const StructMesh &m);
 
 // Planar singular-omega qualification and arrays (rans-uq/src/SIMPLESolver.cpp:92-153).
 void preparePlanarBalance(StructMesh &m);

@@ -27,6 +27,8 @@
  *   rq_mesh_geometry
  *       Mesh::makePeriodicChannel2D / makeCurvedChannelPeriodic2D + computeWallDistance
  *       core/src/Mesh.cpp:490-741, 431-463
+ *   rq_mesh_save_binary
+ *       Mesh::saveBinary (MSH2)                                   core/src/Mesh.cpp:751-811
  */
 #ifndef RQ_B200_H
 #define RQ_B200_H
@@ -180,6 +182,13 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
 
 /* Mesh geometry as built for the device (nCells x 4: cx, cy, volume, wall distance). */
 int rq_mesh_geometry(const rq_mesh_desc *mesh, int32_t *n_cells, double *cells);
+
+/* Mesh::saveBinary (core/src/Mesh.cpp:751-811; Mesh.hpp:264-268): the generated mesh
+   written to `path` in the reference's MSH2 binary layout (native byte order, int32
+   indices, IEEE binary64 geometry, the periodic shift after each face's weight),
+   byte-identical to the reference's file for the same generator call, so the
+   reference's Mesh::loadBinary and tools read it. Host only (no device work). */
+int rq_mesh_save_binary(const rq_mesh_desc *mesh, const char *path);
 
 /* The linear solvers of the forward model on one LDU system, in FP64
    (ILinearSolver::solve, core/include/LinearSolver.hpp:137-153; kinds RQ_SOLVER_*

@@ -301,6 +301,15 @@ def solve_snapshot(case: Case) -> dict | None:
                 turb_established=bool(est.value))
 
 
+def mesh_save_binary(case: Case, path) -> None:
+    """The reference's Mesh::saveBinary of the case's generated mesh (reference only)."""
+    L = lib("ref")
+    s, keep = case.struct()
+    if L.ref_mesh_save_binary(C.byref(s), os.fsencode(path)) != 0:
+        L.ref_last_error.restype = C.c_char_p
+        raise RuntimeError(L.ref_last_error().decode())
+
+
 def mesh(case: Case, kind: str = "ref"):
     """Cell (cx, cy, vol, wd) and face (owner, nbr, cx, cy, nx, ny, area, delta, dx, dy,
     weight, shift_x, patch) arrays of the mesh as the checker builds it."""
@@ -342,5 +351,5 @@ def rel_err(a, b) -> float:
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-__all__ = ["Case", "config1_case", "channel_probes", "solve", "solve_sequence", "solve_snapshot", "mesh", "linear_solve", "have",
+__all__ = ["Case", "config1_case", "channel_probes", "solve", "solve_sequence", "solve_snapshot", "mesh_save_binary", "mesh", "linear_solve", "have",
            "rel_err", "DEFAULT_COEFFS", "P_AMG", "P_PCG", "P_BICGSTAB", "FIELD_NAMES", "math"]

@@ -303,6 +303,20 @@ int ref_solve_snapshot(const orc_case *c, orc_result *res, double *cells, double
     }
 }
 
+// Mesh::saveBinary (core/src/Mesh.cpp:751-811) of the case's generated mesh.
+int ref_mesh_save_binary(const orc_case *c, const char *path) {
+    try {
+        std::streambuf *old = std::cout.rdbuf(nullptr);
+        Mesh mesh = buildMesh(*c);
+        std::cout.rdbuf(old);
+        mesh.saveBinary(path);
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return -1;
+    }
+}
+
 // The reference linear solvers on one LDU system: kind 0 AMG, 1 PCG, 2 BiCGSTAB,
 // 3 GaussSeidel. x is the initial guess on input and the solution on output.
 int ref_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,

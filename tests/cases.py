@@ -9,16 +9,20 @@ import numpy as np
 from oracle import checker as ck
 
 
+def product_mesh(rq, case: ck.Case):
+    """The product's Mesh for the checker case's generator call."""
+    if case.curved:
+        return rq.Mesh.make_curved_channel_periodic_2d(case.x_nodes, case.y_bottom, case.y_top,
+                                                      case.ny, case.re_mesh, case.yplus)
+    return rq.Mesh.make_periodic_channel_2d(case.nx, case.ny, case.lx, case.h, case.re_tau,
+                                            case.yplus)
+
+
 def product_batch(rq, case: ck.Case, pressure_solver: str = "AMG", precision: str = "fp64",
                   block_threads: int = 0, model_class=None):
     """A ForwardBatch (or model_class, e.g. rq.ForwardModel) on the GPU path with the same
     inputs as the checker case."""
-    if case.curved:
-        mesh = rq.Mesh.make_curved_channel_periodic_2d(case.x_nodes, case.y_bottom, case.y_top,
-                                                      case.ny, case.re_mesh, case.yplus)
-    else:
-        mesh = rq.Mesh.make_periodic_channel_2d(case.nx, case.ny, case.lx, case.h, case.re_tau,
-                                                case.yplus)
+    mesh = product_mesh(rq, case)
     mesh.compute_wall_distance()
     obs = rq.ObservationOperator()
     for x, y, v, s in zip(case.obs_x, case.obs_y, case.obs_value, case.obs_sigma):
@@ -79,3 +83,13 @@ def bump_case(nx=24, ny=16, **kw) -> ck.Case:
                    alpha_p=0.25, body_force=(4e-3, 0.0, 0.0), tol=1e-6, max_iter=200,
                    obs_x=x, obs_y=y, obs_value=np.zeros(6), obs_sigma=np.full(6, 1e-2))
     return dataclasses.replace(base, **kw)
+
+
+# Generator calls whose binary mesh files (Mesh::saveBinary) are pinned by digest.
+MESH_BINARY_CASES = {
+    "channel_3x24": ck.Case(ny=24, yplus=1.0),
+    "channel_3x128_config1": ck.config1_case(),
+    "channel_3x512_re1000": ck.Case(ny=512, re_tau=1000.0, yplus=0.5),
+    "bump_24x16": bump_case(24, 16),
+    "bump_200x100": bump_case(200, 100),
+}

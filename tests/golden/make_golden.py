@@ -42,7 +42,19 @@ def sequence_npz(name, case, thetas, byte_budget=64 * 1024 * 1024):
 
 
 def main():
-    which = set(sys.argv[1:]) or {"small", "config1", "goldens", "warm", "snapshot"}
+    which = set(sys.argv[1:]) or {"small", "config1", "goldens", "warm", "snapshot", "meshbin"}
+    if "meshbin" in which:
+        import hashlib
+        import tempfile
+        digests = {}
+        for name, case in cases.MESH_BINARY_CASES.items():
+            with tempfile.TemporaryDirectory() as d:
+                path = Path(d) / "mesh.bin"
+                ck.mesh_save_binary(case, path)
+                data = path.read_bytes()
+            digests[name] = {"bytes": len(data), "sha256": hashlib.sha256(data).hexdigest()}
+            print(name, len(data), flush=True)
+        (OUT / "mesh_binary_sha256.json").write_text(json.dumps(digests, indent=1))
     if "snapshot" in which:
         for name, case in (("snapshot_small_channel_ref", cases.small_channel()),
                            ("snapshot_small_channel_capped_ref", cases.small_channel(max_iter=300))):
