@@ -113,6 +113,10 @@ SIGNATURES = {
     "rq_server_info": ([C.c_void_p, IP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), IP],
                        C.c_int),
     "rq_server_destroy": ([C.c_void_p], C.c_int),
+    "rq_resample_indices": ([DP, C.c_int64, DP, C.c_int64, C.POINTER(C.c_int64)], C.c_int),
+    "rq_predictive_moments": ([DP, C.c_int64, C.c_int32, DP, DP], C.c_int),
+    "rq_conformal_quantile": ([DP, C.c_int64, C.c_double, DP], C.c_int),
+    "rq_split_conformal": ([DP, DP, C.c_int64, DP, C.c_int64, C.c_double, DP, DP], C.c_int),
     "rq_warm_cache_create": ([C.c_void_p, C.c_int32, C.c_double, C.c_uint64,
                               C.POINTER(C.c_void_p)], C.c_int),
     "rq_warm_cache_destroy": ([C.c_void_p], C.c_int),

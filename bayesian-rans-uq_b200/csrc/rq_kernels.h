@@ -32,5 +32,17 @@ cudaError_t launchSolveNoAlloc(const DevJob &job, int block, int arenaDoubles, c
 // Posterior weights (rq_stats.cu): one CTA; out = {max, sum of exp, non-finite count}.
 cudaError_t launchWeights(const double *ll, const double *lq, int64_t n, double *w, double *out,
                           cudaStream_t stream);
+// Statistics of an ensemble (rq_stats.cu), each with numpy's rounding: multinomial
+// indices for given uniforms (cdf: n doubles of scratch), column mean / variance,
+// the k-th smallest nonnegative value, |a - b|, and test -/+ radius.
+cudaError_t launchResample(const double *w, int64_t n, const double *u, int64_t m, int64_t *idx,
+                           double *cdf, cudaStream_t stream);
+cudaError_t launchMoments(const double *x, int64_t n, int d, double *mean, double *var,
+                          cudaStream_t stream);
+cudaError_t launchSelect(const double *v, int64_t n, int64_t k, double *out, cudaStream_t stream);
+cudaError_t launchAbsDiff(const double *a, const double *b, int64_t n, double *out,
+                          cudaStream_t stream);
+cudaError_t launchInterval(const double *test, int64_t m, const double *radius, double *lo,
+                           double *hi, cudaStream_t stream);
 
 } // namespace rq

@@ -19,6 +19,9 @@
  *       several ForwardBatch::evaluate calls (one per mesh class) fused into one launch
  *   rq_solve
  *       SIMPLESolver::initUniform + solve(FlowFields&, Workspace&) rans-uq/src/SIMPLESolver.cpp:267-298, 1193-1716
+ *   rq_resample_indices, rq_predictive_moments, rq_conformal_quantile, rq_split_conformal
+ *       cfdr.statistics resample_posterior / predictive_summary / conformal_quantile /
+ *       split_conformal_intervals                     rans-uq/python/cfdr/statistics.py:235-378
  *   rq_evaluate_cached, rq_warm_cache_*
  *       ForwardModel::evaluateWithDiagnostics with its WarmStartCache rans-uq/src/ForwardModel.cpp:35-137,
  *       rans-uq/include/ForwardModel.hpp:21-157 (size, clear, setByteBudget, byteBudget, retainedBytes)
@@ -278,6 +281,30 @@ int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *co
                    int32_t *launches);
 /* Cancels requests not yet claimed, waits for the solves in flight, frees. */
 int rq_server_destroy(rq_server *s);
+
+/* ---- statistics of a finished ensemble on the GPU (cfdr.statistics,
+   rans-uq/python/cfdr/statistics.py), each with numpy's rounding so the results equal
+   the reference's. Host buffers; the random draws stay with the caller (the
+   reference's per-sample PCG64 streams).
+   rq_resample_indices: resample_posterior's pick (:235-259) for uniforms[j], the first
+   draw of output j's "posterior-resample" stream: numpy's Generator.choice(n, p=weights),
+   i.e. cdf = cumsum(weights) in index order, cdf /= cdf[n-1], indices[j] = number of cdf
+   values <= uniforms[j]. weights must pass choice's admission (nonnegative, Kahan sum
+   within sqrt(eps) of 1) or RQ_E_INVALID. */
+int rq_resample_indices(const double *weights, int64_t n, const double *uniforms, int64_t m,
+                        int64_t *indices);
+/* predictive_summary's latent moments (:277-339): mean and population variance (ddof 0)
+   of each column of the row-major n x d matrix, summed in numpy's order. */
+int rq_predictive_moments(const double *latent, int64_t n, int32_t d, double *mean,
+                          double *variance);
+/* conformal_quantile (:349-355): the ceil((n+1)(1-alpha))-th smallest score, +inf when
+   that rank exceeds n. */
+int rq_conformal_quantile(const double *scores, int64_t n, double alpha, double *quantile);
+/* split_conformal_intervals (:358-378): radius = conformal quantile of |y - prediction|
+   over the calibration set; lower/upper = test_pred -/+ radius (m values each). */
+int rq_split_conformal(const double *cal_y, const double *cal_pred, int64_t n,
+                       const double *test_pred, int64_t m, double alpha, double *lower,
+                       double *upper);
 
 /* ---- warm starts: the sequential model's cache of converged states
    (WarmStartCache, rans-uq/include/ForwardModel.hpp:21-157; the model's own is

@@ -39,3 +39,72 @@ def test_nonfinite_loglik_rejected():
         st.posterior_weights(np.array([-1.0, np.nan, -3.0]))
     with pytest.raises(ValueError, match="finite"):
         st.posterior_weights(np.array([-1.0, -np.inf]))
+
+
+# ---- resampling, predictive moments and split conformal (rq_resample_indices,
+# rq_predictive_moments, rq_conformal_quantile, rq_split_conformal) against the
+# reference's own cfdr.statistics functions (fixture tests/golden/statistics_ref.npz,
+# written by tests/golden/make_statistics_golden.py) and numpy: exact equality, since
+# the device reproduces numpy's summation order and rounding.
+from pathlib import Path  # noqa: E402
+
+from rans_uq_b200.workloads import sample_rng  # noqa: E402
+
+REF = np.load(Path(__file__).parent / "golden" / "statistics_ref.npz")
+
+
+def test_resample_indices_equal_numpy_choice():
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 9, 300, 20000):
+        w = rng.exponential(size=n) ** 3
+        w /= w.sum()
+        ids = range(100, 400)
+        u = [sample_rng(11, i, "posterior-resample").random() for i in ids]
+        want = [int(sample_rng(11, i, "posterior-resample").choice(n, p=w)) for i in ids]
+        np.testing.assert_array_equal(st.resample_indices(w, u), want)
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_resample_posterior_matches_reference(tag):
+    draws = st.resample_posterior(REF[f"{tag}_ids"], REF[f"{tag}_theta"], REF[f"{tag}_ll"],
+                                  REF[f"{tag}_resample_ids"], root_seed=20261010)
+    assert [d[0] for d in draws] == REF[f"{tag}_resample_ids"].tolist()
+    np.testing.assert_array_equal(np.array([d[1] for d in draws]), REF[f"{tag}_resample_theta"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_predictive_summary_matches_reference(tag):
+    d = REF[f"{tag}_pred"].shape[1]
+    s = st.predictive_summary(REF[f"{tag}_ids"], REF[f"{tag}_pred"], root_seed=77,
+                              observation_sigma=REF[f"{tag}_sigma"],
+                              surrogate_variance=np.full(d, 0.01))
+    np.testing.assert_array_equal(np.array(s.latent_mean), REF[f"{tag}_latent_mean"])
+    np.testing.assert_array_equal(np.array(s.latent_variance), REF[f"{tag}_latent_variance"])
+    np.testing.assert_array_equal(np.array(s.total_variance), REF[f"{tag}_total_variance"])
+    np.testing.assert_array_equal(np.array(s.samples), REF[f"{tag}_samples"])
+    assert s.includes_surrogate_noise and s.includes_observation_noise
+    assert not s.includes_discrepancy
+
+
+@pytest.mark.parametrize("n", [1, 19, 1000, 20000])
+def test_conformal_quantile_matches_reference(n):
+    got = [st.conformal_quantile(REF[f"scores_{n}"], a) for a in (0.05, 0.1, 0.5, 0.9)]
+    np.testing.assert_array_equal(got, REF[f"quantile_{n}"])
+
+
+def test_split_conformal_matches_reference():
+    lo, hi = st.split_conformal_intervals(REF["cal_y"], REF["cal_p"], REF["test_p"], alpha=0.1)
+    np.testing.assert_array_equal(lo, REF["split_lo"])
+    np.testing.assert_array_equal(hi, REF["split_hi"])
+
+
+def test_statistics_reject_what_the_reference_rejects():
+    with pytest.raises(ValueError, match="sum to 1"):
+        st.resample_indices([0.5, 0.6], [0.1])
+    with pytest.raises(ValueError, match="non-negative"):
+        st.resample_indices([1.5, -0.5], [0.1])
+    with pytest.raises(ValueError, match="nonnegative"):
+        st.conformal_quantile([1.0, -2.0], 0.1)
+    with pytest.raises(ValueError, match="alpha"):
+        st.conformal_quantile([1.0, 2.0], 1.0)
+    assert st.conformal_quantile([3.0, 1.0, 2.0], 0.05) == np.inf  # rank 4 > n
