@@ -101,6 +101,7 @@ SIGNATURES = {
     "rq_evaluate_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
                             C.c_int),
     "rq_posterior_weights": ([DP, DP, C.c_int64, DP, DP], C.c_int),
+    "rq_posterior_weights_parts": ([DP, DP, C.c_int64, DP, DP, DP], C.c_int),
     "rq_posterior_weights_device": ([C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                      C.c_void_p], C.c_int),
     "rq_server_create": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_int32,

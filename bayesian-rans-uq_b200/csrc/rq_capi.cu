@@ -812,6 +812,32 @@ int rq_posterior_weights(const double *loglik, const double *log_q, int64_t n, d
     });
 }
 
+int rq_posterior_weights_parts(const double *loglik, const double *log_q, int64_t n,
+                               double *weights, double *max_out, double *sum_out) {
+    return guarded([&] {
+        if (n < 1)
+            throw std::invalid_argument("at least one evaluation is required");
+        if (!loglik || !weights || !max_out || !sum_out)
+            throw std::invalid_argument("null argument");
+        DevBuf d;
+        const size_t b = sizeof(double) * static_cast<size_t>(n);
+        d.ensure(3 * b + 4 * sizeof(double));
+        double *dl = d.as<double>(), *dq = log_q ? dl + n : nullptr, *dw = dl + 2 * n,
+               *dout = dl + 3 * n;
+        check(cudaMemcpy(dl, loglik, b, cudaMemcpyHostToDevice), "loglik");
+        if (log_q)
+            check(cudaMemcpy(dq, log_q, b, cudaMemcpyHostToDevice), "log_q");
+        check(rq::launchWeights(dl, dq, n, dw, dout, nullptr), "weights launch");
+        double out[3];
+        check(cudaMemcpy(out, dout, sizeof(out), cudaMemcpyDeviceToHost), "weights");
+        if (out[2] != 0.0)
+            throw std::invalid_argument("successful log likelihoods must be finite");
+        check(cudaMemcpy(weights, dw, b, cudaMemcpyDeviceToHost), "weights");
+        *max_out = out[0];
+        *sum_out = out[1];
+    });
+}
+
 int rq_posterior_weights_device(const double *loglik_dev, const double *log_q_dev, int64_t n,
                                 double *weights_dev, double *out3_dev, void *stream) {
     return guarded([&] {

@@ -9,6 +9,10 @@ across ranks, no exchange inside a solve (a solve never spans GPUs).
 * `reduce_step` combines the per-rank step outcome: the step time is the max
   over ranks, converged solves are summed, and (optionally) the per-draw
   log-likelihoods are gathered to every rank for the importance weights.
+* `sharded_posterior_weights` normalises the importance weights of an ensemble
+  sharded across ranks without gathering it: each rank's log-sum-exp of its own
+  draws on its GPU, one all-reduce (MAX) and one all-reduce (SUM) of FP64 scalars,
+  then every rank rescales its own weights.
 
 Collectives use whatever process group is initialised: NCCL on GPUs, gloo in the
 CPU tests.
@@ -67,3 +71,48 @@ def reduce_step(ms: float, converged: int, loglik=None, device=None):
         dist.all_gather(parts, pad)
         gathered = np.concatenate([p[: int(s.item())].cpu().numpy() for p, s in zip(parts, sizes)])
     return float(t.item()), int(c.item()), gathered
+
+
+def _device_local_weights(loglik, log_q):
+    from . import statistics
+
+    return statistics.posterior_weight_parts(loglik, log_q)
+
+
+def sharded_posterior_weights(loglik, log_q=None, device=None, local=None):
+    """Normalised weights of this rank's draws in the whole sharded ensemble
+    (cfdr.statistics.posterior_weights, rans-uq/python/cfdr/statistics.py:217-232,
+    over the union of all ranks' draws) and the global log evidence.
+
+    Each rank r computes its own weights w_r, m_r = max(l - log q) and
+    s_r = sum exp(l - log q - m_r) on its GPU (`local`, by default
+    rq_posterior_weights_parts). One all-reduce (MAX) gives M = max_r m_r and one
+    all-reduce (SUM) gives S = sum_r s_r exp(m_r - M); this rank's weights are
+    w_r * s_r exp(m_r - M) / S and the log evidence M + log S. The parts stay apart
+    so that no large log value is rounded before the exponential. A rank with no
+    draws contributes nothing."""
+    import torch
+    import torch.distributed as dist
+
+    ll = np.ascontiguousarray(np.asarray(loglik, dtype=np.float64).ravel())
+    lq = None if log_q is None else np.ascontiguousarray(np.asarray(log_q, np.float64).ravel())
+    local = local or _device_local_weights
+    if ll.size:
+        w, m, s = local(ll, lq)
+    else:
+        w, m, s = np.empty(0), -np.inf, 0.0
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        if not ll.size:
+            raise ValueError("at least one evaluation is required")
+        return np.asarray(w, dtype=np.float64), m + float(np.log(s))
+    dev = device if device is not None else torch.device("cpu")
+    mt = torch.tensor([m], dtype=torch.float64, device=dev)
+    dist.all_reduce(mt, op=dist.ReduceOp.MAX)
+    big = float(mt.item())
+    if not np.isfinite(big):
+        raise ValueError("at least one evaluation is required")
+    part = s * float(np.exp(m - big)) if ll.size else 0.0
+    st = torch.tensor([part], dtype=torch.float64, device=dev)
+    dist.all_reduce(st)
+    total = float(st.item())
+    return np.asarray(w, dtype=np.float64) * (part / total), big + float(np.log(total))

@@ -48,6 +48,23 @@ def posterior_weights(evaluations, log_q=None, return_log_evidence: bool = False
     return (w, float(ev.value)) if return_log_evidence else w
 
 
+def posterior_weight_parts(loglik, log_q=None):
+    """(weights, m, s): the normalised weights of these draws with the two parts of
+    their log-sum-exp, m = max(l - log q) and s = sum exp(l - log q - m)
+    (rq_posterior_weights_parts), for combining shards of one ensemble."""
+    ll = _logliks(loglik)
+    lq = None
+    if log_q is not None:
+        lq = np.ascontiguousarray(np.asarray(log_q, dtype=np.float64).ravel())
+        if lq.shape != ll.shape:
+            raise ValueError("log_q must have one value per evaluation")
+    w = np.empty_like(ll)
+    m, s = C.c_double(), C.c_double()
+    N.call("rq_posterior_weights_parts", N.dptr(ll), N.dptr(lq) if lq is not None else None,
+           C.c_int64(ll.size), N.dptr(w), C.byref(m), C.byref(s))
+    return w, float(m.value), float(s.value)
+
+
 # ---- the rest of the statistics of a finished ensemble (cfdr.statistics,
 # rans-uq/python/cfdr/statistics.py:235-378), computed on the GPU with numpy's rounding.
 # Random draws come from the reference's per-sample streams (workloads.sample_rng) on

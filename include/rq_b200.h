@@ -248,6 +248,11 @@ int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_
    m + log(sum), the log-sum-exp. */
 int rq_posterior_weights(const double *loglik, const double *log_q, int64_t n, double *weights,
                          double *log_evidence);
+/* The same with the two parts of the log-sum-exp kept apart: max_out = m and
+   sum_out = sum_j exp(l_j - log_q_j - m), for combining shards of one ensemble held
+   by several ranks without the rounding of m + log(sum). */
+int rq_posterior_weights_parts(const double *loglik, const double *log_q, int64_t n,
+                               double *weights, double *max_out, double *sum_out);
 /* The same on device buffers on a stream, queued without waiting; out3_dev
    receives {m, sum, number of non-finite terms} (weights are unset when the count
    is nonzero). */

@@ -108,3 +108,17 @@ def test_statistics_reject_what_the_reference_rejects():
     with pytest.raises(ValueError, match="alpha"):
         st.conformal_quantile([1.0, 2.0], 1.0)
     assert st.conformal_quantile([3.0, 1.0, 2.0], 0.05) == np.inf  # rank 4 > n
+
+
+def test_weight_parts_match_weights():
+    """rq_posterior_weights_parts: the same weights as rq_posterior_weights, with the
+    log-sum-exp split into its maximum and its scaled sum (the inputs of the sharded
+    combination in rans_uq_b200.replicas, whose two-rank collectives are tested on CPU)."""
+    rng = np.random.default_rng(8)
+    ll = -0.5 * rng.chisquare(30, 5000) * 9.0
+    lq = rng.normal(0.0, 2.0, 5000)
+    w, ev = st.posterior_weights(ll, lq, return_log_evidence=True)
+    w2, m, s = st.posterior_weight_parts(ll, lq)
+    np.testing.assert_array_equal(w2, w)
+    assert m == np.max(ll - lq)
+    assert abs(m + math.log(s) - ev) <= 1e-15 * abs(ev)

@@ -66,3 +66,62 @@ def test_reduce_step_two_gloo_ranks():
     for rank, ms, conv, ll in res:
         assert ms == 250.5 and conv == 169
         assert ll == [0.0, 1.0, 2.0, 10.0, 11.0, 12.0, 13.0]
+
+
+def _reference_weights(ll):
+    """cfdr.statistics.posterior_weights' rule on the host: exp(l - max) / fsum."""
+    import math
+
+    m = max(ll)
+    w = [math.exp(v - m) for v in ll]
+    s = math.fsum(w)
+    return np.asarray(w) / s, m + math.log(s)
+
+
+def _reference_parts(ll):
+    import math
+
+    m = max(ll)
+    w = [math.exp(v - m) for v in ll]
+    s = math.fsum(w)
+    return np.asarray(w) / s, m, s
+
+
+def _weights_worker(rank, world, port, q, parts):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # the per-rank step is the device kernel on a GPU; the host rule stands in here
+        w, g = rp.sharded_posterior_weights(parts[rank],
+                                            local=lambda ll, lq: _reference_parts(list(ll)))
+        q.put((rank, w.tolist(), g))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_posterior_weights_two_gloo_ranks():
+    """Two ranks holding 70 and 30 draws normalise their own weights with one MAX and one
+    SUM all-reduce: the concatenation equals the single-process weights and the log
+    evidence agrees. The tolerance is the rounding of l - max itself: a shard subtracts
+    its own maximum, so exp sees an argument rounded differently by up to an ulp of
+    |l| (4 ulp of the largest |l| here, relative)."""
+    rng = np.random.default_rng(5)
+    ll = -0.5 * rng.chisquare(30, 100) * 12.0
+    parts = [ll[:70], ll[70:]]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_weights_worker, args=(r, 2, port, q, parts)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want, g_ref = _reference_weights(list(ll))
+    got = np.concatenate([np.asarray(r[1]) for r in res])
+    rtol = 4 * np.max(np.abs(ll)) * np.finfo(float).eps
+    np.testing.assert_allclose(got, want, rtol=rtol, atol=0)
+    assert abs(got.sum() - 1.0) < 1e-14
+    for r in res:
+        assert abs(r[2] - g_ref) <= 1e-14 * abs(g_ref)
