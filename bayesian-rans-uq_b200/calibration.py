@@ -9,15 +9,20 @@ solves run as one batch on the GPU (docs/figures/calibration_coverage.py:116-262
 4. two independent Student-t importance samples of 64 draws (nu = 4) from that
    centre and scale (:170-184), each weighted by likelihood over proposal
    density on the GPU in FP64 (statistics.posterior_weights) and resampled
-   (cfdr.statistics.resample_posterior, rans-uq/python/cfdr/statistics.py:235-259).
+   (cfdr.statistics.resample_posterior, rans-uq/python/cfdr/statistics.py:235-259);
+   with the stations' noise sigma, the 400 resampled draws' predictions give the
+   posterior predictive summary and its 90 % ranges (importance_posterior, :183-222)
+5. with the observed profile, the split-conformal recalibration of those ranges on
+   the log scale and their coverage of the held-out third of the stations
+   (calibrate, :257-288).
 
 The stage logic follows the reference step for step (same seeds, sample ids,
 identity strings and tie rules) so the same log-likelihoods give the same path,
-fit and draws; only the forward model changed. The predictive summary and the
-split-conformal intervals of the figure script are not part of this module.
+fit and draws; only the forward model changed.
 
-`evaluator(ids, theta) -> (status names, log-likelihoods)` is the forward model
-of a stage: `batch_evaluator(ForwardBatch)` runs one GPU batch per stage.
+`evaluator(ids, theta) -> (status names, log-likelihoods[, predictions])` is the
+forward model of a stage: `batch_evaluator(ForwardBatch)` runs one GPU batch per
+stage and returns the station predictions too.
 """
 from __future__ import annotations
 
@@ -34,6 +39,7 @@ STAGE1_BOX = ((0.28, 0.084), (0.34, 0.096))
 SEARCH_STEP = (0.004, 0.001)
 PROPOSAL_DRAWS = 64
 PROPOSAL_DOF = 4
+ALPHA = 0.1
 
 
 def batch_evaluator(batch):
@@ -41,16 +47,21 @@ def batch_evaluator(batch):
     def evaluate(ids, theta):
         res = batch.evaluate(np.asarray(theta, dtype=np.float64))
         return ([r.result.status.name for r in res.rows],
-                np.array([r.result.log_lik for r in res.rows], dtype=np.float64))
+                np.array([r.result.log_lik for r in res.rows], dtype=np.float64),
+                np.array([r.result.predictions for r in res.rows], dtype=np.float64))
     return evaluate
 
 
-def _evaluate(evaluator, ids, theta):
-    status, ll = evaluator(list(ids), np.asarray(theta, dtype=np.float64))
+def _evaluate(evaluator, ids, theta, with_predictions=False):
+    out = evaluator(list(ids), np.asarray(theta, dtype=np.float64))
+    status, ll = out[0], out[1]
     failed = sum(1 for s, v in zip(status, ll) if s != "Converged" or not math.isfinite(v))
     if failed:
         raise RuntimeError(f"{failed} solves failed; the posterior is undefined")
-    return np.asarray(ll, dtype=np.float64)
+    ll = np.asarray(ll, dtype=np.float64)
+    if with_predictions:
+        return ll, (np.asarray(out[2], dtype=np.float64) if len(out) > 2 else None)
+    return ll
 
 
 def uniform_design(ids, lower, upper, root_seed):
@@ -110,14 +121,19 @@ def student_t_draws(center, scale, ids, seed, nu=PROPOSAL_DOF):
     return np.array(theta), np.array(log_q)
 
 
-def resample(ids_in, theta, weights, out_ids, root_seed):
-    """IID multinomial draws from the weighted sample: inputs in sample-id order,
-    one stream per output id."""
+def resample_picks(ids_in, weights, out_ids, root_seed):
+    """Indices (into ids_in) of IID multinomial draws from the weighted sample: inputs
+    in sample-id order, one stream per output id."""
     order = np.argsort(np.asarray(ids_in), kind="stable")
-    w, th = np.asarray(weights)[order], np.asarray(theta)[order]
+    w = np.asarray(weights)[order]
     picks = [int(sample_rng(root_seed, i, "posterior-resample").choice(len(w), p=w))
              for i in out_ids]
-    return th[picks]
+    return order[picks]
+
+
+def resample(ids_in, theta, weights, out_ids, root_seed):
+    """The drawn theta rows (resample_posterior's draws, in output-id order)."""
+    return np.asarray(theta)[resample_picks(ids_in, weights, out_ids, root_seed)]
 
 
 @dataclass
@@ -138,32 +154,51 @@ class Calibration:
     scale: np.ndarray
     importance: list = field(default_factory=list)   # main, replicate
     stages: list = field(default_factory=list)
+    study: dict = field(default_factory=dict)        # ranges, recalibration, coverage
 
     @property
     def solves(self) -> int:
         return sum(s.solves for s in self.stages)
 
 
-def importance_stage(evaluator, center, scale, ids, seed, weights=None):
+def importance_stage(evaluator, center, scale, ids, seed, weights=None, sigma=None,
+                     stats=None):
+    """One Student-t importance sample (importance_posterior, :183-222): weights,
+    400 resampled draws and, given the stations' sigma and predictions from the
+    evaluator, the posterior predictive summary of the draws and its 90 % ranges."""
     theta, log_q = student_t_draws(center, scale, ids, seed)
-    ll = _evaluate(evaluator, ids, theta)
+    ll, pred = _evaluate(evaluator, ids, theta, with_predictions=True)
     # flat prior: a draw from q weighs L / q
     w = (weights or gpu_stats.posterior_weights)(ll - log_q)
     mean = w @ theta
-    draws = resample(list(ids), theta, w, range(1000, 1400), seed + 1)
-    return {"solves": len(ids), "effective_sample_size": float(1 / np.sum(w ** 2)),
-            "max_weight": float(w.max()),
-            "distinct_draws": len({tuple(t) for t in draws}),
-            "theta_mean": mean.tolist(),
-            "theta_sd": np.sqrt(w @ (theta - mean) ** 2).tolist(),
-            "weights": w, "theta": theta, "log_q": log_q, "log_lik": ll}
+    picks = resample_picks(list(ids), w, range(1000, 1400), seed + 1)
+    draws = theta[picks]
+    out = {"solves": len(ids), "effective_sample_size": float(1 / np.sum(w ** 2)),
+           "max_weight": float(w.max()),
+           "distinct_draws": len({tuple(t) for t in draws}),
+           "theta_mean": mean.tolist(),
+           "theta_sd": np.sqrt(w @ (theta - mean) ** 2).tolist(),
+           "weights": w, "theta": theta, "log_q": log_q, "log_lik": ll}
+    if sigma is not None and pred is not None:
+        # each draw repeats an evaluated theta: its predictions are reused, not re-solved
+        predictive = (stats or gpu_stats).predictive_summary(
+            range(1000, 1400), pred[picks], root_seed=seed + 2, observation_sigma=sigma)
+        samples = np.asarray(predictive.samples)
+        low, high = np.quantile(samples, [ALPHA / 2, 1 - ALPHA / 2], axis=0)
+        out.update(predictive=predictive, low=low, high=high, posterior_latent=pred[picks])
+    return out
 
 
-def calibrate(evaluator, clock=None, weights=None, trace=None) -> Calibration:
+def calibrate(evaluator, clock=None, weights=None, trace=None, truth=None, sigma=None,
+              stats=None) -> Calibration:
     """All stages, each one batch of solves (pattern-search steps one batch each).
     weights: the importance-weight function (default: FP64 on the GPU); trace (a
     dict, optional) receives each stage's intermediate results as they appear, so
-    a stage that raises leaves the earlier ones behind."""
+    a stage that raises leaves the earlier ones behind. With the stations' observed
+    profile `truth` and noise `sigma` (and an evaluator that returns predictions),
+    the study's predictive ranges, split-conformal recalibration and coverage follow
+    (out.study); `stats` supplies predictive_summary and split_conformal_intervals
+    (default: the GPU ones)."""
     import time
 
     clock = clock or time.perf_counter
@@ -195,6 +230,37 @@ def calibrate(evaluator, clock=None, weights=None, trace=None) -> Calibration:
     for name, ids, seed in (("importance", range(300, 300 + PROPOSAL_DRAWS), SEED + 1),
                             ("replicate", range(400, 400 + PROPOSAL_DRAWS), SEED + 11)):
         t = clock()
-        out.importance.append(importance_stage(evaluator, center, scale, ids, seed, weights))
+        out.importance.append(importance_stage(evaluator, center, scale, ids, seed, weights,
+                                               sigma, stats))
         stages.append(Stage(name, len(ids), clock() - t))
+    if truth is not None and "predictive" in out.importance[0]:
+        out.study = coverage_study(out.importance[0], out.importance[1],
+                                   np.asarray(truth, dtype=float), stats or gpu_stats)
     return out
+
+
+def coverage_study(main, replicate, truth, stats):
+    """The study's ranges and their honesty (calibrate, :257-288): stations split
+    into thirds by index (likelihood, conformal calibration, held out); the
+    split-conformal correction of the main sample's latent mean on the log scale;
+    how many held-out stations each range covers."""
+    group = np.arange(len(truth)) % 3
+    cal, test = group == 1, group == 2
+    prediction = np.asarray(main["predictive"].latent_mean)
+    log_lo, log_hi = stats.split_conformal_intervals(np.log(truth[cal]), np.log(prediction[cal]),
+                                                     np.log(prediction), alpha=ALPHA)
+    low, high = main["low"], main["high"]
+    rec_low, rec_high = np.exp(log_lo), np.exp(log_hi)
+    r_low, r_high = replicate["low"], replicate["high"]
+    return {"group": group.tolist(), "prediction": prediction.tolist(),
+            "standard_low": low.tolist(), "standard_high": high.tolist(),
+            "recalibrated_low": rec_low.tolist(), "recalibrated_high": rec_high.tolist(),
+            "latent_variance": list(main["predictive"].latent_variance),
+            "observation_variance": list(main["predictive"].observation_variance),
+            "standard_covered": int(np.sum((truth >= low) & (truth <= high) & test)),
+            "recalibrated_covered": int(np.sum((truth >= rec_low) & (truth <= rec_high) & test)),
+            "held_out": int(test.sum()),
+            "replicate": {"prediction": list(replicate["predictive"].latent_mean),
+                          "standard_low": r_low.tolist(), "standard_high": r_high.tolist(),
+                          "standard_covered": int(np.sum((truth >= r_low) & (truth <= r_high)
+                                                         & test))}}

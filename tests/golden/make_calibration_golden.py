@@ -117,5 +117,93 @@ out = {"stage1_best": list(first.theta), "stage1_best_ll": first.log_likelihood,
        "center": center.tolist(), "scale": scale.tolist(),
        "main": importance(range(300, 300 + cal.PROPOSAL_DRAWS), cal.SEED + 1),
        "replicate": importance(range(400, 400 + cal.PROPOSAL_DRAWS), cal.SEED + 11)}
+
+
+# ---- the reference's whole study, calibrate() (calibration_coverage.py:225-307), on
+# the same analytic log-likelihood with 30 analytic station predictions, and a
+# synthetic profile written in the simulation files' column layout (y/delta, y+, U+):
+# the posterior predictive ranges, the split-conformal recalibration and coverage.
+def station_speed(y):
+    """A smooth positive stand-in for the mean profile at y (in half heights)."""
+    yp = np.asarray(y) * cal.RE_TAU
+    return 2.5 * np.log1p(yp) + 5.0 * (1.0 - np.exp(-yp / 11.0))
+
+
+def analytic_predictions(theta, y):
+    return station_speed(y) * (1 + 4 * (theta[0] - 0.3137) - 9 * (theta[1] - 0.0912))
+
+
+class Vec3:
+    def __init__(self, x=0.0, y=0.0, z=0.0):
+        self.x, self.y, self.z = x, y, z
+
+
+class Observations:
+    def __init__(self):
+        self.y = []
+
+    def add_velocity_profile(self, at, component, value, sigma):
+        self.y.append(at.y)
+
+
+class _StudyResult:
+    def __init__(self, theta, y):
+        self.status = _Status()
+        self.log_lik = analytic_loglik(theta)
+        self.predictions = [float(v) for v in analytic_predictions(theta, y)]
+        self.simple_iters = 1
+
+
+class StudyBatch(ForwardBatch):
+    def __init__(self, mesh=None, params=None, obs=None, *args):
+        self.y = np.asarray(obs.y)
+
+    def evaluate(self, theta, workers=1):
+        rows = []
+        for t in np.asarray(theta):
+            row = _Row(t)
+            row.result = _StudyResult(t, self.y)
+            rows.append(row)
+        return types.SimpleNamespace(rows=rows)
+
+
+class Mesh:
+    @staticmethod
+    def make_periodic_channel_2d(*args):
+        return types.SimpleNamespace(compute_wall_distance=lambda: None)
+
+
+core.Vec3 = Vec3
+core.ObservationOperator = Observations
+core.Mesh = Mesh
+core.SolverSettings = types.SimpleNamespace
+core.FlowBoundaryConditions = types.SimpleNamespace(channel_defaults=lambda *a: None)
+core.InferenceParameterSet = types.SimpleNamespace(a1_betaStar=lambda: None)
+core.ForwardBatch = StudyBatch
+cal.c = core
+
+import tempfile  # noqa: E402
+
+yp_grid = np.geomspace(0.05, 182.088, 400)
+speed = station_speed(yp_grid / cal.RE_TAU)
+noise = np.random.default_rng(5).standard_normal(400)
+with tempfile.TemporaryDirectory() as d:
+    mean_file, stdev_file = Path(d) / "mean.dat", Path(d) / "stdev.dat"
+    np.savetxt(mean_file, np.column_stack([yp_grid / cal.RE_TAU, yp_grid,
+                                           speed * (1 + 0.01 * noise)]), header="synthetic",
+               comments="% ")
+    np.savetxt(stdev_file, np.column_stack([yp_grid / cal.RE_TAU, yp_grid, 0.0014 * speed]),
+               header="synthetic", comments="% ")
+    study = cal.calibrate(mean_file, stdev_file, 1)
+keys = ("y_plus", "truth", "sigma", "group", "prediction", "standard_low", "standard_high",
+        "recalibrated_low", "recalibrated_high", "latent_variance", "observation_variance",
+        "standard_covered", "recalibrated_covered", "held_out", "effective_sample_size",
+        "distinct_draws", "solves")
+out["study"] = {k: study[k] for k in keys}
+out["study"]["replicate"] = {k: study["replicate"][k] for k in
+                             ("prediction", "standard_low", "standard_high", "standard_covered")}
+out["study"]["predictive_samples_head"] = study["predictive_samples"][:3]
+out["study"]["predictive_samples_mean"] = np.mean(study["predictive_samples"], axis=0).tolist()
+print("study", study["standard_covered"], study["recalibrated_covered"], study["held_out"])
 (HERE / "calibration_stages.json").write_text(json.dumps(out, indent=1))
 print("path steps", len(path), "center", center, "ESS", out["main"]["effective_sample_size"])

@@ -74,3 +74,72 @@ def test_resample_order_invariance():
     a = cal.resample(ids, theta, w, range(5), 7)
     b = cal.resample([ids[k] for k in perm], theta[perm], w[perm], range(5), 7)
     np.testing.assert_array_equal(a, b)
+
+
+# ---- the whole study: predictive ranges, split-conformal recalibration, coverage.
+# The golden is the reference's calibrate() itself (make_calibration_golden.py) on the
+# analytic log-likelihood with 30 analytic station predictions and a synthetic profile.
+STUDY = GOLD["study"]
+
+
+def station_speed(y):
+    """The stand-in profile of make_calibration_golden.py."""
+    yp = np.asarray(y) * 182.088
+    return 2.5 * np.log1p(yp) + 5.0 * (1.0 - np.exp(-yp / 11.0))
+
+
+def study_evaluator(ids, theta):
+    y = np.asarray(STUDY["y_plus"]) / 182.088
+    pred = np.array([station_speed(y) * (1 + 4 * (t[0] - 0.3137) - 9 * (t[1] - 0.0912))
+                     for t in theta])
+    return ["Converged"] * len(theta), np.array([analytic_loglik(t) for t in theta]), pred
+
+
+class HostStats:
+    """cfdr.statistics.predictive_summary (:277-339) and split_conformal_intervals
+    (:358-378) restated with numpy, for the CPU run of the study."""
+
+    @staticmethod
+    def predictive_summary(sample_ids, predictions, *, root_seed, observation_sigma):
+        from types import SimpleNamespace
+
+        from rans_uq_b200.workloads import sample_rng
+
+        ids = list(sample_ids)
+        latent = np.asarray(predictions, dtype=float)
+        obs = np.asarray(observation_sigma, dtype=float) ** 2
+        samples = latent.copy()
+        for i, sid in enumerate(ids):
+            samples[i] += sample_rng(root_seed, sid, "observation-noise").normal(
+                0, np.sqrt(obs), latent.shape[1])
+        canonical = latent[np.argsort(ids)]
+        return SimpleNamespace(samples=samples, latent_mean=canonical.mean(axis=0),
+                               latent_variance=canonical.var(axis=0, ddof=0),
+                               observation_variance=obs)
+
+    @staticmethod
+    def split_conformal_intervals(y, p, t, *, alpha):
+        scores = np.abs(np.asarray(y) - np.asarray(p))
+        k = math.ceil((scores.size + 1) * (1 - alpha))
+        r = math.inf if k > scores.size else float(np.partition(scores, k - 1)[k - 1])
+        return np.asarray(t) - r, np.asarray(t) + r
+
+
+def check_study(study):
+    for key in ("prediction", "standard_low", "standard_high", "recalibrated_low",
+                "recalibrated_high", "latent_variance", "observation_variance"):
+        np.testing.assert_array_equal(study[key], STUDY[key], err_msg=key)
+    for key in ("standard_covered", "recalibrated_covered", "held_out", "group"):
+        assert study[key] == STUDY[key], key
+    for key in ("prediction", "standard_low", "standard_high", "standard_covered"):
+        np.testing.assert_array_equal(study["replicate"][key], STUDY["replicate"][key],
+                                      err_msg=key)
+
+
+def test_study_ranges_and_recalibration_match_reference():
+    out = cal.calibrate(study_evaluator, weights=host_weights, truth=STUDY["truth"],
+                        sigma=STUDY["sigma"], stats=HostStats)
+    check(out, 1e-15)
+    check_study(out.study)
+    samples = np.asarray(out.importance[0]["predictive"].samples)
+    np.testing.assert_array_equal(samples[:3], STUDY["predictive_samples_head"])
