@@ -28,6 +28,9 @@ struct MappedBuf {
 // persistent kernel drains while the host keeps appending to it.
 struct rq_server {
     std::vector<rq_problem *> problems;
+    // every slot runs 512 threads whatever the classes' own CTA sizes, so a request's
+    // result does not depend on which other classes the server holds (a batch of a
+    // class above 1024 cells runs 768 threads; its served requests agree to rounding)
     int capacity = 0, thetaStride = 1, predStride = 1, block = 512, grid = 1, arena = 0;
     long wsStride = 0;
     long long idleNs = 0;
