@@ -32,7 +32,7 @@ int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
     if (knobKb > 0)
         bytes = std::min<long>(knobKb * 1024L, optin - shared);
     else if (nmax <= 768)
-        bytes = (optin / 2 - 1024) - shared; // two CTAs per SM
+        bytes = (optin / 2 - 1024) - shared; // half the SM (the whole hot set fits)
     else
         bytes = 0;
     bytes = std::max<long>(0, std::min(bytes, wsDoubles * 8));
