@@ -130,3 +130,64 @@ def test_config1_mixed_within_1e6(rq):
     assert row.result.status.name == "Converged"
     assert rel(row.result.predictions, g["predictions"]) < 1e-6
     assert rel(fields[0, 0], g["Ux"]) < 1e-6
+
+
+def test_768_thread_cta_matches_reference(rq):
+    """768-thread CTAs (the default above 1024 cells) on the small channel: the same
+    converged profile as the reference to 1e-10 (the CTA size changes only the order
+    of the block reductions)."""
+    g = np.load(GOLDEN + "small_channel_ref.npz")
+    case = cases.small_channel()
+    batch = cases.product_batch(rq, case, block_threads=768)
+    res, fields, _ = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]])
+    row = res.rows[0]
+    assert row.result.status.name == str(g["status"])
+    assert rel(row.result.predictions, g["predictions"]) < RTOL_CONV
+    assert rel(fields[0, 0], g["Ux"]) < RTOL_CONV
+
+
+def ensemble_case(re_tau, ny, max_iter):
+    """The benchmark's class (workloads.channel_batch) as a checker case."""
+    import rans_uq_b200.workloads as wl
+
+    x, y = wl.channel_probes(re_tau)
+    return ck.Case(ny=ny, re_tau=re_tau, nu=1 / re_tau, yplus=0.5, alpha_u=wl.ALPHA_U,
+                   tol=wl.TOL, max_iter=max_iter, obs_x=x, obs_y=y, obs_value=np.zeros(30),
+                   obs_sigma=np.ones(30)).with_theta(0.31, 0.09)
+
+
+@pytest.mark.parametrize("n_iter", [40, 600])
+def test_1536_cell_class_fields_after_n_iterations(rq, checker, n_iter):
+    """The benchmark's largest class (Re_tau 1000, 3 x 512 cells, 768-thread CTAs) against
+    the restatement after 40 and 600 outer iterations (past the turbulence start at 500)."""
+    import rans_uq_b200.workloads as wl
+
+    want = checker.solve(ensemble_case(1000.0, 512, n_iter), "oracle")
+    batch = wl.channel_batch(1000.0, 512, max_iter=n_iter)
+    assert batch._problem.n_cells == 1536
+    res, fields, _ = batch.evaluate_fields([[0.31, 0.09]])
+    assert res.rows[0].result.simple_iters == n_iter
+    for name in ("Ux", "k", "omega", "nuT"):
+        i = ck.FIELD_NAMES.index(name)
+        assert rel(fields[0, i], want.fields[i]) < RTOL_TRAJ, name
+
+
+def test_ensemble_classes_match_reference(rq):
+    """The benchmark's three classes at (0.31, 0.09), one multi-class launch: each
+    converges to the reference's own converged profile (the ensemble's synthetic
+    truth, written by data/make_channel_truth.py from oracle/_ref) to 1e-10, in an
+    iteration count within 2 % of the reference's (12460, 58690, 258900)."""
+    import json
+
+    import rans_uq_b200.workloads as wl
+
+    from pathlib import Path
+
+    truth = json.loads((Path(wl.__file__).parent / "data" / "channel_truth.json").read_text())
+    batches = [wl.channel_batch(re, ny) for re, ny in wl.CLASSES]
+    res = rq.evaluate_multi(batches, [0, 1, 2], np.array([[0.31, 0.09]] * 3))
+    for c, row in enumerate(res.rows):
+        want = truth[str(c)]
+        assert row.result.status.name == want["status"] == "Converged"
+        assert rel(row.result.predictions, want["profile"]) < RTOL_CONV, c
+        assert abs(row.result.simple_iters - want["iterations"]) <= 0.02 * want["iterations"], c
