@@ -137,8 +137,14 @@ def reference_arm(args):
 
 # ---------------------------------------------------------------- GPU arm
 class Clocks:
+    """nvidia-smi samples (every 200 ms) of one GPU's clocks and throttle reasons during
+    the timed region, written to a scratch file and summarised into the JSON line."""
+
     def __init__(self, index: int):
-        self.index, self.proc, self.path = index, None, ROOT / "gpurun_out" / "clocks.csv"
+        import tempfile
+
+        self.index, self.proc = index, None
+        self.path = Path(tempfile.gettempdir()) / f"rq_clocks_gpu{index}_{os.getpid()}.csv"
 
     def __enter__(self):
         self.path.parent.mkdir(exist_ok=True)
