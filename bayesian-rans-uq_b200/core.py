@@ -721,6 +721,7 @@ class ForwardModel:
                                    k_init, omega_init)
         self._cache = WarmStartCache(self._batch._problem)
         self._last = None
+        self._retain = True
 
     def cache(self) -> WarmStartCache:
         return self._cache
@@ -750,7 +751,7 @@ class ForwardModel:
                C.byref(est) if snapshot else None, C.byref(used))
         row = _rows_from_native([out], pred[None, :no], no, self._batch.n_parameters())[0]
         keep = row.result.status in (EvaluationStatus.Converged, EvaluationStatus.Unconverged)
-        self._last = fields if keep else None
+        self._last = fields if keep and self._retain else None
         snap = _snapshot(fields, bnd, flux, bool(est.value)) if snapshot and keep else None
         return ForwardEvaluationResult(row.result, row.final_worst_measure, row.contraction_rate_u,
                                        row.stalled, row.error, fields if keep else None, None,
@@ -760,13 +761,36 @@ class ForwardModel:
         r = self.evaluate(theta)
         return r.log_lik if r.status == EvaluationStatus.Converged else -1e30
 
+    def set_retain_last_fields(self, retain: bool) -> None:
+        """setRetainLastFields (ForwardModel.hpp:221-227): stop (or resume) keeping the
+        last solve's fields; stopping drops the ones kept."""
+        self._retain = bool(retain)
+        if not self._retain:
+            self._last = None
+
+    def param_set(self):
+        return self._batch.param_set
+
     def has_last_fields(self) -> bool:
         return self._last is not None
 
-    def last_fields(self) -> np.ndarray:
+    def last_fields(self) -> dict:
+        """The last solve's cell fields as the reference binding returns them
+        (extractFields, rans-uq/python/bindings.cpp:272-287): U as (n_cells, 3) and the
+        scalar fields p, k, omega, nuT, F1, F2, Pk, CDkw."""
         if self._last is None:
-            raise RuntimeError("No fields retained for the last evaluation")
-        return self._last
+            raise RuntimeError("No fields available — call evaluate() first")
+        f = self._last
+        out = {"U": np.ascontiguousarray(f[0:3].T)}
+        for i, name in enumerate(_SNAPSHOT_SCALARS):
+            out[name] = f[3 + i].copy()
+        return out
 
     def set_target_anisotropy(self, b_target):
         raise NotImplementedError("Reynolds-stress injection is outside the B200 forward-model path")
+
+    def has_target_anisotropy(self) -> bool:
+        return False
+
+    def clear_target_anisotropy(self) -> None:
+        """Nothing to clear: no target anisotropy is ever set on this path."""

@@ -131,3 +131,24 @@ def test_no_snapshot_for_invalid_parameters(rq):
     model = cases.product_batch(rq, cases.small_channel(), model_class=rq.ForwardModel)
     ev = model.evaluate_with_diagnostics((0.95, 0.09), snapshot=True)
     assert ev.result.status.name == "InvalidParameters" and ev.snapshot is None
+
+
+def test_last_fields_as_the_reference_binding_returns_them(rq):
+    """last_fields() is the binding's dict (extractFields, bindings.cpp:272-287);
+    set_retain_last_fields(False) drops and stops keeping them (ForwardModel.hpp:221-227)."""
+    case = cases.small_channel(max_iter=50)
+    model = cases.product_batch(rq, case, model_class=rq.ForwardModel)
+    ev = model.evaluate_with_diagnostics((0.31, 0.09))
+    assert ev.result.status.name == "Unconverged" and model.has_last_fields()
+    lf = model.last_fields()
+    assert set(lf) == {"U", "p", "k", "omega", "nuT", "F1", "F2", "Pk", "CDkw"}
+    assert lf["U"].shape == (case.n_cells, 3)
+    np.testing.assert_array_equal(lf["U"][:, 0], ev.fields[0])
+    np.testing.assert_array_equal(lf["omega"], ev.fields[5])
+    model.set_retain_last_fields(False)
+    assert not model.has_last_fields()
+    model.evaluate((0.31, 0.09))
+    assert not model.has_last_fields()
+    with pytest.raises(RuntimeError, match="No fields available"):
+        model.last_fields()
+    assert model.param_set() is not None and not model.has_target_anisotropy()
