@@ -55,6 +55,7 @@ class Mesh:
     y_top: float = 0.0
     re: float = 0.0
     _wall_distance: bool = False
+    _stored: dict | None = None
 
     @staticmethod
     def make_periodic_channel_2d(nx, ny, Lx, h, re_tau, yplus_target=1.0) -> "Mesh":
@@ -103,14 +104,112 @@ class Mesh:
         N.call("rq_mesh_geometry", C.byref(d), C.byref(nc), N.dptr(out))
         return out
 
-    def cell_centers(self) -> np.ndarray:
-        return self.cell_geometry()[:, :2]
-
     def save_binary(self, path) -> None:
         """Mesh::saveBinary (core/src/Mesh.cpp:751-811): the reference's MSH2 binary mesh
         file, byte-identical to the reference's for the same generator call."""
         d = self.desc()
         N.call("rq_mesh_save_binary", C.byref(d), os.fsencode(path))
+
+    # ---- introspection as the reference binding exposes it (rans-uq/python/bindings.cpp:
+    # 128-246, 556-571), read back from the mesh's own binary file so that every array is
+    # the reference's, in its face, node and patch order
+    def _mesh_record(self) -> dict:
+        if self._stored is None:
+            import tempfile
+
+            with tempfile.TemporaryDirectory() as d:
+                path = os.path.join(d, "mesh.bin")
+                self.save_binary(path)
+                with open(path, "rb") as f:
+                    self._stored = _read_mesh_binary(f.read())
+        return self._stored
+
+    def n_faces(self) -> int:
+        return len(self._mesh_record()["faces"])
+
+    def n_internal_faces(self) -> int:
+        return self._mesh_record()["n_internal"]
+
+    def n_nodes(self) -> int:
+        return len(self._mesh_record()["nodes"])
+
+    def n_patches(self) -> int:
+        return len(self._mesh_record()["patches"])
+
+    def patch_names(self) -> list:
+        return [p["name"] for p in self._mesh_record()["patches"]]
+
+    def patch_types(self) -> list:
+        return [p["type"] for p in self._mesh_record()["patches"]]
+
+    def cell_centers(self) -> np.ndarray:
+        """(n_cells, 3) cell centres (z = half the unit depth)."""
+        return self._mesh_record()["cell_centers"].copy()
+
+    def cell_volumes(self) -> np.ndarray:
+        return self._mesh_record()["cell_volumes"].copy()
+
+    def node_coords(self) -> np.ndarray:
+        return self._mesh_record()["nodes"].copy()
+
+    def face_centers(self) -> np.ndarray:
+        return np.ascontiguousarray(self._mesh_record()["faces"]["center"])
+
+    def wall_patch_data(self, name: str) -> dict:
+        """meshWallPatchData (bindings.cpp:186-233): owner, delta, centre, normal and area
+        of the named patch's faces, in patch order."""
+        rec = self._mesh_record()
+        for p in rec["patches"]:
+            if p["name"] == name:
+                f = rec["faces"][p["faces"]]
+                return {"name": p["name"], "type": p["type"], "n_faces": len(f),
+                        "owner": f["owner"].astype(np.int32), "delta": f["delta"].copy(),
+                        "center": np.ascontiguousarray(f["center"]),
+                        "normal": np.ascontiguousarray(f["normal"]),
+                        "area": f["area"].copy()}
+        raise RuntimeError(f"Mesh::wall_patch_data: unknown patch '{name}'")
+
+
+_FACE_RECORD = np.dtype([("owner", "<i4"), ("neighbor", "<i4"), ("patch", "<i4"),
+                         ("center", "<f8", 3), ("normal", "<f8", 3), ("area", "<f8"),
+                         ("delta", "<f8"), ("d", "<f8", 3), ("weight", "<f8"),
+                         ("shift", "<f8", 3)])
+
+
+def _read_mesh_binary(data: bytes) -> dict:
+    """The arrays of an MSH2 binary mesh file (Mesh::loadBinary's layout,
+    core/src/Mesh.cpp:813-905): nodes, face records, cell centres / volumes / face
+    lists, and named patches with their face indices."""
+    if np.frombuffer(data, "<u4", 1)[0] != 0x4D534832:
+        raise ValueError("not an MSH2 binary mesh")
+    nc, nf, nn, npatch, n_internal = (int(v) for v in np.frombuffer(data, "<i4", 5, 4))
+    off = 24
+    nodes = np.frombuffer(data, "<f8", 3 * nn, off).reshape(nn, 3).copy()
+    off += 24 * nn
+    faces = np.frombuffer(data, _FACE_RECORD, nf, off).copy()
+    off += _FACE_RECORD.itemsize * nf
+    centers, volumes, cell_faces = np.empty((nc, 3)), np.empty(nc), []
+    for c in range(nc):
+        rec = np.frombuffer(data, "<f8", 4, off)
+        centers[c], volumes[c] = rec[:3], rec[3]
+        k = int(np.frombuffer(data, "<i4", 1, off + 32)[0])
+        cell_faces.append(np.frombuffer(data, "<i4", k, off + 36).copy())
+        off += 36 + 4 * k
+    patches = []
+    for _ in range(npatch):
+        text = []
+        for _field in range(2):
+            k = int(np.frombuffer(data, "<i4", 1, off)[0])
+            text.append(data[off + 4:off + 4 + k].decode())
+            off += 4 + k
+        k = int(np.frombuffer(data, "<i4", 1, off)[0])
+        patches.append({"name": text[0], "type": text[1],
+                        "faces": np.frombuffer(data, "<i4", k, off + 4).copy()})
+        off += 4 + 4 * k
+    if off != len(data):
+        raise ValueError("unexpected trailing bytes in the binary mesh")
+    return {"n_internal": n_internal, "nodes": nodes, "faces": faces, "cell_centers": centers,
+            "cell_volumes": volumes, "cell_faces": cell_faces, "patches": patches}
 
 
 @dataclass
