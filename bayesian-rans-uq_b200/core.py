@@ -246,6 +246,8 @@ class SolverSettings:
     momentum_solver: str = "BiCGSTAB"
     turbulence_solver: str = "BiCGSTAB"
     use_wall_functions: bool = False
+    alpha_t: float = 0.7       # compressible solver only; kept for the settings' shape
+    von_karman: float = 0.41   # wall functions only (rejected on this path)
     sst_variant: int = 0
     # B200 path only
     precision: str = "fp64"
@@ -423,6 +425,28 @@ class ObservationOperator:
 
     def n_obs(self) -> int:
         return len(self._probes)
+
+    # The integral and feature observables of other flows (bindings.cpp: add_drag,
+    # add_skin_friction, add_reattachment_length) and the host-side evaluate(mesh,
+    # fields, nu) are not on this path: the probes are evaluated on the GPU inside
+    # each solve. They fail loudly rather than being ignored.
+    def add_drag(self, *args, **kwargs):
+        raise NotImplementedError("drag observations are outside the B200 forward-model path")
+
+    def add_skin_friction(self, *args, **kwargs):
+        raise NotImplementedError("skin-friction observations are outside the B200 "
+                                  "forward-model path")
+
+    def add_reattachment_length(self, *args, **kwargs):
+        raise NotImplementedError("reattachment-length observations are outside the B200 "
+                                  "forward-model path")
+
+    def prepare(self, mesh) -> None:
+        """Probe stencils are prepared on the host when a batch is built (nothing to do)."""
+
+    def evaluate(self, mesh, fields, nu):
+        raise NotImplementedError("predictions are evaluated on the GPU by every solve; "
+                                  "use the rows' predictions")
 
     def log_likelihood_from_predictions(self, predictions) -> float:
         """ObservationOperator::logLikelihood (ObservationOperator.hpp:592-609)."""
