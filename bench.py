@@ -257,8 +257,9 @@ def gpu_arm(args):
         t0 = time.perf_counter()
         r = b.evaluate(np.array([[0.31, 0.09]]))
         per_it.append((time.perf_counter() - t0) / max(r.rows[0].result.simple_iters, 1))
-    cpu = None
-    if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+    cpu = None  # the host baseline is timed at N = 1 only (rank 0), never beside N > 1 ranks
+    if not args.no_cpu_baseline and world == 1 and \
+            (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
         cpu = cpu_baseline(recs["iterations"], ens.cls, args.cpu_sample_iters)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if \
         (ROOT / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
