@@ -2222,6 +2222,9 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         const double *src[11] = {W.Ux, W.Uy, nullptr, W.p, W.k, W.w, W.nuT, W.F1, W.F2, W.Pk, W.CD};
         for (int b = 0; b < 11; ++b)
             FOR_CELLS(c) job.fields[(long)b * n + c] = src[b] ? src[b][c] : 0.0;
+    } else if (job.fields) { // a diverged solve leaves no valid state (ForwardModel.cpp:88-96)
+        for (long e = threadIdx.x; e < 11L * n; e += blockDim.x)
+            job.fields[e] = __longlong_as_double(0x7ff8000000000000LL);
     }
     if (job.snap && status != 2) {
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x)

@@ -262,10 +262,13 @@ int rq_evaluate_cached(rq_warm_cache *c, const double *theta, rq_row_out *row,
         if (predictions && p->nObs > 0)
             check(cudaMemcpy(predictions, p->dPred.p, sizeof(double) * p->nObs,
                              cudaMemcpyDeviceToHost), "predictions");
-        if (fields)
+        const bool solved = o.status == RQ_CONVERGED || o.status == RQ_UNCONVERGED;
+        if (fields && solved)
             check(cudaMemcpy(fields, c->staging->p, sizeof(double) * 11L * nc,
                              cudaMemcpyDeviceToHost), "fields");
-        if (wantSnap && (o.status == RQ_CONVERGED || o.status == RQ_UNCONVERGED))
+        else if (fields) // no state to report (the reference keeps no fields either)
+            std::fill(fields, fields + 11L * nc, std::numeric_limits<double>::quiet_NaN());
+        if (wantSnap && solved)
             writeSnapshot(*p, c->staging->as<double>(), c->dSnap.as<double>(), boundary,
                           face_fluxes, turb_established);
         // a Converged verdict (finite predictions and likelihood included) seeds the cache

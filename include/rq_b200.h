@@ -332,8 +332,8 @@ int rq_warm_cache_set_byte_budget(rq_warm_cache *c, uint64_t byte_budget);
    an admitted theta (n_active values, host) starts from the nearest cached state closer
    than the threshold (strictly; ties keep the older entry), else cold; a Converged solve
    is stored (replacing an entry with the same theta). row, predictions (n_obs) and the
-   optional fields (11 x n_cells) are host buffers; used_warm_start (optional) reports
-   ForwardEvaluationResult::usedWarmStart.
+   optional fields (11 x n_cells; NaN unless the row is Converged or Unconverged) are
+   host buffers; used_warm_start (optional) reports ForwardEvaluationResult::usedWarmStart.
    Snapshot (evaluateWithDiagnostics(theta, snapshot = true); OwnedFlowSnapshot,
    ForwardModel.hpp:162-186), optional, written only for a Converged or Unconverged row
    (the rows the reference snapshots). On these nx x ny periodic meshes there are

@@ -152,3 +152,28 @@ def test_last_fields_as_the_reference_binding_returns_them(rq):
     with pytest.raises(RuntimeError, match="No fields available"):
         model.last_fields()
     assert model.param_set() is not None and not model.has_target_anisotropy()
+
+
+def test_diverged_call_reports_no_state(rq):
+    """A warm start that the reference classifies Diverged leaves no valid state: the C
+    ABI's fields buffer comes back NaN (not the previous solve's state), and no snapshot
+    or last fields are kept."""
+    import ctypes as C
+
+    import rans_uq_b200._native as N
+
+    model = cases.product_batch(rq, cases.small_channel(), model_class=rq.ForwardModel)
+    assert model.evaluate((0.2, 0.05)).status.name == "Converged"
+    nc = model._batch._problem.n_cells
+    fields = np.zeros((11, nc))
+    pred = np.zeros(8)
+    row = N.RowOut()
+    used = C.c_int32()
+    theta = np.array([0.21, 0.052])
+    N.call("rq_evaluate_cached", model.cache().handle, N.dptr(theta), C.byref(row),
+           N.dptr(pred), N.dptr(fields), None, None, None, C.byref(used))
+    assert row.status == 2 and used.value == 1
+    assert np.isnan(fields).all()
+    ev = model.evaluate_with_diagnostics((0.21, 0.052), snapshot=True)
+    assert ev.result.status.name == "DivergenceDetected" and ev.snapshot is None
+    assert not model.has_last_fields()
