@@ -81,13 +81,42 @@ def resample_indices(weights, uniforms) -> np.ndarray:
     return idx
 
 
-def resample_posterior(design_ids, theta, evaluations, sample_ids, *, root_seed: int):
+@dataclass(frozen=True)
+class Sample:
+    """A drawn design point (cfdr.statistics.Sample, statistics.py:60-66)."""
+    sample_id: int
+    theta: tuple
+
+
+def _records(evaluations):
+    """(ids, theta rows, log-likelihoods, predictions) of an evaluation set with the
+    reference's record fields (EvaluationSet.records: sample_id, theta, status, error,
+    log_likelihood, predictions), every record required to be a success (_resolved,
+    statistics.py:208-214)."""
+    recs = tuple(evaluations.records)
+    if not recs:
+        raise ValueError("at least one evaluation is required")
+    failed = sum(1 for r in recs if r.status != "Converged" or r.error)
+    if failed:
+        raise ValueError(f"{failed} unresolved evaluations; posterior is undefined")
+    return ([int(r.sample_id) for r in recs], np.array([r.theta for r in recs], dtype=float),
+            np.array([r.log_likelihood for r in recs], dtype=float),
+            np.array([r.predictions for r in recs], dtype=float))
+
+
+def resample_posterior(design_ids, theta=None, evaluations=None, sample_ids=None, *,
+                       root_seed: int):
     """resample_posterior (statistics.py:235-259): IID multinomial draws from the
-    importance posterior of a design (ids, theta rows, and a ForwardBatchResult or
-    log-likelihoods in design order). Inputs are put in sample-id order, output id i
-    draws from its own "posterior-resample" stream. Returns (sample_id, theta) pairs."""
+    importance posterior of a design. Called as the reference is,
+    resample_posterior(evaluation_set, sample_ids, root_seed=...), with records carrying
+    sample_id / theta / log_likelihood; or with arrays: design ids, theta rows, and a
+    ForwardBatchResult or log-likelihoods in design order. Inputs are put in sample-id
+    order, output id i draws from its own "posterior-resample" stream. Returns Samples."""
     from .workloads import sample_rng
 
+    if hasattr(design_ids, "records"):  # the reference's call form
+        sample_ids = theta
+        design_ids, theta, evaluations, _ = _records(design_ids)
     ids = [int(i) for i in design_ids]
     out_ids = [int(i) for i in sample_ids]
     if len(set(ids)) != len(ids) or len(set(out_ids)) != len(out_ids):
@@ -102,7 +131,7 @@ def resample_posterior(design_ids, theta, evaluations, sample_ids, *, root_seed:
     w = posterior_weights(ll[order])
     u = [sample_rng(root_seed, i, "posterior-resample").random() for i in out_ids]
     picks = resample_indices(w, u)
-    return tuple((i, tuple(float(x) for x in th[k])) for i, k in zip(out_ids, picks))
+    return tuple(Sample(i, tuple(float(x) for x in th[k])) for i, k in zip(out_ids, picks))
 
 
 @dataclass(frozen=True)
@@ -133,14 +162,18 @@ def predictive_moments(latent) -> tuple[np.ndarray, np.ndarray]:
     return mean, var
 
 
-def predictive_summary(sample_ids, predictions, *, root_seed: int, observation_sigma=None,
+def predictive_summary(sample_ids, predictions=None, *, root_seed: int, observation_sigma=None,
                        surrogate_variance=None, discrepancy_variance=None) -> PredictiveSummary:
-    """predictive_summary (statistics.py:277-339) for converged evaluations given by their
-    sample ids and prediction rows: the equal-weight latent mixture's mean and variance
-    (on the GPU, canonical sample-id order) plus the specified Gaussian components, and
-    one noisy sample per evaluation from the reference's per-sample streams."""
+    """predictive_summary (statistics.py:277-339) for converged evaluations, given as the
+    reference takes them (an evaluation set whose records carry sample_id and
+    predictions) or as sample ids and prediction rows: the equal-weight latent mixture's
+    mean and variance (on the GPU, canonical sample-id order) plus the specified
+    Gaussian components, and one noisy sample per evaluation from the reference's
+    per-sample streams."""
     from .workloads import sample_rng
 
+    if hasattr(sample_ids, "records"):  # the reference's call form
+        sample_ids, _, _, predictions = _records(sample_ids)
     ids = [int(i) for i in sample_ids]
     if not ids:
         raise ValueError("at least one evaluation is required")

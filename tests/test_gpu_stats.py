@@ -68,8 +68,40 @@ def test_resample_indices_equal_numpy_choice():
 def test_resample_posterior_matches_reference(tag):
     draws = st.resample_posterior(REF[f"{tag}_ids"], REF[f"{tag}_theta"], REF[f"{tag}_ll"],
                                   REF[f"{tag}_resample_ids"], root_seed=20261010)
-    assert [d[0] for d in draws] == REF[f"{tag}_resample_ids"].tolist()
-    np.testing.assert_array_equal(np.array([d[1] for d in draws]), REF[f"{tag}_resample_theta"])
+    assert [d.sample_id for d in draws] == REF[f"{tag}_resample_ids"].tolist()
+    np.testing.assert_array_equal(np.array([d.theta for d in draws]),
+                                  REF[f"{tag}_resample_theta"])
+
+
+def _evaluation_set(tag):
+    """An object shaped as cfdr.statistics.EvaluationSet (records with sample_id, theta,
+    status, error, log_likelihood, predictions), from the fixture's ensemble."""
+    from types import SimpleNamespace
+
+    recs = [SimpleNamespace(sample_id=int(i), theta=tuple(t), status="Converged", error="",
+                            log_likelihood=float(ll), predictions=tuple(p))
+            for i, t, ll, p in zip(REF[f"{tag}_ids"], REF[f"{tag}_theta"], REF[f"{tag}_ll"],
+                                   REF[f"{tag}_pred"])]
+    return SimpleNamespace(records=tuple(recs))
+
+
+@pytest.mark.parametrize("tag", ["a", "c"])
+def test_reference_call_forms(tag):
+    """resample_posterior(evaluation_set, ids, root_seed=) and
+    predictive_summary(evaluation_set, ...) as the reference is called."""
+    ev = _evaluation_set(tag)
+    draws = st.resample_posterior(ev, REF[f"{tag}_resample_ids"], root_seed=20261010)
+    np.testing.assert_array_equal(np.array([d.theta for d in draws]),
+                                  REF[f"{tag}_resample_theta"])
+    d = REF[f"{tag}_pred"].shape[1]
+    s = st.predictive_summary(ev, root_seed=77, observation_sigma=REF[f"{tag}_sigma"],
+                              surrogate_variance=np.full(d, 0.01))
+    np.testing.assert_array_equal(np.array(s.samples), REF[f"{tag}_samples"])
+    np.testing.assert_array_equal(np.array(s.latent_variance), REF[f"{tag}_latent_variance"])
+    bad = _evaluation_set(tag)
+    bad.records[0].status = "DivergenceDetected"
+    with pytest.raises(ValueError, match="unresolved"):
+        st.resample_posterior(bad, [1], root_seed=1)
 
 
 @pytest.mark.parametrize("tag", ["a", "b", "c"])
