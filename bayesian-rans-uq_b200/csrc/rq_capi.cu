@@ -433,6 +433,31 @@ void launchRows(rq_problem &owner, const std::vector<const rq_problem *> &probOf
     cudaEventDestroy(fork);
 }
 
+// weights of n host log-likelihoods (and optional log proposal densities) on the device:
+// out = {m, sum of exp(. - m)}; the weights land in `weights` (host)
+void weightsOnDevice(const double *loglik, const double *log_q, int64_t n, double *weights,
+                     double out[2]) {
+    if (n < 1)
+        throw std::invalid_argument("at least one evaluation is required");
+    if (!loglik || !weights)
+        throw std::invalid_argument("null argument");
+    DevBuf d;
+    const size_t b = sizeof(double) * static_cast<size_t>(n);
+    d.ensure(3 * b + 4 * sizeof(double));
+    double *dl = d.as<double>(), *dq = log_q ? dl + n : nullptr, *dw = dl + 2 * n,
+           *dout = dl + 3 * n;
+    check(cudaMemcpy(dl, loglik, b, cudaMemcpyHostToDevice), "loglik");
+    if (log_q)
+        check(cudaMemcpy(dq, log_q, b, cudaMemcpyHostToDevice), "log_q");
+    check(rq::launchWeights(dl, dq, n, dw, dout, nullptr), "weights launch");
+    double o3[3];
+    check(cudaMemcpy(o3, dout, sizeof(o3), cudaMemcpyDeviceToHost), "weights");
+    if (o3[2] != 0.0)
+        throw std::invalid_argument("successful log likelihoods must be finite");
+    check(cudaMemcpy(weights, dw, b, cudaMemcpyDeviceToHost), "weights");
+    out[0] = o3[0];
+    out[1] = o3[1];
+}
 } // namespace
 
 extern "C" {
@@ -789,52 +814,22 @@ int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_
 int rq_posterior_weights(const double *loglik, const double *log_q, int64_t n, double *weights,
                          double *log_evidence) {
     return guarded([&] {
-        if (n < 1)
-            throw std::invalid_argument("at least one evaluation is required");
-        if (!loglik || !weights)
-            throw std::invalid_argument("null argument");
-        DevBuf d;
-        const size_t b = sizeof(double) * static_cast<size_t>(n);
-        d.ensure(3 * b + 4 * sizeof(double));
-        double *dl = d.as<double>(), *dq = log_q ? dl + n : nullptr, *dw = dl + 2 * n,
-               *dout = dl + 3 * n;
-        check(cudaMemcpy(dl, loglik, b, cudaMemcpyHostToDevice), "loglik");
-        if (log_q)
-            check(cudaMemcpy(dq, log_q, b, cudaMemcpyHostToDevice), "log_q");
-        check(rq::launchWeights(dl, dq, n, dw, dout, nullptr), "weights launch");
-        double out[3];
-        check(cudaMemcpy(out, dout, sizeof(out), cudaMemcpyDeviceToHost), "weights");
-        if (out[2] != 0.0)
-            throw std::invalid_argument("successful log likelihoods must be finite");
-        check(cudaMemcpy(weights, dw, b, cudaMemcpyDeviceToHost), "weights");
+        double ms[2];
+        weightsOnDevice(loglik, log_q, n, weights, ms);
         if (log_evidence)
-            *log_evidence = out[0] + std::log(out[1]);
+            *log_evidence = ms[0] + std::log(ms[1]);
     });
 }
 
 int rq_posterior_weights_parts(const double *loglik, const double *log_q, int64_t n,
                                double *weights, double *max_out, double *sum_out) {
     return guarded([&] {
-        if (n < 1)
-            throw std::invalid_argument("at least one evaluation is required");
-        if (!loglik || !weights || !max_out || !sum_out)
+        if (!max_out || !sum_out)
             throw std::invalid_argument("null argument");
-        DevBuf d;
-        const size_t b = sizeof(double) * static_cast<size_t>(n);
-        d.ensure(3 * b + 4 * sizeof(double));
-        double *dl = d.as<double>(), *dq = log_q ? dl + n : nullptr, *dw = dl + 2 * n,
-               *dout = dl + 3 * n;
-        check(cudaMemcpy(dl, loglik, b, cudaMemcpyHostToDevice), "loglik");
-        if (log_q)
-            check(cudaMemcpy(dq, log_q, b, cudaMemcpyHostToDevice), "log_q");
-        check(rq::launchWeights(dl, dq, n, dw, dout, nullptr), "weights launch");
-        double out[3];
-        check(cudaMemcpy(out, dout, sizeof(out), cudaMemcpyDeviceToHost), "weights");
-        if (out[2] != 0.0)
-            throw std::invalid_argument("successful log likelihoods must be finite");
-        check(cudaMemcpy(weights, dw, b, cudaMemcpyDeviceToHost), "weights");
-        *max_out = out[0];
-        *sum_out = out[1];
+        double ms[2];
+        weightsOnDevice(loglik, log_q, n, weights, ms);
+        *max_out = ms[0];
+        *sum_out = ms[1];
     });
 }
 
