@@ -39,6 +39,18 @@ int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
     return static_cast<int>(bytes / 8 / 32 * 32);
 }
 
+void runOneJob(rq_problem &p, const rq::DevJob &job) {
+    const int arena = chooseArena({&p});
+    p.dJobs.ensure(sizeof(rq::DevJob));
+    p.dWs.ensure(sizeof(double) * p.cls.wsDoubles);
+    p.dCounter.ensure(sizeof(int));
+    check(cudaMemcpy(p.dJobs.p, &job, sizeof(rq::DevJob), cudaMemcpyHostToDevice), "job");
+    check(cudaMemset(p.dCounter.p, 0, sizeof(int)), "counter");
+    check(rq::launchSolve(p.dJobs.as<rq::DevJob>(), 1, p.dCounter.as<int>(), p.dWs.as<double>(),
+                          p.cls.wsDoubles, 1, p.block, arena, nullptr),
+          "solve launch");
+}
+
 int chooseArena(const std::vector<const rq_problem *> &probs) {
     long ws = 0;
     int knob = 0;
@@ -722,10 +734,8 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
         if (wantHist)
             p->dHist.ensure(sizeof(double) * 11L * hist_cap);
         check(cudaMemcpy(p->dTheta.p, coeffs, sizeof(double) * 11, cudaMemcpyHostToDevice), "coeffs");
-        std::vector<const rq_problem *> probOfRow{p};
         // one job whose class descriptor is the all-eleven view
-        std::vector<rq::DevJob> jobs(1);
-        rq::DevJob &j = jobs[0];
+        rq::DevJob j{};
         j.cls = dAll.as<rq::DevClass>();
         j.theta = p->dTheta.as<double>();
         j.row = p->dRows.as<rq::RowOut>();
@@ -733,17 +743,7 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
         j.fields = fields ? p->dFields.as<double>() : nullptr;
         j.hist = wantHist ? p->dHist.as<double>() : nullptr;
         j.histCap = hist_cap;
-        j.clock = nullptr;
-        const int arena = chooseArena(probOfRow);
-        p->dJobs.ensure(sizeof(rq::DevJob));
-        p->dWs.ensure(sizeof(double) * p->cls.wsDoubles);
-        p->dCounter.ensure(sizeof(int));
-        check(cudaMemcpy(p->dJobs.p, jobs.data(), sizeof(rq::DevJob), cudaMemcpyHostToDevice), "jobs");
-        check(cudaMemset(p->dCounter.p, 0, sizeof(int)), "counter");
-        check(rq::launchSolve(p->dJobs.as<rq::DevJob>(), 1, p->dCounter.as<int>(),
-                              p->dWs.as<double>(), p->cls.wsDoubles, 1, p->block, arena,
-                              nullptr),
-              "solve launch");
+        runOneJob(*p, j);
         rq::RowOut o;
         check(cudaMemcpy(&o, p->dRows.p, sizeof(o), cudaMemcpyDeviceToHost), "row");
         *row = toRow(o);

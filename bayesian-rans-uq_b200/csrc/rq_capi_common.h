@@ -116,6 +116,10 @@ struct rq_problem {
 };
 
 namespace rqc {
+// one job on the problem's own workspace: a grid of one CTA of the class's size, the
+// arena the batch path would give the class, queued on the legacy stream and finished
+// by the time the caller copies results back (the problem's mutex held by the caller)
+void runOneJob(rq_problem &p, const rq::DevJob &job);
 int maxSmemOptin();
 // shared-memory arena (doubles) of a launch of these classes
 int arenaDoublesFor(long wsDoubles, int knobKb, int nmax);

@@ -28,7 +28,7 @@ struct rq_warm_cache {
     size_t budget = 64u << 20, retained = 0;
     std::deque<Entry> q; // front = oldest
     std::unique_ptr<DevBuf> staging;
-    DevBuf dCounter, dSnap;
+    DevBuf dSnap;
     std::mutex mu;
 
     // entryBytes (ForwardModel.hpp:39-47): theta, Vec3 over cells + boundary faces,
@@ -245,15 +245,7 @@ int rq_evaluate_cached(rq_warm_cache *c, const double *theta, rq_row_out *row,
         j.warm = hit ? hit->state->as<double>() : nullptr;
         j.warmBeta = hit ? hit->beta1 : 0.0;
         j.snap = wantSnap ? c->dSnap.as<double>() : nullptr;
-        const int arena = chooseArena({p});
-        p->dJobs.ensure(sizeof(rq::DevJob));
-        p->dWs.ensure(sizeof(double) * p->cls.wsDoubles);
-        c->dCounter.ensure(sizeof(int));
-        check(cudaMemcpy(p->dJobs.p, &j, sizeof(j), cudaMemcpyHostToDevice), "job");
-        check(cudaMemset(c->dCounter.p, 0, sizeof(int)), "counter");
-        check(rq::launchSolve(p->dJobs.as<rq::DevJob>(), 1, c->dCounter.as<int>(),
-                              p->dWs.as<double>(), p->cls.wsDoubles, 1, p->block, arena, nullptr),
-              "solve launch");
+        runOneJob(*p, j);
         rq::RowOut o;
         check(cudaMemcpy(&o, p->dRows.p, sizeof(o), cudaMemcpyDeviceToHost), "row");
         *row = toRow(o);

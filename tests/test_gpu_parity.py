@@ -191,3 +191,30 @@ def test_ensemble_classes_match_reference(rq):
         assert row.result.status.name == want["status"] == "Converged"
         assert rel(row.result.predictions, want["profile"]) < RTOL_CONV, c
         assert abs(row.result.simple_iters - want["iterations"]) <= 0.02 * want["iterations"], c
+
+
+def test_rq_solve_equals_batch_row(rq):
+    """rq_solve (all eleven coefficients, SIMPLESolver::initUniform + solve) gives the
+    same row, predictions, fields and residual history as the batch row of the same
+    coefficients: the same per-solve code on a class view whose every coefficient is
+    active."""
+    import ctypes as C
+
+    import rans_uq_b200._native as N
+
+    case = cases.small_channel(max_iter=300)
+    batch = cases.product_batch(rq, case)
+    res, fields, hist = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]], hist_cap=300)
+    coeffs = np.array(case.coeffs, dtype=float)
+    n = batch._problem.n_cells
+    row = N.RowOut()
+    pred = np.zeros(len(case.obs_x))
+    f = np.zeros((11, n))
+    h = np.zeros((300, 11))
+    N.call("rq_solve", batch._problem.handle, N.dptr(coeffs), C.byref(row), N.dptr(pred),
+           N.dptr(f), N.dptr(h), C.c_int32(300))
+    want = res.rows[0].result
+    assert row.status == int(want.status) and row.iterations == want.simple_iters == 300
+    np.testing.assert_array_equal(pred, want.predictions)
+    np.testing.assert_array_equal(f, fields[0])
+    np.testing.assert_array_equal(h, hist[0])
