@@ -61,3 +61,7 @@ def test_warm_cache_and_model_entry_points_check_arguments(rq):
     assert L.rq_warm_cache_set_byte_budget(None, 0) == -1
     assert L.rq_warm_cache_destroy(None) == 0  # deleting nothing is allowed, as delete is
     assert L.rq_mesh_save_binary(None, b"x") == -1
+
+
+def test_version_is_reported(rq):
+    assert rq.lib().rq_version() > 0
