@@ -33,9 +33,9 @@ UNIT = "solves/s"
 REF_ITERS = (12460, 58690, 258900)
 BYTES_OUTER, BYTES_KRYLOV, BYTES_PRESSURE = 1600, 360, 400  # algorithmic B/cell (FP64)
 # DRAM bytes (read + write) of one 1536-cell draw as ncu counted them over a
-# 600-iteration solve: the first touch of the mesh class and the workspace; later
-# iterations hit L2, so the figure does not grow with iterations
-DRAM_BYTES_PER_DRAW_1536 = 848_384 + 256
+# 600-iteration solve with 768-thread CTAs: the first touch of the mesh class and the
+# workspace; later iterations hit L2, so the figure does not grow with iterations
+DRAM_BYTES_PER_DRAW_1536 = 1_236_992 + 2_048
 
 
 def parse():
