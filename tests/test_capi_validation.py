@@ -65,3 +65,26 @@ def test_warm_cache_and_model_entry_points_check_arguments(rq):
 
 def test_version_is_reported(rq):
     assert rq.lib().rq_version() > 0
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the built CUDA library every call raises: there is no CPU path."""
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import rans_uq_b200._native as N\n"
+        "from pathlib import Path\n"
+        "N.LIB_PATH = Path(%r)\n"
+        "import rans_uq_b200 as rq\n"
+        "try:\n"
+        "    rq.Mesh.make_periodic_channel_2d(3, 8, 1.0, 1.0, 180.0, 1.0).cell_geometry()\n"
+        "except ImportError as e:\n"
+        "    print('raised', e)\n"
+    ) % (str(root), str(tmp_path / "absent.so"))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                         timeout=120)
+    assert "raised" in out.stdout and "no CPU fallback" in out.stdout, out.stdout + out.stderr
