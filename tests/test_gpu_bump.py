@@ -60,3 +60,16 @@ def test_bump_pcg_matches_reference(rq):
     assert res.rows[0].result.status.name == want.status
     errs = field_errors(fields[0], want)
     assert max(errs.values()) < RTOL, errs
+
+
+@pytest.mark.parametrize("solver,ps", [("AMG", ck.P_AMG), ("PCG", ck.P_PCG)])
+def test_full_size_bump_after_5_iterations(rq, checker, solver, ps):
+    """The benchmark's bump-wall mesh (200 x 100 cells; 768-thread CTAs, the default
+    above 1024 cells) against the restatement after 5 outer iterations (1e-9)."""
+    case = cases.bump_case(200, 100, max_iter=5, pressure_solver=ps)
+    want = checker.solve(case, "oracle", hist_cap=5)
+    batch = cases.product_batch(rq, case, pressure_solver=solver)
+    res, fields, _ = batch.evaluate_fields([[case.coeffs[9], case.coeffs[8]]], hist_cap=5)
+    assert res.rows[0].result.simple_iters == want.iterations == 5
+    errs = field_errors(fields[0], want)
+    assert max(errs.values()) < RTOL, errs

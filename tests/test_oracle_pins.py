@@ -159,3 +159,13 @@ def test_warm_sequence_unconverged_not_stored():
     b = ck.solve_sequence(case, th, "ref")
     _same_sequence(a, b)
     assert not a.used_warm.any() and a.retained.tolist() == [0, 0]
+
+
+@need_ref
+def test_full_size_bump_trajectory_bitwise_equal_to_reference(checker):
+    """The benchmark's bump-wall mesh (200 x 100 cells): the restatement's fields after 3
+    outer iterations with the PCG pressure solver equal the reference's bit for bit."""
+    case = cases.bump_case(200, 100, max_iter=3, pressure_solver=ck.P_PCG)
+    a = checker.solve(case, "ref")
+    b = checker.solve(case, "oracle")
+    np.testing.assert_array_equal(a.fields, b.fields)
