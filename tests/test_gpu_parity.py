@@ -218,3 +218,22 @@ def test_rq_solve_equals_batch_row(rq):
     np.testing.assert_array_equal(pred, want.predictions)
     np.testing.assert_array_equal(f, fields[0])
     np.testing.assert_array_equal(h, hist[0])
+
+
+def test_batch_edge_cases(rq):
+    """ForwardBatch::evaluate's edge cases (ForwardBatch.hpp:52-124, bindings.cpp:893-905):
+    an empty batch returns no rows; a theta of the wrong shape or a worker count below
+    one is rejected; non-finite parameters are InvalidParameters rows with the -1e30
+    sentinel and NaN predictions, as out-of-bound ones are."""
+    batch = cases.product_batch(rq, cases.small_channel(max_iter=5))
+    empty = batch.evaluate(np.zeros((0, 2)))
+    assert empty.rows == [] and empty.predictions.shape == (0, 8)
+    with pytest.raises(ValueError, match="shape"):
+        batch.evaluate(np.zeros((2, 3)))
+    with pytest.raises(ValueError, match="workers"):
+        batch.evaluate(np.array([[0.31, 0.09]]), workers=0)
+    res = batch.evaluate(np.array([[np.nan, 0.09], [0.31, np.inf], [0.31, 0.09]]))
+    for r in res.rows[:2]:
+        assert r.result.status.name == "InvalidParameters" and r.result.log_lik == -1e30
+        assert np.all(np.isnan(r.result.predictions))
+    assert res.rows[2].result.status.name == "Unconverged"
