@@ -52,7 +52,7 @@ def parse():
                          "workload's own cap is 300000)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="ensemble",
-                    choices=["ensemble", "linear", "serve", "bump", "calibrate"],
+                    choices=["ensemble", "linear", "serve", "bump", "calibrate", "plain"],
                     help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
                          "variable-coefficient Poisson systems by AMG-PCG; serve: open-loop "
                          "Poisson arrivals of channel requests to the serving loop")
@@ -691,6 +691,87 @@ def bump_arm(args):
     }))
 
 
+# ---------------------------------------------------------------- plain small case
+PLAIN_METRIC = "plain FP64 solve time, Re_tau 182 channel on 3 x 128 cells to tol 1e-10"
+
+
+def plain_cpu_seconds_per_iteration(cap: int = 20000) -> float:
+    """The reference's own ForwardModel (oracle/_ref) on the same case, capped at `cap`
+    outer iterations on one host thread (about 20 s): seconds per outer iteration."""
+    import dataclasses
+
+    from oracle import checker as ck
+
+    t = time.perf_counter()
+    out = ck.solve(dataclasses.replace(ck.config1_case(), max_iter=cap), "ref")
+    return (time.perf_counter() - t) / max(out.iterations, 1)
+
+
+def plain_arm(args):
+    """The survey's configuration 1: one cold FP64 solve at (a1, beta*) = (0.31, 0.09) on
+    the 3 x 128 channel (y+ 0.5, alpha_U 0.5, tol 1e-10, cap 150000), timed on the device
+    with theta resident, and once more through the host API (e2e)."""
+    import torch
+    import rans_uq_b200 as rq
+    import rans_uq_b200.workloads as wl
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    batch = wl.channel_batch(182.088, 128, observed=np.zeros(30), sigma=np.full(30, 1e-3),
+                             alpha_u=0.5, tol=1e-10, max_iter=150000)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    th = torch.tensor([[0.31, 0.09]], dtype=torch.float64, device=dev)
+    rows = torch.zeros(40, dtype=torch.uint8, device=dev)
+    pred = torch.zeros((1, 30), dtype=torch.float64, device=dev)
+    clock = torch.zeros((1, 12), dtype=torch.int64, device=dev)
+
+    def step():
+        rq.evaluate_multi_device([batch], np.zeros(1, np.int32), th.data_ptr(), rows.data_ptr(),
+                                 pred.data_ptr(), stream.cuda_stream, clock.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    rec = rq.rows_from_device_bytes(rows.cpu().numpy())
+    t0 = time.perf_counter()
+    host = batch.evaluate(np.array([[0.31, 0.09]]))
+    e2e_s = time.perf_counter() - t0
+    cpu = None
+    if not args.no_cpu_baseline and (ROOT / "oracle" / "_ref" / "libcfdr_ref.so").exists():
+        per = plain_cpu_seconds_per_iteration()
+        iters = int(rec["iterations"][0])
+        cpu = {"value": per * iters, "unit": "s", "cores": 1, "kind": "reference",
+               "sample": f"the reference's ForwardModel (oracle/_ref, g++ -O2) capped at 20000 "
+                         f"outer iterations: {1e3 * per:.3f} ms each x the {iters} iterations "
+                         f"of the solve (extrapolated)"}
+    print(json.dumps({
+        "metric": PLAIN_METRIC, "value": ms / 1e3, "unit": "s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "Re_tau 182.088 channel, 3 x 128 cells, y+ 0.5, alpha_U 0.5, "
+                               "tol 1e-10, (a1, beta*) = (0.31, 0.09)", "max_iter": 150000},
+        "status": int(rec["status"][0]), "iterations": int(rec["iterations"][0]),
+        "ms_per_outer_iteration": ms / max(int(rec["iterations"][0]), 1),
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16,
+                "d2h_bytes_per_step": 40 + 30 * 8},
+        "e2e_status": host.rows[0].result.status.name,
+        "gpu_launches": args.steps, "cpu_baseline": cpu,
+    }))
+
+
 # ---------------------------------------------------------------- calibration workload
 CAL_METRIC = "calibration study wall time: uniform design, pattern search, Laplace grid, 2 x 64 importance draws"
 
@@ -743,6 +824,9 @@ def main():
     args = parse()
     if args.workload == "calibrate":
         calibrate_arm(args)
+        return
+    if args.workload == "plain":
+        plain_arm(args)
         return
     if args.workload == "bump":
         bump_arm(args)
