@@ -66,3 +66,16 @@ def test_summary_when_nothing_converges():
                           [1e-4, 2e-4, 4e-4], {"hbm_gbs": 6552.3}, {}, None)
     assert out["value"] == 0.0 and out["batched_vs_plain"] is None
     assert out["roofline"]["peak_source"] == "fallback"
+
+
+def test_summary_of_two_replicas():
+    """At N = 2 the line reports the whole job: n_gpus 2, the converged solves of both
+    ranks over the max-over-ranks step time, replicas x2, and no host CPU baseline."""
+    raw, clock, cls, cells = fake_step()
+    recs = rq.rows_from_device_bytes(raw)
+    args = argparse.Namespace(steps=1, warmup=3, precision="fp64")
+    out = bench.summarize(recs, clock, cls, cells, 5.0, 22, 2, args, 300000, 3.0, 100, 200,
+                          [1e-4, 2e-4, 4e-4], {"hbm_gbs": 6552.3}, {"sm_mhz": 1900}, None)
+    assert out["n_gpus"] == 2 and out["config"]["parallelism"] == "replicas x2"
+    assert out["value"] == 22 / 5e-3 and out["cpu_baseline"] is None
+    assert out["scaling"] == "weak"
