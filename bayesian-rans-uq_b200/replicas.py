@@ -46,6 +46,32 @@ def partition_lpt(cost, world: int) -> list:
     return [np.array(sorted(p), dtype=np.int64) for p in parts]
 
 
+def reduce_max(value: float, device=None) -> float:
+    """Max of one FP64 scalar over ranks (the value itself on one process)."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64,
+                     device=device if device is not None else torch.device("cpu"))
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_count(count: int, device=None) -> int:
+    """Sum of one integer over ranks (the value itself on one process)."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return int(count)
+    t = torch.tensor([int(count)], dtype=torch.int64,
+                     device=device if device is not None else torch.device("cpu"))
+    dist.all_reduce(t)
+    return int(t.item())
+
+
 def reduce_step(ms: float, converged: int, loglik=None, device=None):
     """(max step ms over ranks, total converged, gathered logliks or None)."""
     import torch

@@ -78,6 +78,29 @@ class Ensemble:
     truth: list              # per class: noise-free synthetic profile
 
 
+def stored_truth(c: int):
+    """Noise-free probe profile of class c from data/channel_truth.json (the
+    reference solver's own converged solve at (0.31, 0.09)), or None."""
+    path = Path(__file__).parent / "data" / "channel_truth.json"
+    if not path.exists():
+        return None
+    rec = json.loads(path.read_text()).get(str(c))
+    if rec is None or rec["ny"] != CLASSES[c][1] or rec["status"] != "Converged":
+        return None
+    return np.asarray(rec["profile"], dtype=np.float64)
+
+
+def class_observation(c: int, truth=None):
+    """(observed, sigma) of class c: truth x (1 + 0.0014 eps), eps seeded per class,
+    sigma = 0.0014 |truth|. Host arithmetic only (no solve)."""
+    u = stored_truth(c) if truth is None else np.asarray(truth, dtype=np.float64)
+    if u is None:
+        raise FileNotFoundError("data/channel_truth.json holds no converged profile for "
+                                f"class {c}")
+    eps = sample_rng(SEED, c, "synthetic-observation-noise").standard_normal(len(u))
+    return u * (1 + NOISE * eps), NOISE * np.abs(u)
+
+
 def channel_ensemble(n: int = 256, precision: str = "fp64", first_id: int = 0,
                      alpha_u=ALPHA_U, max_iter=MAX_ITER) -> Ensemble:
     """The 256-draw channel ensemble: draw i -> class i mod 3. The synthetic observed
@@ -87,21 +110,15 @@ def channel_ensemble(n: int = 256, precision: str = "fp64", first_id: int = 0,
     own converged solve, written by data/make_channel_truth.py) when present, else
     from a GPU solve here."""
     batches, truth = [], []
-    stored = {}
-    path = Path(__file__).parent / "data" / "channel_truth.json"
-    if path.exists():
-        stored = json.loads(path.read_text())
     for c, (re_tau, ny) in enumerate(CLASSES):
-        rec = stored.get(str(c))
-        if rec is not None and rec["ny"] == ny and rec["status"] == "Converged":
-            u = np.asarray(rec["profile"], dtype=np.float64)
-        else:
+        u = stored_truth(c)
+        if u is None:
             probe = channel_batch(re_tau, ny, alpha_u=alpha_u, max_iter=MAX_ITER)
             res = probe.evaluate(np.array([[0.31, 0.09]]))
             u = np.asarray(res.rows[0].result.predictions)
-        eps = sample_rng(SEED, c, "synthetic-observation-noise").standard_normal(len(u))
-        batches.append(channel_batch(re_tau, ny, u * (1 + NOISE * eps), NOISE * np.abs(u),
-                                     precision=precision, alpha_u=alpha_u, max_iter=max_iter))
+        observed, sigma = class_observation(c, u)
+        batches.append(channel_batch(re_tau, ny, observed, sigma, precision=precision,
+                                     alpha_u=alpha_u, max_iter=max_iter))
         truth.append(u)
     ids = np.arange(first_id, first_id + n)
     return Ensemble(batches, uniform_design(ids), ids % 3, truth)

@@ -79,3 +79,46 @@ def test_summary_of_two_replicas():
     assert out["n_gpus"] == 2 and out["config"]["parallelism"] == "replicas x2"
     assert out["value"] == 22 / 5e-3 and out["cpu_baseline"] is None
     assert out["scaling"] == "weak"
+
+
+def test_timed_steps_fit_the_driver_run():
+    """The driver runs `--steps 20 --warmup 5` under an 1800 s limit. With a 148 s
+    ensemble step, set-up and untimed legs of 120 s, and 2 full warm-up steps, the
+    plan keeps the whole run inside the 1400 s default budget and still times at
+    least one step."""
+    elapsed = 120.0 + 2 * 148.0
+    k = bench.plan_timed_steps(20, elapsed, 148.0, 1400.0)
+    assert 1 <= k < 20
+    assert elapsed + k * 148.0 + 30.0 <= 1400.0
+    assert elapsed + (k + 1) * 148.0 + 30.0 > 1400.0
+    # a short step runs every requested step; an over-budget run still times one
+    assert bench.plan_timed_steps(20, 100.0, 1.0, 1400.0) == 20
+    assert bench.plan_timed_steps(20, 1390.0, 148.0, 1400.0) == 1
+
+
+def test_summary_reports_requested_and_timed_steps():
+    raw, clock, cls, cells = fake_step()
+    recs = rq.rows_from_device_bytes(raw)
+    args = argparse.Namespace(steps=6, steps_requested=20, warmup=5, warmup_requested=5,
+                              precision="fp64")
+    out = bench.summarize(recs, clock, cls, cells, 4.0, 11, 1, args, 300000, 1.5, 100, 200,
+                          [1e-4, 2e-4, 4e-4], {"hbm_gbs": 6552.3, "gpu_name": "x"},
+                          {"sm_mhz": 1900}, None)
+    assert out["steps"] == 6 and out["steps_requested"] == 20
+    assert out["warmup"] == 5 and out["gpu_launches"] == 3 * 6
+
+
+def test_cpu_baseline_extrapolates_each_draws_iterations():
+    """The CPU line multiplies each draw's own outer iterations by its class's
+    contended per-iteration time and divides by the cores; the measured subset's own
+    counts replace the table's for the draws it ran."""
+    cls = np.arange(6) % 3
+    sample = {"cores": 2, "per_iteration_s": [1e-3, 2e-3, 4e-3],
+              "subset": {"draws": [0], "iterations": [150], "statuses": ["Converged"],
+                         "wall_s": 0.2, "solves_per_s": 5.0},
+              "capped": {"draws": [1, 2], "iterations": 1500}}
+    iters = np.array([100, 200, 400, 100, 200, 400])
+    cb = bench.cpu_baseline(np.zeros((6, 2)), cls, iters, sample, "test")
+    total = 150 * 1e-3 + 200 * 2e-3 + 400 * 4e-3 + 100 * 1e-3 + 200 * 2e-3 + 400 * 4e-3
+    assert abs(cb["value"] - 6 / (total / 2)) < 1e-12
+    assert cb["measured_subset"]["solves_per_s"] == 5.0 and cb["cores"] == 2

@@ -41,9 +41,22 @@ def _worker(rank, world, port, q):
         conv = [85, 84][rank]
         ll = np.arange(3 + rank, dtype=np.float64) + 10 * rank
         out = rp.reduce_step(ms, conv, ll)
-        q.put((rank, out[0], out[1], out[2].tolist()))
+        # the timed-step plan: every rank must reach the same count of timed steps
+        import bench
+
+        est = rp.reduce_max([148.0, 151.0][rank])
+        elapsed = rp.reduce_max([400.0, 420.0][rank])
+        k = bench.plan_timed_steps(20, elapsed, est, 1400.0)
+        e2e = rp.reduce_count([80, 81][rank])
+        q.put((rank, out[0], out[1], out[2].tolist(), k, e2e))
     finally:
         dist.destroy_process_group()
+
+
+def bench_plan(*a):
+    import bench
+
+    return bench.plan_timed_steps(*a)
 
 
 def _free_port():
@@ -63,9 +76,10 @@ def test_reduce_step_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, ms, conv, ll in res:
+    for rank, ms, conv, ll, k, e2e in res:
         assert ms == 250.5 and conv == 169
         assert ll == [0.0, 1.0, 2.0, 10.0, 11.0, 12.0, 13.0]
+        assert k == bench_plan(20, 420.0, 151.0, 1400.0) and e2e == 161
 
 
 def _reference_weights(ll):
