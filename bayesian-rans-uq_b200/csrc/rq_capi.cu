@@ -544,6 +544,7 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
         if (base[2] == 0 || base[8] == 0)
             throw std::invalid_argument("SST beta1 and betaStar must be positive");
         auto P = std::make_unique<rq_problem>();
+        check(cudaGetDevice(&P->device), "cudaGetDevice");
         P->mesh = buildMesh(*mesh);
         P->amg = rq::buildAmg(P->mesh);
         P->active.assign(active, active + n_active);
@@ -552,12 +553,20 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
         P->block = settings->block_threads ? rq::normalizeBlock(settings->block_threads)
                                            : defaultBlock(P->mesh.n);
         upload(*P, obs, nu, *settings, init);
+        // the device address of rq_evaluate_noalloc's fixed scratch array, resolved here
+        // (this call allocates anyway) so that the allocation-free call itself only launches
+        check(rq::noAllocScratch(&P->noallocScratch), "scratch address");
         *out = P.release();
     });
 }
 
 int rq_problem_destroy(rq_problem *p) {
-    return guarded([&] { delete p; });
+    return guarded([&] {
+        if (!p)
+            return;
+        DeviceScope on(p->device);
+        delete p;
+    });
 }
 
 int rq_problem_info(const rq_problem *p, int32_t *n_cells, int32_t *n_obs, int32_t *n_active,
@@ -590,6 +599,7 @@ int rq_evaluate_multi(rq_problem *const *problems, int32_t n_problems,
         for (int i = 0; i < n_problems; ++i) {
             if (!problems[i])
                 throw std::invalid_argument("null problem");
+            requireDevice(*problems[i]);
             maxActive = std::max<int>(maxActive, static_cast<int>(problems[i]->active.size()));
             maxObs = std::max(maxObs, problems[i]->nObs);
         }
@@ -639,6 +649,7 @@ int rq_evaluate_multi_device(rq_problem *const *problems, int32_t n_problems,
         for (int i = 0; i < n_problems; ++i) {
             if (!problems[i])
                 throw std::invalid_argument("null problem");
+            requireDevice(*problems[i]);
             maxActive = std::max<int>(maxActive, static_cast<int>(problems[i]->active.size()));
             maxObs = std::max(maxObs, problems[i]->nObs);
         }
@@ -667,6 +678,7 @@ int rq_evaluate_batch(rq_problem *p, const double *theta, int64_t n, rq_row_out 
             throw std::invalid_argument("null argument");
         if (n < 0 || hist_cap < 0)
             throw std::invalid_argument("negative size");
+        requireDevice(*p);
         if (n == 0)
             return;
         std::lock_guard<std::mutex> lock(p->mu);
@@ -712,6 +724,7 @@ int rq_solve(rq_problem *p, const double coeffs[11], rq_row_out *row, double *pr
                 throw std::invalid_argument("SST coefficients must be finite and nonnegative");
         if (coeffs[2] == 0 || coeffs[8] == 0)
             throw std::invalid_argument("SST beta1 and betaStar must be positive");
+        requireDevice(*p);
         // a one-off problem view whose parameter set activates all eleven coefficients
         std::lock_guard<std::mutex> lock(p->mu);
         rq::DevClass all = p->cls;
@@ -792,6 +805,7 @@ int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_
     return guarded([&] {
         if (!p || !theta_dev || !row_dev || (p->nObs > 0 && !predictions_dev))
             throw std::invalid_argument("null argument");
+        requireDevice(*p);
         const long need = static_cast<long>(p->cls.wsDoubles);
         if (need > rq::noAllocScratchDoubles())
             throw std::invalid_argument(
@@ -806,7 +820,8 @@ int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_
         job.pred = predictions_dev;
         // shared-memory arena as the batch path sizes it for one class
         const int arena = arenaDoublesFor(need, p->arenaKb, p->mesh.n);
-        check(rq::launchSolveNoAlloc(job, p->block, arena, static_cast<cudaStream_t>(stream)),
+        check(rq::launchSolveNoAlloc(job, p->noallocScratch, p->block, arena,
+                                     static_cast<cudaStream_t>(stream)),
               "allocation-free solve launch");
     });
 }

@@ -93,6 +93,8 @@ inline long pad32(long n) { return (n + 31) / 32 * 32; }
 } // namespace rqc
 
 struct rq_problem {
+    int device = -1;         // CUDA device ordinal the class lives on (current at create)
+    double *noallocScratch = nullptr; // device address of the fixed scratch array on `device`
     rq::StructMesh mesh;
     rq::AmgHost amg;
     rq::DevClass cls{};      // host copy with device pointers
@@ -116,6 +118,31 @@ struct rq_problem {
 };
 
 namespace rqc {
+// The calling thread's current device must be the one a handle was created on: every
+// device pointer behind the handle belongs to that device.
+inline void requireDevice(int device, const char *what) {
+    int cur = -1;
+    check(cudaGetDevice(&cur), "cudaGetDevice");
+    if (cur != device)
+        throw std::invalid_argument(std::string(what) + " was created on CUDA device " +
+                                    std::to_string(device) + " but the current device is " +
+                                    std::to_string(cur) + "; call cudaSetDevice first");
+}
+inline void requireDevice(const rq_problem &p) { requireDevice(p.device, "this problem"); }
+// Makes a handle's device current for the scope (destroy paths), then restores.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        if (device >= 0 && device != prev)
+            cudaSetDevice(device);
+    }
+    ~DeviceScope() {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
 // one job on the problem's own workspace: a grid of one CTA of the class's size, the
 // arena the batch path would give the class, queued on the legacy stream and finished
 // by the time the caller copies results back (the problem's mutex held by the caller)

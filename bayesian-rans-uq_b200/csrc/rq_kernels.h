@@ -24,11 +24,13 @@ cudaError_t launchServe(const ServeQueue &q, double *ws, long wsStride, int grid
 int serveBlocksPerSM(int block, int arenaDoubles);
 int normalizeBlock(int block);
 // One solve of one job in the module's fixed scratch array (no device allocation):
-// capacity in doubles, and the launch (grid of one CTA of `block` threads). The
-// first call on a device looks the array's address up (noAllocScratch).
+// capacity in doubles, the array's device address on the current device (looked up
+// by cudaGetSymbolAddress at every call of noAllocScratch, which allocates nothing),
+// and the launch (grid of one CTA of `block` threads) on that address.
 long noAllocScratchDoubles();
 cudaError_t noAllocScratch(double **out);
-cudaError_t launchSolveNoAlloc(const DevJob &job, int block, int arenaDoubles, cudaStream_t stream);
+cudaError_t launchSolveNoAlloc(const DevJob &job, double *scratch, int block, int arenaDoubles,
+                               cudaStream_t stream);
 // Posterior weights (rq_stats.cu): one CTA; out = {max, sum of exp, non-finite count}.
 cudaError_t launchWeights(const double *ll, const double *lq, int64_t n, double *w, double *out,
                           cudaStream_t stream);

@@ -27,6 +27,7 @@ struct MappedBuf {
 // The serving loop's host half: a request queue in host-mapped memory that a
 // persistent kernel drains while the host keeps appending to it.
 struct rq_server {
+    int device = -1; // CUDA device of the server's classes, slots and launches
     std::vector<rq_problem *> problems;
     // every slot runs 512 threads whatever the classes' own CTA sizes, so a request's
     // result does not depend on which other classes the server holds (a batch of a
@@ -99,11 +100,13 @@ int rq_server_create(rq_problem *const *problems, int32_t n_problems, int32_t ca
         if (max_slots < 0)
             throw std::invalid_argument("max_slots must be nonnegative");
         auto S = std::make_unique<rq_server>();
+        check(cudaGetDevice(&S->device), "cudaGetDevice");
         std::vector<const rq_problem *> cp;
         long ws = 0;
         for (int i = 0; i < n_problems; ++i) {
             if (!problems[i])
                 throw std::invalid_argument("null problem");
+            requireDevice(*problems[i]);
             S->problems.push_back(problems[i]);
             cp.push_back(problems[i]);
             S->thetaStride = std::max<int>(S->thetaStride, static_cast<int>(problems[i]->active.size()));
@@ -168,6 +171,7 @@ int rq_server_submit(rq_server *s, int32_t problem, const double *theta, int64_t
         if (!s || !theta || !ticket)
             throw std::invalid_argument("null argument");
         std::lock_guard<std::mutex> lock(s->mu);
+        DeviceScope on(s->device); // a relaunch goes to the server's device
         if (__atomic_load_n(s->closed, __ATOMIC_ACQUIRE))
             throw std::invalid_argument("server is closed");
         if (problem < 0 || problem >= static_cast<int>(s->problems.size()))
@@ -204,6 +208,7 @@ int rq_server_poll(rq_server *s, int64_t ticket, int32_t *done, rq_row_out *row,
         if (!s || !done)
             throw std::invalid_argument("null argument");
         std::lock_guard<std::mutex> lock(s->mu);
+        DeviceScope on(s->device);
         if (ticket < 0 || ticket >= s->submitted)
             throw std::invalid_argument("unknown ticket");
         *done = __atomic_load_n(s->done + ticket, __ATOMIC_ACQUIRE) ? 1 : 0;
@@ -229,6 +234,7 @@ int rq_server_wait(rq_server *s, double timeout_s, int64_t *completed) {
         for (;;) {
             {
                 std::lock_guard<std::mutex> lock(s->mu);
+                DeviceScope on(s->device);
                 int64_t n = 0;
                 for (int i = 0; i < s->submitted; ++i)
                     n += __atomic_load_n(s->done + i, __ATOMIC_ACQUIRE) ? 1 : 0;
@@ -277,7 +283,12 @@ int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *co
 }
 
 int rq_server_destroy(rq_server *s) {
-    return guarded([&] { delete s; });
+    return guarded([&] {
+        if (!s)
+            return;
+        DeviceScope on(s->device);
+        delete s;
+    });
 }
 
 } // extern "C"

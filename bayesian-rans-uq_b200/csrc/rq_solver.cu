@@ -22,7 +22,6 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
-#include <mutex>
 
 #include <type_traits>
 
@@ -2513,44 +2512,33 @@ void *pickOne(int block) {
     default: return nullptr;
     }
 }
-constexpr int kMaxDevices = 64;
-std::mutex g_scratchMu;
-double *g_scratchAddr[kMaxDevices] = {};
 } // namespace
 
-// The device address of the scratch array on the current device, looked up once
-// per device with cudaGetSymbolAddress (the host-side name of a __device__
-// array is only a stand-in, not an address a kernel may use).
+// The device address of the scratch array on the current device. The host-side name
+// of a __device__ array is only a stand-in, not an address a kernel may use, so it is
+// looked up with cudaGetSymbolAddress (no allocation; the first lookup on a device
+// loads the module there). Callers resolve it once per handle, when the handle is
+// created, so that nothing stale survives a device reset.
 cudaError_t noAllocScratch(double **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    double *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noallocScratch);
     if (e != cudaSuccess)
         return e;
-    if (dev < 0 || dev >= kMaxDevices)
-        return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_scratchMu);
-    if (!g_scratchAddr[dev]) {
-        double *p = nullptr;
-        e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_noallocScratch);
-        if (e != cudaSuccess)
-            return e;
-        g_scratchAddr[dev] = p;
-    }
-    *out = g_scratchAddr[dev];
+    *out = p;
     return cudaSuccess;
 }
 
-cudaError_t launchSolveNoAlloc(const DevJob &job, int block, int arenaDoubles,
+cudaError_t launchSolveNoAlloc(const DevJob &job, double *scratch, int block, int arenaDoubles,
                                cudaStream_t stream) {
-    double *ws = nullptr;
-    cudaError_t e = noAllocScratch(&ws);
-    if (e != cudaSuccess)
-        return e;
+    if (!scratch)
+        return cudaErrorInvalidDevicePointer;
+    double *ws = scratch;
     void *fn = pickOne(block);
     if (!fn)
         return cudaErrorInvalidConfiguration;
     const size_t smem = solveSharedBytes() + sizeof(double) * static_cast<size_t>(arenaDoubles);
-    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
     if (e != cudaSuccess)
         return e;
     DevJob j = job;

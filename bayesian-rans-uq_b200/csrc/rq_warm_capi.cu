@@ -148,6 +148,7 @@ int rq_warm_cache_create(rq_problem *p, int32_t max_size, double threshold, uint
     return guarded([&] {
         if (!p || !out)
             throw std::invalid_argument("null argument");
+        requireDevice(*p);
         if (max_size < 0 || !std::isfinite(threshold) || threshold < 0)
             throw std::invalid_argument("Invalid warm-start cache limits");
         auto c = std::make_unique<rq_warm_cache>();
@@ -160,7 +161,12 @@ int rq_warm_cache_create(rq_problem *p, int32_t max_size, double threshold, uint
 }
 
 int rq_warm_cache_destroy(rq_warm_cache *c) {
-    return guarded([&] { delete c; });
+    return guarded([&] {
+        if (!c)
+            return;
+        DeviceScope on(c->p ? c->p->device : -1);
+        delete c;
+    });
 }
 
 int rq_warm_cache_info(rq_warm_cache *c, int32_t *size, uint64_t *retained_bytes,
@@ -208,6 +214,7 @@ int rq_evaluate_cached(rq_warm_cache *c, const double *theta, rq_row_out *row,
             throw std::invalid_argument("null argument");
         std::lock_guard<std::mutex> lock(c->mu);
         rq_problem *p = c->p;
+        requireDevice(*p);
         std::lock_guard<std::mutex> plock(p->mu);
         const int na = static_cast<int>(p->active.size());
         const int nc = p->mesh.n, no = std::max(p->nObs, 1);

@@ -146,7 +146,10 @@ int rq_default_settings(rq_settings *s);
 
 /* Builds a mesh class on the device. init = {Ux, Uy, Uz, p, k, omega} (cold start);
    active = InferenceParameterSet active indices (0..10), base = the 11 coefficients
-   that fill the inactive ones (SSTCoefficients order). */
+   that fill the inactive ones (SSTCoefficients order). The class lives on the
+   device current at this call: every later call on the problem (and on servers and
+   warm-start caches built from it) must be made with that device current, else it
+   returns RQ_E_INVALID; the destroy calls switch to it themselves. */
 int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
                       const rq_settings *settings, const rq_obs_desc *obs, const double init[6],
                       const int32_t *active, int32_t n_active, const double base[11],
@@ -232,11 +235,13 @@ int rq_linsys_destroy(rq_linsys *L);
    8 MiB array in the library (held on every GPU that loads it until exit), so
    mesh classes needing more (above about 17000 cells) are rejected with
    RQ_E_INVALID. The problem must come from rq_problem_create (which does
-   allocate). Queued on `stream` (cudaStream_t as void*) without waiting. The
-   first call on a device looks the scratch address up; make that first call
-   before any stream capture. Nothing in the scratch needs to start at zero (a
+   allocate, and which also resolves the scratch array's device address on its
+   device), so the call itself only launches. It must be made with the problem's
+   device current (RQ_E_INVALID otherwise). Queued on `stream` (cudaStream_t as
+   void*) without waiting. Nothing in the scratch needs to start at zero (a
    solve writes every array before reading it), but every call shares it:
-   calls whose solves overlap on the GPU race and corrupt each other. */
+   calls whose solves overlap on the GPU race and corrupt each other. Like every
+   handle, the problem does not survive a reset of its device. */
 int rq_evaluate_noalloc(rq_problem *p, const double *theta_dev, rq_row_out *row_dev,
                         double *predictions_dev, void *stream);
 
