@@ -70,8 +70,10 @@ def uniform_design(ids, lower, upper, root_seed):
 
 
 def pattern_search(evaluator, start, start_ll, step=SEARCH_STEP):
-    """Move a 3 x 3 stencil to its best point; halve the step when the centre wins,
-    three times. Returns (centre, final step, path of [a1, beta*, loglik])."""
+    """Compass search on the 3 x 3 grid of points one step apart around the centre:
+    the centre moves to the grid's highest log-likelihood; when the centre itself is
+    highest the step shrinks by half, up to three times. Returns (centre, final step,
+    path of [a1, beta*, loglik])."""
     center, best, step = np.asarray(start, dtype=float), float(start_ll), np.asarray(step)
     path, halvings, solves = [[*center, best]], 0, 0
     offsets = [(i, j) for i in (-1, 0, 1) for j in (-1, 0, 1) if (i, j) != (0, 0)]

@@ -7,6 +7,7 @@ Run in a checkout where the reference sources are present:
 
     python tests/golden/make_calibration_golden.py /path/to/reference
 """
+import os
 import dataclasses
 import importlib.util
 import json
@@ -18,7 +19,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RQ_REFERENCE_DIR", "/root/reference"))
 
 
 def analytic_loglik(theta):

@@ -1,8 +1,8 @@
-"""Writes channel_truth.json: the noise-free synthetic observed profile of each
+"""Writes bayesian-rans-uq_b200/data/channel_truth.json: the noise-free synthetic observed profile of each
 Re_tau class of the channel ensemble -- the reference's own FP64 ForwardModel
 solve at (a1, beta*) = (0.31, 0.09) on that class's mesh, sampled at the 30
 stations (the survey's stand-in for the Lee-Moser DNS profile, which is not
-shipped). Run where oracle/_ref is built:  python bayesian-rans-uq_b200/data/make_channel_truth.py
+shipped). Run where oracle/_ref is built:  python tests/golden/make_channel_truth.py
 """
 import json
 import multiprocessing
@@ -35,4 +35,5 @@ if __name__ == "__main__":
     with ProcessPoolExecutor(3, mp_context=multiprocessing.get_context("spawn")) as ex:
         recs = list(ex.map(run, range(3)))
     out = {str(c): r for c, r in enumerate(recs)}
-    (Path(__file__).parent / "channel_truth.json").write_text(json.dumps(out, indent=1))
+    (ROOT / "bayesian-rans-uq_b200" / "data" / "channel_truth.json").write_text(
+        json.dumps(out, indent=1))

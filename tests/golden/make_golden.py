@@ -6,6 +6,7 @@ Every number written here was computed by the compiled reference
 (oracle/_ref/libcfdr_ref.so, the reference's own ForwardModel), or read from
 the reference's committed golden JSON.
 """
+import os
 import json
 import sys
 from pathlib import Path
@@ -19,7 +20,7 @@ from oracle import checker as ck  # noqa: E402
 import cases  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
-REF = Path("/root/reference")
+REF = Path(os.environ.get("RQ_REFERENCE_DIR", "/root/reference"))
 
 
 def solve_npz(name, case, hist=0):

@@ -7,6 +7,7 @@ reference sources are present:
 
     python tests/golden/make_statistics_golden.py /path/to/reference
 """
+import os
 import importlib.util
 import sys
 import types
@@ -15,7 +16,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+REF = Path(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RQ_REFERENCE_DIR", "/root/reference"))
 
 pkg = types.ModuleType("cfdr")
 pkg.__path__ = [str(REF / "rans-uq" / "python" / "cfdr")]

@@ -6,6 +6,7 @@ reads every row's status name, predictions, log_lik, simple_iters and error, whi
 must all be this package's result types. No GPU is used: the batch's rows are built
 by the same decoding the GPU path uses (_rows_from_native over rq_row_out records),
 and posterior_weights / resample_posterior / predictive_summary then run on them."""
+import os
 import importlib.util
 import sys
 import types
@@ -18,7 +19,7 @@ import rans_uq_b200 as rq
 import rans_uq_b200._native as N
 from rans_uq_b200 import core
 
-REF = Path("/root/reference")
+REF = Path(os.environ.get("RQ_REFERENCE_DIR", "/root/reference"))
 pytestmark = pytest.mark.skipif(not (REF / "rans-uq/python/cfdr/statistics.py").exists(),
                                 reason="reference sources not present")
 
