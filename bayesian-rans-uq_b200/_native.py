@@ -60,6 +60,11 @@ class SolverResult(C.Structure):
                 ("final_res", C.c_double), ("initial_res", C.c_double)]
 
 
+class LaunchShape(C.Structure):
+    _fields_ = [("block_threads", C.c_int32), ("arena_kb", C.c_int32),
+                ("us_per_iteration", C.c_double)]
+
+
 class Ldu(C.Structure):
     _fields_ = [("n_cells", C.c_int32), ("n_faces", C.c_int32), ("diag", DP), ("upper", DP),
                 ("lower", DP), ("source", DP), ("owner", IP), ("neighbour", IP)]
@@ -75,6 +80,10 @@ SIGNATURES = {
                            C.POINTER(C.c_void_p)], C.c_int),
     "rq_problem_destroy": ([C.c_void_p], C.c_int),
     "rq_problem_info": ([C.c_void_p, IP, IP, IP, IP], C.c_int),
+    "rq_problem_tune": ([C.c_void_p, DP, C.c_int32, C.POINTER(LaunchShape), C.c_int32,
+                         C.POINTER(LaunchShape), C.POINTER(LaunchShape)], C.c_int),
+    "rq_problem_set_launch": ([C.c_void_p, C.POINTER(LaunchShape)], C.c_int),
+    "rq_problem_get_launch": ([C.c_void_p, C.POINTER(LaunchShape)], C.c_int),
     "rq_evaluate_batch": ([C.c_void_p, DP, C.c_int64, C.POINTER(RowOut), DP, DP, DP, C.c_int32],
                           C.c_int),
     "rq_evaluate_multi": ([C.POINTER(C.c_void_p), C.c_int32, IP, DP, C.c_int32, C.c_int64,

@@ -590,6 +590,43 @@ class ForwardBatch:
     def n_observations(self) -> int:
         return self.obs_op.n_obs()
 
+    def tune(self, theta=None, iters: int = 200, candidates=None):
+        """Times one solve capped at `iters` outer iterations per candidate launch shape
+        ((block_threads, arena_kb) pairs; None = the library's set), applies the fastest
+        to this mesh class (rq_problem_tune) and returns (chosen, [(block_threads,
+        arena_kb, us_per_iteration), ...]). theta defaults to the centre of the bounds."""
+        if theta is None:
+            theta = 0.5 * (np.asarray(self.param_set.lower_bounds()) +
+                           np.asarray(self.param_set.upper_bounds()))
+        theta = np.ascontiguousarray(np.asarray(theta, dtype=np.float64).ravel())
+        if theta.size != self.n_parameters():
+            raise ValueError("theta must have n_parameters values")
+        if candidates is None:
+            cand, nc = None, 0
+            meas = (N.LaunchShape * 9)()
+        else:
+            nc = len(candidates)
+            cand = (N.LaunchShape * nc)(*[N.LaunchShape(int(b), int(a), 0.0)
+                                          for b, a in candidates])
+            meas = (N.LaunchShape * nc)()
+        chosen = N.LaunchShape()
+        N.call("rq_problem_tune", self._problem.handle, N.dptr(theta), C.c_int32(iters), cand,
+               C.c_int32(nc), meas, C.byref(chosen))
+        return ((chosen.block_threads, chosen.arena_kb),
+                [(m.block_threads, m.arena_kb, m.us_per_iteration) for m in meas])
+
+    def set_launch(self, block_threads: int, arena_kb: int = -1) -> None:
+        """Applies a launch shape (rq_problem_set_launch): CTA size and shared-memory
+        arena in KiB (-1 = the default rule, 0 = none)."""
+        shape = N.LaunchShape(int(block_threads), int(arena_kb), 0.0)
+        N.call("rq_problem_set_launch", self._problem.handle, C.byref(shape))
+
+    def launch(self):
+        """The mesh class's current launch shape: (block_threads, arena_kb)."""
+        shape = N.LaunchShape()
+        N.call("rq_problem_get_launch", self._problem.handle, C.byref(shape))
+        return shape.block_threads, shape.arena_kb
+
     def evaluate(self, theta, workers: int = 1) -> ForwardBatchResult:
         if int(workers) < 1:
             raise ValueError("workers must be positive")

@@ -29,7 +29,7 @@ int arenaDoublesFor(long wsDoubles, int knobKb, int nmax) {
     const long shared = static_cast<long>(rq::solveSharedBytes());
     const long optin = maxSmemOptin();
     long bytes;
-    if (knobKb > 0)
+    if (knobKb >= 0)
         bytes = std::min<long>(knobKb * 1024L, optin - shared);
     else if (nmax <= 768)
         bytes = (optin / 2 - 1024) - shared; // half the SM (the whole hot set fits)
@@ -53,7 +53,7 @@ void runOneJob(rq_problem &p, const rq::DevJob &job) {
 
 int chooseArena(const std::vector<const rq_problem *> &probs) {
     long ws = 0;
-    int knob = 0;
+    int knob = -1;
     int nmax = 0;
     for (const auto *p : probs) {
         ws = std::max(ws, static_cast<long>(p->cls.wsDoubles));
@@ -300,25 +300,51 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
         if (l > 0 || L == 1)
             vecOff += static_cast<int>(pad32(5L * Lv.n)); // b, xa, xb, r, 1/diag
         if (l + 1 < L) {
-            addI(&dl.agg, Lv.agg);
-            addI(&dl.childPtr, Lv.childPtr);
-            addI(&dl.childIdx, Lv.childIdx);
+            // transfer operators as ELL (slot k * rows + row, -1 padding)
+            auto ell = [](const std::vector<int> &ptr, const std::vector<int> &col,
+                          const std::vector<double> &val, int rows, int &w,
+                          std::vector<int> &ec, std::vector<double> &ev) {
+                w = 0;
+                for (int r = 0; r < rows; ++r)
+                    w = std::max(w, ptr[r + 1] - ptr[r]);
+                ec.assign(static_cast<size_t>(w) * rows, -1);
+                ev.assign(static_cast<size_t>(w) * rows, 0.0);
+                for (int r = 0; r < rows; ++r)
+                    for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+                        ec[static_cast<size_t>(k - ptr[r]) * rows + r] = col[k];
+                        ev[static_cast<size_t>(k - ptr[r]) * rows + r] = val[k];
+                    }
+            };
+            const int nc = h.lev[l + 1].n;
+            std::vector<int> pc, rc;
+            std::vector<double> pv, rv;
+            ell(Lv.pPtr, Lv.pCol, Lv.pVal, Lv.n, dl.pw, pc, pv);
+            ell(Lv.rPtr, Lv.rCol, Lv.rVal, nc, dl.rw, rc, rv);
+            addI(&dl.pcol, pc);
+            addD(&dl.pval, pv);
+            addI(&dl.rcol, rc);
+            addD(&dl.rval, rv);
             // gather lists in the next level's slot order; sources of level >= 1 as slots
-            const int ns = width[l + 1] * h.lev[l + 1].n;
+            const int ns = width[l + 1] * nc;
             std::vector<int> gp(ns + 1, 0), gs;
+            std::vector<double> gw;
             for (int slot = 0; slot < ns; ++slot) {
                 const int e = entryOf[l + 1][slot];
                 if (e >= 0)
-                    for (int k = Lv.gPtr[e]; k < Lv.gPtr[e + 1]; ++k)
+                    for (int k = Lv.gPtr[e]; k < Lv.gPtr[e + 1]; ++k) {
                         gs.push_back(l == 0 ? Lv.gSrc[k] : slotOf[l][Lv.gSrc[k]]);
+                        gw.push_back(Lv.gW[k]);
+                    }
                 gp[slot + 1] = static_cast<int>(gs.size());
             }
             addI(&dl.gPtr, gp);
             addI(&dl.gSrc, gs);
+            addD(&dl.gW, gw);
         }
     }
     C.amgW = h.w;
     C.amgAlpha = h.alpha;
+    C.amgSweeps = h.sweeps;
     C.amgVals = valOff;
     C.amgVecs = vecOff;
     C.nActive = static_cast<int32_t>(P.active.size());
@@ -566,6 +592,117 @@ int rq_problem_destroy(rq_problem *p) {
             return;
         DeviceScope on(p->device);
         delete p;
+    });
+}
+
+int rq_problem_set_launch(rq_problem *p, const rq_launch_shape *shape) {
+    return guarded([&] {
+        if (!p || !shape)
+            throw std::invalid_argument("null argument");
+        requireDevice(*p);
+        if (!rq::launchVariantExists(shape->block_threads))
+            throw std::invalid_argument("block_threads must be 64, 128, 256, 512, 768 or 1024");
+        if (shape->arena_kb < -1)
+            throw std::invalid_argument("arena_kb must be -1 (default rule), 0 or positive");
+        std::lock_guard<std::mutex> lock(p->mu);
+        const int arena = arenaDoublesFor(p->cls.wsDoubles, shape->arena_kb, p->mesh.n);
+        if (rq::solveBlocksPerSM(shape->block_threads, arena) < 1)
+            throw std::invalid_argument("this launch shape does not fit on an SM");
+        p->block = shape->block_threads;
+        p->arenaKb = shape->arena_kb;
+    });
+}
+
+int rq_problem_get_launch(const rq_problem *p, rq_launch_shape *shape) {
+    return guarded([&] {
+        if (!p || !shape)
+            throw std::invalid_argument("null argument");
+        shape->block_threads = p->block;
+        shape->arena_kb = p->arenaKb;
+        shape->us_per_iteration = 0.0;
+    });
+}
+
+int rq_problem_tune(rq_problem *p, const double *theta, int32_t iters,
+                    const rq_launch_shape *candidates, int32_t n_candidates,
+                    rq_launch_shape *measured, rq_launch_shape *chosen) {
+    return guarded([&] {
+        if (!p || !theta || !chosen)
+            throw std::invalid_argument("null argument");
+        if (iters < 1)
+            throw std::invalid_argument("iters must be positive");
+        if (candidates && n_candidates < 1)
+            throw std::invalid_argument("need at least one candidate");
+        requireDevice(*p);
+        std::vector<rq_launch_shape> cand;
+        if (candidates) {
+            cand.assign(candidates, candidates + n_candidates);
+        } else {
+            const long ws = p->cls.wsDoubles;
+            const int largest = static_cast<int>(
+                std::min<long>(maxSmemOptin() - static_cast<long>(rq::solveSharedBytes()), ws * 8) /
+                1024);
+            for (int b : {256, 512, 768})
+                for (int a : {0, -1, largest})
+                    cand.push_back(rq_launch_shape{b, a, 0.0});
+        }
+        std::lock_guard<std::mutex> lock(p->mu);
+        const int na = static_cast<int>(p->active.size());
+        // the class with its outer-iteration cap set to `iters` and no convergence exit
+        rq::DevClass capped = p->cls;
+        capped.st.maxIter = iters;
+        capped.st.tol = -1.0;
+        DevBuf dCap, dTheta, dRow, dPred, dClock, dWs, dJob, dCounter;
+        dCap.ensure(sizeof(rq::DevClass));
+        dTheta.ensure(sizeof(double) * na);
+        dRow.ensure(sizeof(rq::RowOut));
+        dPred.ensure(sizeof(double) * std::max(p->nObs, 1));
+        dClock.ensure(sizeof(long long) * 12);
+        dWs.ensure(sizeof(double) * p->cls.wsDoubles);
+        dJob.ensure(sizeof(rq::DevJob));
+        dCounter.ensure(sizeof(int));
+        check(cudaMemcpy(dCap.p, &capped, sizeof(capped), cudaMemcpyHostToDevice), "class");
+        check(cudaMemcpy(dTheta.p, theta, sizeof(double) * na, cudaMemcpyHostToDevice), "theta");
+        rq::DevJob job{};
+        job.cls = dCap.as<rq::DevClass>();
+        job.theta = dTheta.as<double>();
+        job.row = dRow.as<rq::RowOut>();
+        job.pred = dPred.as<double>();
+        job.clock = dClock.as<long long>();
+        check(cudaMemcpy(dJob.p, &job, sizeof(job), cudaMemcpyHostToDevice), "job");
+        int best = -1;
+        for (size_t k = 0; k < cand.size(); ++k) {
+            rq_launch_shape &c = cand[k];
+            c.us_per_iteration = -1.0;
+            if (!rq::launchVariantExists(c.block_threads) || c.arena_kb < -1)
+                continue;
+            const int arena = arenaDoublesFor(p->cls.wsDoubles, c.arena_kb, p->mesh.n);
+            if (rq::solveBlocksPerSM(c.block_threads, arena) < 1)
+                continue;
+            check(cudaMemset(dCounter.p, 0, sizeof(int)), "counter");
+            check(rq::launchSolve(dJob.as<rq::DevJob>(), 1, dCounter.as<int>(), dWs.as<double>(),
+                                  p->cls.wsDoubles, 1, c.block_threads, arena, nullptr),
+                  "tuning launch");
+            check(cudaDeviceSynchronize(), "tuning solve");
+            long long clk[12];
+            rq::RowOut row;
+            check(cudaMemcpy(clk, dClock.p, sizeof(clk), cudaMemcpyDeviceToHost), "clock");
+            check(cudaMemcpy(&row, dRow.p, sizeof(row), cudaMemcpyDeviceToHost), "row");
+            if (row.status == 3) // InvalidParameters: theta outside the box
+                throw std::invalid_argument("tuning theta is outside the parameter bounds");
+            const int it = std::max(row.iterations, 1);
+            c.us_per_iteration = static_cast<double>(clk[1] - clk[0]) / 1e3 / it;
+            if (best < 0 || c.us_per_iteration < cand[best].us_per_iteration)
+                best = static_cast<int>(k);
+        }
+        if (measured)
+            for (size_t k = 0; k < cand.size(); ++k)
+                measured[k] = cand[k];
+        if (best < 0)
+            throw std::invalid_argument("no candidate launch shape fits on an SM");
+        p->block = cand[best].block_threads;
+        p->arenaKb = cand[best].arena_kb;
+        *chosen = cand[best];
     });
 }
 

@@ -103,7 +103,7 @@ struct rq_problem {
     double base[11];
     int32_t nObs = 0;
     int block = 512; // CTA size of this class's launches
-    int arenaKb = 0; // shared-memory arena per CTA, 0 = automatic
+    int arenaKb = -1; // shared-memory arena per CTA in KiB: -1 = the default rule, 0 = none
     cudaStream_t stream = nullptr; // for concurrent per-class launches of a multi-class batch
     cudaEvent_t done = nullptr;
     ~rq_problem() {

@@ -29,15 +29,21 @@ struct DevSettings {
 
 // Levels >= 1 are stored in ELL form: value slot k*n + i holds the k-th entry of
 // row i in column order (a warp reading slot k of 32 consecutive rows touches
-// consecutive addresses); shorter rows are padded with column -1.
+// consecutive addresses); shorter rows are padded with column -1. The transfer
+// operators between level l and level l+1 (nc rows) are ELL too: the prolongation
+// P (slot k*n + i: the k-th coarse row of fine row i and its weight) and the
+// restriction P^T (slot k*nc + I: the k-th fine row of coarse row I and its
+// weight), padded with -1.
 struct DevAmgLevel {
     int32_t n, nnz;             // rows; value slots (levels >= 1: width x n)
     int32_t valOff, vecOff;     // per-solve value / vector offsets (levels >= 1)
     int32_t width, pad;         // ELL width (levels >= 1)
+    int32_t pw, rw;             // prolongation / restriction ELL widths (all but the last level)
     const int32_t *ecol, *diagPos;       // ELL columns (-1: padding); slot of the diagonal
-    const int32_t *agg;                  // row -> next-level row
-    const int32_t *childPtr, *childIdx;  // next-level row -> rows of this level
+    const int32_t *pcol, *rcol;          // prolongation / restriction ELL columns
+    const double *pval, *rval;           // and weights
     const int32_t *gPtr, *gSrc;          // next-level value slot -> entries of this level
+    const double *gW;                    // each entry's weight P_iI P_jJ in the Galerkin sum
 };
 
 struct DevClass {
@@ -61,6 +67,7 @@ struct DevClass {
     DevAmgLevel lev[kMaxLevels];
     double amgW, amgAlpha;     // V-cycle smoother weight, coarse-correction scale
     int32_t amgVals, amgVecs;  // per-solve doubles for coarse values / vectors
+    int32_t amgSweeps, pad4;   // damped-Jacobi sweeps before and after each coarse correction
     int64_t wsDoubles;         // per-solve workspace
     // InferenceParameterSet: active indices, the coefficients filling the rest,
     // and the admission bounds (core/include/InferenceParameters.hpp:67-77, 127-165)

@@ -513,6 +513,83 @@ void rowRelativeAggregate(const Csr &A, std::vector<int> &map, int &nc) {
         map[i] = id[map[i]];
     }
 }
+// Smoothed-aggregation prolongation of one level (weight > 0), or the tentative
+// piecewise-constant one (weight 0): P = (I - omega D_F^-1 F) P_tent, where F keeps the
+// strong entries of A (|a_ij| / sqrt(a_ii a_jj) > 0.25, the aggregation's rule) and
+// lumps the weak ones into its diagonal, and omega = weight / rho(D_F^-1 F) from a
+// power iteration. Rows list their coarse columns ascending; exact zeros are dropped.
+struct Prolong {
+    std::vector<int> ptr, col;
+    std::vector<double> val;
+};
+
+Prolong smoothedProlongation(const Csr &A, const std::vector<int> &agg, int nc, double weight) {
+    const int n = A.n;
+    Prolong P;
+    P.ptr.assign(n + 1, 0);
+    std::vector<double> fd(n, 0.0); // filtered (lumped) diagonal
+    auto strongAt = [&](int i, int k) {
+        const int c = A.col[k];
+        return c != i &&
+               std::abs(A.val[k]) / std::sqrt(std::abs(A.dg[i]) * std::abs(A.dg[c]) + 1e-30) > 0.25;
+    };
+    for (int i = 0; i < n; ++i) {
+        double d = A.dg[i];
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+            if (A.col[k] != i && !strongAt(i, k))
+                d += A.val[k];
+        fd[i] = d;
+    }
+    // a row whose lumped diagonal vanishes (all its couplings weak) is not smoothed
+    auto usable = [&](int i) { return std::abs(fd[i]) > 1e-12 * std::abs(A.dg[i]); };
+    double omega = 0.0;
+    if (weight > 0.0) {
+        std::vector<double> x(n), y(n);
+        for (int i = 0; i < n; ++i)
+            x[i] = 1.0 + 0.1 * (i % 7);
+        double rho = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double ny = 0.0, nx = 0.0;
+            for (int i = 0; i < n; ++i) {
+                double s = 0.0;
+                if (usable(i)) {
+                    s = fd[i] * x[i];
+                    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                        if (strongAt(i, k))
+                            s += A.val[k] * x[A.col[k]];
+                    s /= fd[i];
+                }
+                y[i] = s;
+                ny += s * s;
+                nx += x[i] * x[i];
+            }
+            rho = std::sqrt(ny / std::max(nx, 1e-300));
+            const double inv = 1.0 / std::max(std::sqrt(ny), 1e-300);
+            for (int i = 0; i < n; ++i)
+                x[i] = y[i] * inv;
+        }
+        omega = rho > 0.0 ? weight / rho : 0.0;
+    }
+    for (int i = 0; i < n; ++i) {
+        std::map<int, double> row;
+        row[agg[i]] += 1.0;
+        if (omega > 0.0 && usable(i)) {
+            const double sc = omega / fd[i];
+            row[agg[i]] -= sc * fd[i];
+            for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                if (strongAt(i, k))
+                    row[agg[A.col[k]]] -= sc * A.val[k];
+        }
+        for (auto &e : row)
+            if (e.second != 0.0) {
+                P.col.push_back(e.first);
+                P.val.push_back(e.second);
+            }
+        P.ptr[i + 1] = static_cast<int>(P.col.size());
+    }
+    (void)nc;
+    return P;
+}
 } // namespace
 
 AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
@@ -579,11 +656,26 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
             rowRelativeAggregate(F, map, nc);
         if (nc == 0 || nc >= F.n)
             break;
-        // coarse pattern and Galerkin values
+        // prolongation: smoothed aggregation on the reference-rule hierarchy (the
+        // tentative piecewise-constant P smoothed by one damped Jacobi step of the
+        // filtered geometric matrix), the tentative P itself on the fallback
+        const Prolong P = attempt == 0 ? smoothedProlongation(F, map, nc, kProlongWeight)
+                                       : smoothedProlongation(F, map, nc, 0.0);
+        // coarse pattern and values P^T A P, and per coarse entry the weighted fine
+        // entries it sums, both in one fixed order: fine rows ascending, each row's
+        // entries in column order, then P's entries of the row and of the column
         std::vector<std::map<int, double>> rows(nc);
+        std::vector<std::map<int, std::vector<std::pair<int, double>>>> terms(nc);
         for (int i = 0; i < F.n; ++i)
-            for (int k = F.ptr[i]; k < F.ptr[i + 1]; ++k)
-                rows[map[i]][map[F.col[k]]] += F.val[k];
+            for (int k = F.ptr[i]; k < F.ptr[i + 1]; ++k) {
+                const int j = F.col[k];
+                for (int a = P.ptr[i]; a < P.ptr[i + 1]; ++a)
+                    for (int b = P.ptr[j]; b < P.ptr[j + 1]; ++b) {
+                        const double w = P.val[a] * P.val[b];
+                        rows[P.col[a]][P.col[b]] += w * F.val[k];
+                        terms[P.col[a]][P.col[b]].push_back({l == 0 ? slot[k] : k, w});
+                    }
+            }
         Csr Cm;
         Cm.n = nc;
         Cm.ptr.assign(nc + 1, 0);
@@ -606,33 +698,38 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
             for (int i = 0; i < F.n; ++i)
                 L.diagPos[i] = F.find(i, i);
         }
-        L.agg = map;
-        // restriction lists (children ascending)
-        L.childPtr.assign(nc + 1, 0);
-        for (int i = 0; i < F.n; ++i)
-            ++L.childPtr[map[i] + 1];
+        L.pPtr = P.ptr;
+        L.pCol = P.col;
+        L.pVal = P.val;
+        // restriction R = P^T: coarse row -> (fine row, weight), fine rows ascending
+        L.rPtr.assign(nc + 1, 0);
+        for (int c : P.col)
+            ++L.rPtr[c + 1];
         for (int I = 0; I < nc; ++I)
-            L.childPtr[I + 1] += L.childPtr[I];
-        L.childIdx.resize(F.n);
+            L.rPtr[I + 1] += L.rPtr[I];
+        L.rCol.resize(P.col.size());
+        L.rVal.resize(P.col.size());
         {
-            std::vector<int> fill(L.childPtr.begin(), L.childPtr.end() - 1);
+            std::vector<int> fill(L.rPtr.begin(), L.rPtr.end() - 1);
             for (int i = 0; i < F.n; ++i)
-                L.childIdx[fill[map[i]]++] = i;
+                for (int a = P.ptr[i]; a < P.ptr[i + 1]; ++a) {
+                    const int t = fill[P.col[a]]++;
+                    L.rCol[t] = i;
+                    L.rVal[t] = P.val[a];
+                }
         }
-        // Galerkin gather lists in fine CSR order (fine entry id: level 0 -> slot, else nnz)
+        // gather lists in the coarse CSR order (fine entry id: level 0 -> slot, else nnz)
         const int cnnz = static_cast<int>(Cm.col.size());
-        std::vector<std::vector<int>> src(cnnz);
-        for (int i = 0; i < F.n; ++i)
-            for (int k = F.ptr[i]; k < F.ptr[i + 1]; ++k) {
-                const int e = Cm.find(map[i], map[F.col[k]]);
-                src[e].push_back(l == 0 ? slot[k] : k);
-            }
         L.gPtr.assign(cnnz + 1, 0);
-        for (int e = 0; e < cnnz; ++e) {
-            L.gPtr[e + 1] = L.gPtr[e] + static_cast<int>(src[e].size());
-            for (int s : src[e])
-                L.gSrc.push_back(s);
-        }
+        for (int I = 0, e = 0; I < nc; ++I)
+            for (auto &t : terms[I]) {
+                for (auto &sw : t.second) {
+                    L.gSrc.push_back(sw.first);
+                    L.gW.push_back(sw.second);
+                }
+                L.gPtr[e + 1] = static_cast<int>(L.gSrc.size());
+                ++e;
+            }
         h.lev.push_back(std::move(L));
         mats.push_back(std::move(Cm));
     }
@@ -651,6 +748,7 @@ AmgHost buildAmg(const StructMesh &m, int minCoarse, int maxLevels) {
     if (attempt == 1) {
         h.w = 0.75;
         h.alpha = 1.7;
+        h.sweeps = 2;
     }
     if (h.coarseN() <= minCoarse)
         break;

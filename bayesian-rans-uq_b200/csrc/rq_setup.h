@@ -51,23 +51,32 @@ void preparePlanarBalance(StructMesh &m);
 // structured 5-point matrix (entry slot*n + cell, slots: 0 diag, 1 W, 2 E,
 // 3 S, 4 N); coarser levels are CSR. Aggregation is the reference's greedy
 // strength-0.25 rule (core/include/LinearSolver.hpp:535-575) applied to the
-// geometric Laplacian area/delta with the cell-0 pin; coarse values are
-// Galerkin sums (:578-618) gathered in fine CSR order.
+// geometric Laplacian area/delta with the cell-0 pin. On that hierarchy the
+// prolongation is smoothed (smoothed aggregation: one damped-Jacobi step of the
+// strength-filtered geometric matrix applied to the piecewise-constant
+// prolongation); on the row-relative fallback it stays piecewise constant. Coarse
+// values are the Galerkin products P^T A P of the current matrix, gathered per
+// coarse entry as weighted fine entries in one fixed order.
 struct AmgHost {
     struct Level {
         int n = 0;
         std::vector<int> ptr, col;            // CSR (levels >= 1)
         std::vector<int> diagPos;             // CSR position of (i,i)
-        std::vector<int> agg;                 // row -> coarse row (all but the last level)
-        std::vector<int> childPtr, childIdx;  // coarse row -> fine rows, ascending
-        std::vector<int> gPtr, gSrc;          // coarse nnz -> fine entries summed into it
+        std::vector<int> pPtr, pCol;          // prolongation: row -> coarse rows (all but
+        std::vector<double> pVal;             //   the last level), columns ascending
+        std::vector<int> rPtr, rCol;          // restriction P^T: coarse row -> fine rows,
+        std::vector<double> rVal;             //   ascending
+        std::vector<int> gPtr, gSrc;          // coarse nnz -> fine entries summed into it,
+        std::vector<double> gW;               //   each times its weight P_iI P_jJ
     };
     std::vector<Level> lev;
-    // V-cycle smoother weight and coarse-correction scale: 0.6 and 1 on the
-    // reference-rule hierarchy; 0.75 and 1.7 on the row-relative fallback, whose
-    // piecewise-constant prolongation under-corrects (bump-wall meshes: 29 -> 16
-    // PCG iterations per outer iteration on 200 x 100 cells)
+    // V-cycle smoother weight, coarse-correction scale and damped-Jacobi sweeps
+    // before and after the coarse correction: 0.6, 1 and 1 on the smoothed-aggregation
+    // hierarchy; 0.75, 1.7 and 2 on the row-relative fallback, whose piecewise-constant
+    // prolongation under-corrects (bump-wall meshes: 29 -> 16 PCG iterations per outer
+    // iteration on 200 x 100 cells)
     double w = 0.6, alpha = 1.0;
+    int sweeps = 1;
     int coarseN() const { return lev.back().n; }
     size_t coarseNnz() const { return lev.size() > 1 ? lev.back().col.size() : 0; }
 };
@@ -75,6 +84,10 @@ struct AmgHost {
 // up to 64 rows costs less per V-cycle than the two levels below it (measured 7 %
 // per outer iteration at 768 and 1536 cells).
 AmgHost buildAmg(const StructMesh &m, int minCoarse = 64, int maxLevels = 20);
+// Smoothing weight of the prolongation, as a fraction of 1 / rho(D_F^-1 F): 0.85
+// (PCG on pressure systems taken from Re_tau 182-1000 channel solves needs 2-4
+// iterations with it; 1.15 and above lose the coarse correction).
+constexpr double kProlongWeight = 0.85;
 
 // Velocity/pressure probe (PreparedObservation, core/include/ObservationOperator.hpp:630-670).
 struct ProbeHost {

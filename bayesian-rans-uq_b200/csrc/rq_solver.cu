@@ -261,6 +261,7 @@ struct LinRes {
     int iterations;
     double finalRes, initialRes;
     bool converged;
+    bool breakdown = false; // stopped on the |p.Ap| < 1e-30 guard (a round-off right-hand side)
 };
 
 #define FOR_CELLS(c) for (int c = threadIdx.x; c < n; c += blockDim.x)
@@ -422,9 +423,11 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
         // one aggregate), so they are always formed from the FP64 finest matrix
         for (int e = threadIdx.x; e < Q.nnz; e += blockDim.x) {
             double s = 0.0;
-            for (int k = __ldg(F.gPtr + e); k < __ldg(F.gPtr + e + 1); ++k)
-                s += (l == 0) ? level0EntryT(S.K64, C.n, __ldg(F.gSrc + k))
-                              : double(fv[__ldg(F.gSrc + k)]);
+            for (int k = __ldg(F.gPtr + e); k < __ldg(F.gPtr + e + 1); ++k) {
+                const double v = (l == 0) ? level0EntryT(S.K64, C.n, __ldg(F.gSrc + k))
+                                          : double(fv[__ldg(F.gSrc + k)]);
+                s += __ldg(F.gW + k) * v;
+            }
             cv[e] = T(s);
         }
         __syncthreads();
@@ -534,29 +537,69 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
     }
 }
 
-// row i of an ELL level times x, entries in column order
-template <typename T>
-__device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
+// Sum over the slots of one ELL row, k ascending, of coef(k) * vec(col(k)) for columns
+// >= 0. The loads of four slots are issued before their products are added (padding
+// slots load entry 0 and add nothing), so a wide row costs a few load latencies, not
+// one per slot; the order of the additions is the slots' order.
+template <typename T, typename C, typename V>
+__device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V *vec, int width,
+                                    int stride, int row) {
     T s = T(0);
-    for (int k = 0; k < L.width; ++k) {
-        const int c = __ldg(L.ecol + k * L.n + i);
+    int k = 0;
+    for (; k + 4 <= width; k += 4) {
+        int c[4];
+        T v[4], x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            c[u] = __ldg(cols + (k + u) * stride + row);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v[u] = T(coef[(k + u) * stride + row]);
+            x[u] = T(vec[c[u] < 0 ? 0 : c[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            if (c[u] >= 0)
+                s += v[u] * x[u];
+    }
+    if (k + 2 <= width) {
+        const int c0 = __ldg(cols + k * stride + row), c1 = __ldg(cols + (k + 1) * stride + row);
+        const T v0 = T(coef[k * stride + row]), v1 = T(coef[(k + 1) * stride + row]);
+        const T x0 = T(vec[c0 < 0 ? 0 : c0]), x1 = T(vec[c1 < 0 ? 0 : c1]);
+        if (c0 >= 0)
+            s += v0 * x0;
+        if (c1 >= 0)
+            s += v1 * x1;
+        k += 2;
+    }
+    if (k < width) {
+        const int c = __ldg(cols + k * stride + row);
         if (c >= 0)
-            s += val[k * L.n + i] * x[c];
+            s += T(coef[k * stride + row]) * T(vec[c]);
     }
     return s;
 }
 
-// z = M^-1 b at level 0 (b = K.r, z -> K.z): pre-smoothing from zero (two damped
-// Jacobi sweeps), aggregate-sum restriction fused into the next level's first
-// sweep, dense coarsest solve, aggregate-broadcast prolongation fused into the
-// first of two post sweeps (symmetric). Returns (r, z), reduced in the last phase.
-// (Running the small coarse levels in one warp with warp barriers measured 15 %
-// slower per outer iteration: one warp exposes the latency of its dependent loads
-// that a CTA's many warps hide.)
+// row i of an ELL level times x, entries in column order
+template <typename T>
+__device__ __forceinline__ T csrRowT(const DevAmgLevel &L, const T *val, const T *x, int i) {
+    return ellDot<T>(L.ecol, val, x, L.width, L.n, i);
+}
+
+// z = M^-1 b at level 0 (b = K.r, z -> K.z): on every level above the coarsest,
+// C.amgSweeps damped-Jacobi sweeps from zero, the residual, restriction by P^T (fused
+// into the next level's first sweep), and after the coarse correction x + alpha P x_c
+// (fused into the first post sweep) the same number of sweeps again (symmetric);
+// a dense inverse on the coarsest level. Returns (r, z), reduced in the last phase.
+// With one sweep a level costs three barrier-separated phases (two down, one up);
+// with two, five. (Running the small coarse levels in one warp with warp barriers
+// measured 15 % slower per outer iteration: one warp exposes the latency of its
+// dependent loads that a CTA's many warps hide.)
 template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp, const KW<T> &K) {
     const DevClass &C = S.C;
     const Work &W = S.W;
     const int L = C.nlev, n0 = C.n, nx = C.nx;
+    const bool two = C.amgSweeps >= 2;
     const T om = T(C.amgW), al = T(C.amgAlpha);
     const Mat<T> M = matOf(K);
     T *const Krd = K.rd, *const Kr = K.r, *const Kz = K.z, *const Kxa = K.xa, *const Kxb = K.xb,
@@ -564,7 +607,20 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     auto vb = [&](int l) { return amgVec + C.lev[l].vecOff; }; // b, xa, xb, r, 1/diag
     auto sync = [] { __syncthreads(); };
     const int t0 = threadIdx.x, ts = blockDim.x;
-    // one level of the down sweep
+    // residual of level l-1 restricted to row I of level l: sum_k R_Ik r_k
+    auto restrictRow = [&](int l, int I) {
+        const DevAmgLevel &F = C.lev[l - 1];
+        const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
+        return ellDot<T>(F.rcol, F.rval, fr, F.rw, C.lev[l].n, I);
+    };
+    // the prolongated coarse correction at row i of level l: sum_k P_ik x_c
+    auto prolong = [&](int l, int i) {
+        const DevAmgLevel &Lv = C.lev[l];
+        const T *xc = vb(l + 1) + 2 * C.lev[l + 1].n;
+        return ellDot<T>(Lv.pcol, Lv.pval, xc, Lv.pw, Lv.n, i);
+    };
+    // one level of the down sweep; the pre-smoothed iterate ends in xa (one sweep) or
+    // xb (two sweeps), the residual in rr
     auto down = [&](int l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
@@ -586,31 +642,31 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             if (l == 0) {
                 bi = b[i];
             } else {
-                const DevAmgLevel &F = C.lev[l - 1];
-                const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
-                bi = T(0);
-                for (int k = __ldg(F.childPtr + i); k < __ldg(F.childPtr + i + 1); ++k)
-                    bi += fr[__ldg(F.childIdx + k)];
+                bi = restrictRow(l, i);
                 b[i] = bi;
             }
             const T ri = (l == 0) ? Krd[i] : b[4 * n + i];
             xa[i] = om * bi * ri;
         }
         sync();
-        for (int i = t0; i < n; i += ts) {
-            T ax, ri;
-            if (l == 0) {
-                ax = rowDotT(cellOf(C, i), M, xa, nx);
-                ri = Krd[i];
-            } else {
-                ax = csrRowT(Lv, val, xa, i);
-                ri = b[4 * n + i];
+        const T *xs = xa;
+        if (two) {
+            for (int i = t0; i < n; i += ts) {
+                T ax, ri;
+                if (l == 0) {
+                    ax = rowDotT(cellOf(C, i), M, xa, nx);
+                    ri = Krd[i];
+                } else {
+                    ax = csrRowT(Lv, val, xa, i);
+                    ri = b[4 * n + i];
+                }
+                xb[i] = xa[i] + om * (b[i] - ax) * ri;
             }
-            xb[i] = xa[i] + om * (b[i] - ax) * ri;
+            sync();
+            xs = xb;
         }
-        sync();
         for (int i = t0; i < n; i += ts) {
-            const T ax = (l == 0) ? rowDotT(cellOf(C, i), M, xb, nx) : csrRowT(Lv, val, xb, i);
+            const T ax = (l == 0) ? rowDotT(cellOf(C, i), M, xs, nx) : csrRowT(Lv, val, xs, i);
             rr[i] = b[i] - ax;
         }
         sync();
@@ -624,14 +680,8 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             for (int i = t0; i < m; i += ts)
                 b[i] = Kr[i];
         } else {
-            const DevAmgLevel &F = C.lev[l - 1];
-            const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
-            for (int i = t0; i < m; i += ts) {
-                T bi = T(0);
-                for (int k = __ldg(F.childPtr + i); k < __ldg(F.childPtr + i + 1); ++k)
-                    bi += fr[__ldg(F.childIdx + k)];
-                b[i] = bi;
-            }
+            for (int i = t0; i < m; i += ts)
+                b[i] = restrictRow(l, i);
         }
         sync();
         // the coarsest solve stays FP64 in both forms: the coarsest level of the
@@ -646,28 +696,43 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         }
         sync();
     };
-    // one level of the up sweep (levels >= 1; level 0 ends in the reduction below)
+    // one level of the up sweep (levels >= 1; level 0 ends in the reduction below):
+    // x = x_pre + alpha P x_c, then the post sweeps; the result ends in xb. With a
+    // piecewise-constant P (one coarse row per fine row) x is formed inside the first
+    // sweep; with a smoothed P it is formed in a phase of its own (into the level's
+    // residual slot, free by then), so that the sweep over a wide coarse row loads
+    // each neighbour's x once instead of re-forming it from P.
     auto up = [&](int l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
-        const T *xc = vb(l + 1) + 2 * C.lev[l + 1].n;
-        T *b = vb(l), *xa = b + n, *xb = b + 2 * n;
+        T *b = vb(l), *xa = b + n, *xb = b + 2 * n, *xi = b + 3 * n;
+        const T *xpre = two ? xb : xa;
+        T *out = two ? xa : xb;
         const T *val = amgVal + Lv.valOff;
-        const int *agg = Lv.agg;
-        for (int i = t0; i < n; i += ts) {
-            const T xi = xb[i] + al * xc[__ldg(agg + i)];
-            T ax = T(0);
-            for (int k = 0; k < Lv.width; ++k) {
-                const int jj = __ldg(Lv.ecol + k * n + i);
-                if (jj >= 0)
-                    ax += val[k * n + i] * (xb[jj] + al * xc[__ldg(agg + jj)]);
+        if (Lv.pw > 1) {
+            for (int i = t0; i < n; i += ts)
+                xi[i] = xpre[i] + al * prolong(l, i);
+            sync();
+            for (int i = t0; i < n; i += ts)
+                out[i] = xi[i] + om * (b[i] - csrRowT(Lv, val, xi, i)) * b[4 * n + i];
+        } else {
+            for (int i = t0; i < n; i += ts) {
+                const T x0 = xpre[i] + al * prolong(l, i);
+                T ax = T(0);
+                for (int k = 0; k < Lv.width; ++k) {
+                    const int jj = __ldg(Lv.ecol + k * n + i);
+                    if (jj >= 0)
+                        ax += val[k * n + i] * (xpre[jj] + al * prolong(l, jj));
+                }
+                out[i] = x0 + om * (b[i] - ax) * b[4 * n + i];
             }
-            xa[i] = xi + om * (b[i] - ax) * b[4 * n + i];
         }
         sync();
-        for (int i = t0; i < n; i += ts)
-            xb[i] = xa[i] + om * (b[i] - csrRowT(Lv, val, xa, i)) * b[4 * n + i];
-        sync();
+        if (two) {
+            for (int i = t0; i < n; i += ts)
+                xb[i] = xa[i] + om * (b[i] - csrRowT(Lv, val, xa, i)) * b[4 * n + i];
+            sync();
+        }
     };
     for (int l = 0; l + 1 < L; ++l)
         down(l);
@@ -676,32 +741,35 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         up(l);
     const int tid = t0, nt = ts;
     double rz = 0.0;
-    if (L > 1) { // level 0: prolongation fused into the first post sweep, then the second
-        const DevAmgLevel &Lv = C.lev[0];
-        const int n = Lv.n;
-        const T *xc = vb(1) + 2 * C.lev[1].n;
-        const int *agg = Lv.agg;
-        const T *xprev = Kxb;
+    if (L > 1) { // level 0: prolongation fused into the first post sweep (then the second)
+        const int n = C.lev[0].n;
+        const T *xprev = two ? Kxb : Kxa;
+        T *out = two ? Kxa : Kz;
+        double part = 0.0;
         for (int i = tid; i < n; i += nt) {
-            const T xi = xprev[i] + al * xc[__ldg(agg + i)];
+            const T xi = xprev[i] + al * prolong(0, i);
             const Cell q = cellOf(C, i);
             const int c = i;
-            auto X = [&](int jj) { return xprev[jj] + al * xc[__ldg(agg + jj)]; };
+            auto X = [&](int jj) { return xprev[jj] + al * prolong(0, jj); };
             const T tW = M.aW[c] * X(q.W), tE = M.aE[c] * X(q.E);
             const T tS = q.south ? M.aS[c] * X(c - nx) : T(0);
             const T tN = q.north ? M.aN[c] * X(c + nx) : T(0);
             const T x1 = q.xEfirst ? tE : tW, x2 = q.xEfirst ? tW : tE;
             const T y1 = q.yNfirst ? tN : tS, y2 = q.yNfirst ? tS : tN;
             const T ax = (((M.d[c] * xi + x1) + x2) + y1) + y2;
-            Kxa[i] = xi + om * (Kr[i] - ax) * Krd[c];
+            const T zi = xi + om * (Kr[i] - ax) * Krd[c];
+            out[i] = zi;
+            if (!two)
+                part += double(Kr[i]) * double(zi);
         }
-        __syncthreads();
-        double part = 0.0;
-        for (int i = tid; i < n; i += nt) {
-            const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
-            const T zi = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
-            Kz[i] = zi;
-            part += double(Kr[i]) * double(zi);
+        if (two) {
+            __syncthreads();
+            for (int i = tid; i < n; i += nt) {
+                const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
+                const T zi = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
+                Kz[i] = zi;
+                part += double(Kr[i]) * double(zi);
+            }
         }
         double a[1] = {part};
         blockSum<1>(a, S, rp);
@@ -805,8 +873,10 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
         }
         blockSum<1>(a1, S, rp);
         const double pAp = a1[0];
-        if (fabs(pAp) < 1e-30)
+        if (fabs(pAp) < 1e-30) {
+            res.breakdown = true;
             break;
+        }
         const double alpha = rz / pAp;
         double a2[1] = {0.0};
         FOR_CELLS(c) {
@@ -918,11 +988,14 @@ __device__ __forceinline__ LinRes solveBicg(Shared &S, int &rp, double *x, doubl
     return bicgstabT<double>(S, rp, S.K64, x, r0n, maxIter, tol);
 }
 
-// The AMG coarse values (Galerkin sums and the coarsest inverse) are refreshed
-// when the previous pressure solve degraded -- more than 1.5x (+2) the PCG
-// iterations of the solve right after the last refresh, or not converged --
-// the rule AMGSolver applies to its aggregation (LinearSolver.hpp:924-941). The
-// stale coarse operator stays SPD, so PCG remains valid; the finest level
+// The AMG coarse values (Galerkin products and the coarsest inverse) are refreshed
+// when the previous pressure solve degraded: more than 1.5x (+2) the PCG iterations
+// of the solve right after the last refresh, or stopped short of its tolerance
+// other than on the |p.Ap| < 1e-30 guard. That is the rule AMGSolver applies to its
+// aggregation (LinearSolver.hpp:924-941), except that a guard exit does not count:
+// late in a solve the p' right-hand side is round-off (|b| ~ 1e-15), PCG stops on the
+// guard whatever the preconditioner, and fresh coarse values would not change that.
+// The stale coarse operator stays SPD, so PCG remains valid; the finest level
 // always uses the current matrix.
 __device__ __forceinline__ LinRes solvePressure(Shared &S, int &rp, double *x, double r0n,
                                                 int maxIter, double tol, int kind,
@@ -944,7 +1017,8 @@ __device__ __forceinline__ LinRes solvePressure(Shared &S, int &rp, double *x, d
             itersAfterRefresh = res.iterations;
         } else if (itersAfterRefresh <= 0) {
             itersAfterRefresh = res.iterations;
-        } else if (!res.converged || res.iterations > 1.5 * itersAfterRefresh + 2) {
+        } else if ((!res.converged && !res.breakdown) ||
+                   res.iterations > 1.5 * itersAfterRefresh + 2) {
             needRefresh = 1;
         }
     }

@@ -94,7 +94,8 @@ typedef struct rq_settings {
     int32_t nut_floor_iters;     /* 500     */
     int32_t pressure_solver;     /* RQ_SOLVER_AMG */
     int32_t precision;           /* RQ_PREC_FP64 */
-    int32_t block_threads;       /* 0 = autotuned CTA size */
+    int32_t block_threads;       /* 0 = the class's launch shape (default rule, or what
+                                    rq_problem_tune / rq_problem_set_launch chose) */
     double convergence_tol;      /* 1e-5    */
     double inner_tolerance;      /* 1e-3    */
     double divergence_limit;     /* 1e6     */
@@ -157,6 +158,31 @@ int rq_problem_create(const rq_mesh_desc *mesh, const rq_bc_desc *bc, double nu,
 int rq_problem_destroy(rq_problem *p);
 int rq_problem_info(const rq_problem *p, int32_t *n_cells, int32_t *n_obs, int32_t *n_active,
                     int32_t *amg_levels);
+
+/* Launch shape of a mesh class: the CTA size of its solves and the shared-memory
+   arena each CTA places the solve's hottest arrays in. */
+typedef struct rq_launch_shape {
+    int32_t block_threads;   /* 64, 128, 256, 512, 768 or 1024 */
+    int32_t arena_kb;        /* arena per CTA in KiB; 0 = none; -1 = the default rule (half
+                                the SM's shared memory up to 768 cells, none above) */
+    double us_per_iteration; /* measured by rq_problem_tune; 0 when not measured */
+} rq_launch_shape;
+
+/* Autotuner of the launch shape per mesh class (no reference counterpart). For every
+   candidate (NULL = the built-in set: 256, 512, 768 threads x arena none / default /
+   largest that fits) it times one solve at theta (n_active values, host) capped at
+   `iters` outer iterations with the GPU's own timer, writes the measured time per
+   outer iteration into measured[k] (NULL allowed; candidates that do not fit on an SM
+   get a negative time), applies the fastest to the problem and returns it in *chosen.
+   Results do not depend on the arena; the CTA size changes only the order of the
+   block sums (agreement to rounding). Blocks until the timings are in. */
+int rq_problem_tune(rq_problem *p, const double *theta, int32_t iters,
+                    const rq_launch_shape *candidates, int32_t n_candidates,
+                    rq_launch_shape *measured, rq_launch_shape *chosen);
+/* Applies a launch shape (for example one the tuner chose earlier, from a cache);
+   RQ_E_INVALID when the CTA size is not one of the six or it does not fit on an SM. */
+int rq_problem_set_launch(rq_problem *p, const rq_launch_shape *shape);
+int rq_problem_get_launch(const rq_problem *p, rq_launch_shape *shape);
 
 /* theta: n rows x n_active (host). rows: n (host). predictions: n x n_obs (host,
    NaN where the reference returns none). fields (optional, host): n x 11 x n_cells,

@@ -276,6 +276,7 @@ struct LinResult {
     int iterations = 0;
     double finalRes = 0.0, initialRes = 0.0;
     bool converged = false;
+    bool breakdown = false; // PCG stopped on |p.Ap| < 1e-30
 };
 
 // Right-Jacobi BiCGSTAB (LinearSolver.hpp:251-345)
@@ -340,8 +341,12 @@ static LinResult bicgstab(const Ldu &A, Vec &x, int maxIter, double tol) {
 
 // ---------------------------------------------------------------- device-style AMG
 // Hierarchy fixed per mesh: greedy strength-0.25 aggregation (LinearSolver.hpp:535-575)
-// of the geometric Laplacian area/delta with the cell-0 pin of the pressure system,
-// Galerkin summation (:578-618) refreshed from the current level-0 values, damped
+// of the geometric Laplacian area/delta with the cell-0 pin of the pressure system.
+// The prolongation is smoothed (smoothed aggregation: P = (I - omega D_F^-1 F) P_tent,
+// F the strength-filtered geometric matrix with weak entries lumped into its diagonal,
+// omega = 0.85 / rho(D_F^-1 F)); the row-relative fallback and the standalone linear
+// solves keep the piecewise-constant P_tent. Coarse values are Galerkin products
+// P^T A P (:578-618 with P_tent) refreshed from the current level-0 values, damped
 // Jacobi smoothing and an exact dense coarsest solve.
 struct Csr {
     int n = 0;
@@ -351,9 +356,12 @@ struct Csr {
 
 struct AmgLevel {
     Csr A;
-    std::vector<int> agg; // fine row -> coarse row
     int nc = 0;
-    std::vector<int> gIdx; // fine nnz -> coarse nnz
+    std::vector<int> pPtr, pCol; // prolongation rows: fine row -> coarse rows ascending
+    Vec pVal;
+    // Galerkin terms in generation order: coarse nnz tC[t] += tW[t] * fine nnz tF[t]
+    std::vector<int> tF, tC;
+    Vec tW;
     std::vector<int> dpos;
 };
 
@@ -362,13 +370,16 @@ struct Amg {
     std::vector<int> upPos, loPos; // LDU face -> level-0 nnz
     Vec inv;                        // dense inverse of the coarsest level (row major)
     // coarse values are re-summed only when the previous solve degraded, the rule
-    // AMGSolver applies to its aggregation (LinearSolver.hpp:924-941)
+    // AMGSolver applies to its aggregation (LinearSolver.hpp:924-941), a stop on the
+    // |p.Ap| < 1e-30 guard not counting as degradation
     bool needRefresh = true;
     int itersAfterRefresh = -1;
-    // smoother weight and coarse-correction scale: the pressure hierarchy uses
-    // 0.6 and 1; the standalone linear solves 0.75 and 1.7 (over-correction of
+    // smoother weight, coarse-correction scale and sweeps before / after the coarse
+    // correction: the smoothed-aggregation pressure hierarchy uses 0.6, 1 and 1; the
+    // fallback and the standalone linear solves 0.75, 1.7 and 2 (over-correction of
     // the piecewise-constant prolongation)
     double w = 0.6, alpha = 1.0;
+    int sweeps = 1;
     int levels() const { return static_cast<int>(lev.size()); }
 };
 
@@ -378,7 +389,7 @@ struct Amg {
 static const int AMG_MIN_COARSE = 64;
 static const int AMG_MIN_COARSE_LINEAR = 32;
 static const int AMG_MAX_LEVELS = 20;  // :663
-static const int AMG_SWEEPS = 2;
+static const double AMG_PROLONG_WEIGHT = 0.85;
 
 static Csr lduCsr(int n, const std::vector<int> &own, const std::vector<int> &nbr, int nf,
                   const Vec &d, const Vec &up, const Vec &lo, std::vector<int> *upPos,
@@ -520,29 +531,124 @@ static void aggregateLinear(const Csr &A, std::vector<int> &map, int &nc) {
     }
 }
 
-static Csr galerkinPattern(const Csr &A, const std::vector<int> &map, int nc) {
-    std::vector<std::map<int, double>> rows(nc);
-    for (int i = 0; i < A.n; ++i)
+// P of one level: smoothed (weight > 0) or piecewise constant (weight 0), rows with
+// their coarse columns ascending and exact zeros dropped.
+static void prolongation(const Csr &A, const std::vector<int> &agg, double weight,
+                         AmgLevel &fine) {
+    const int n = A.n;
+    auto strongAt = [&](int i, int k) {
+        const int c = A.col[k];
+        return c != i &&
+               std::abs(A.val[k]) / std::sqrt(std::abs(A.dg[i]) * std::abs(A.dg[c]) + 1e-30) > 0.25;
+    };
+    Vec fd(n);
+    for (int i = 0; i < n; ++i) {
+        double d = A.dg[i];
         for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
-            rows[map[i]][map[A.col[k]]] += 0.0;
-    Csr C;
+            if (A.col[k] != i && !strongAt(i, k))
+                d += A.val[k];
+        fd[i] = d;
+    }
+    auto usable = [&](int i) { return std::abs(fd[i]) > 1e-12 * std::abs(A.dg[i]); };
+    double omega = 0.0;
+    if (weight > 0.0) { // rho(D_F^-1 F) by 100 power iterations from a fixed start
+        Vec x(n), y(n);
+        for (int i = 0; i < n; ++i)
+            x[i] = 1.0 + 0.1 * (i % 7);
+        double rho = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double ny = 0.0, nx = 0.0;
+            for (int i = 0; i < n; ++i) {
+                double v = 0.0;
+                if (usable(i)) {
+                    v = fd[i] * x[i];
+                    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                        if (strongAt(i, k))
+                            v += A.val[k] * x[A.col[k]];
+                    v /= fd[i];
+                }
+                y[i] = v;
+                ny += v * v;
+                nx += x[i] * x[i];
+            }
+            rho = std::sqrt(ny / std::max(nx, 1e-300));
+            const double inv = 1.0 / std::max(std::sqrt(ny), 1e-300);
+            for (int i = 0; i < n; ++i)
+                x[i] = y[i] * inv;
+        }
+        omega = rho > 0.0 ? weight / rho : 0.0;
+    }
+    fine.pPtr.assign(n + 1, 0);
+    fine.pCol.clear();
+    fine.pVal.clear();
+    for (int i = 0; i < n; ++i) {
+        std::map<int, double> row;
+        row[agg[i]] += 1.0;
+        if (omega > 0.0 && usable(i)) {
+            const double sc = omega / fd[i];
+            row[agg[i]] -= sc * fd[i];
+            for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                if (strongAt(i, k))
+                    row[agg[A.col[k]]] -= sc * A.val[k];
+        }
+        for (auto &e : row)
+            if (e.second != 0.0) {
+                fine.pCol.push_back(e.first);
+                fine.pVal.push_back(e.second);
+            }
+        fine.pPtr[i + 1] = static_cast<int>(fine.pCol.size());
+    }
+}
+
+// The coarse level of `fine` under its P: the pattern of P^T A P and the Galerkin terms
+// in generation order (fine rows ascending, each row's entries in column order, then
+// P's entries of the row and of the column), then the values from the fine values.
+static void galerkinLevel(AmgLevel &fine, AmgLevel &coarse) {
+    const Csr &A = fine.A;
+    const int nc = fine.nc;
+    std::vector<std::map<int, int>> rows(nc);
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            const int j = A.col[k];
+            for (int a = fine.pPtr[i]; a < fine.pPtr[i + 1]; ++a)
+                for (int b = fine.pPtr[j]; b < fine.pPtr[j + 1]; ++b)
+                    rows[fine.pCol[a]][fine.pCol[b]] = 0;
+        }
+    Csr &C = coarse.A;
+    C = Csr{};
     C.n = nc;
     C.ptr.assign(nc + 1, 0);
     C.dg.assign(nc, 0.0);
     for (int I = 0; I < nc; ++I) {
         C.ptr[I + 1] = C.ptr[I] + static_cast<int>(rows[I].size());
         for (auto &e : rows[I]) {
+            e.second = static_cast<int>(C.col.size());
             C.col.push_back(e.first);
             C.val.push_back(0.0);
         }
     }
-    return C;
+    fine.tF.clear();
+    fine.tC.clear();
+    fine.tW.clear();
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+            const int j = A.col[k];
+            for (int a = fine.pPtr[i]; a < fine.pPtr[i + 1]; ++a)
+                for (int b = fine.pPtr[j]; b < fine.pPtr[j + 1]; ++b) {
+                    fine.tF.push_back(k);
+                    fine.tC.push_back(rows[fine.pCol[a]][fine.pCol[b]]);
+                    fine.tW.push_back(fine.pVal[a] * fine.pVal[b]);
+                }
+        }
+    coarse.dpos.resize(nc);
+    for (int I = 0; I < nc; ++I)
+        coarse.dpos[I] = csrFind(C, I, I);
 }
 
 static void sumCoarse(const AmgLevel &fine, AmgLevel &coarse) {
     std::fill(coarse.A.val.begin(), coarse.A.val.end(), 0.0);
-    for (size_t k = 0; k < fine.A.val.size(); ++k)
-        coarse.A.val[fine.gIdx[k]] += fine.A.val[k];
+    for (size_t t = 0; t < fine.tF.size(); ++t)
+        coarse.A.val[fine.tC[t]] += fine.tW[t] * fine.A.val[fine.tF[t]];
     for (int I = 0; I < coarse.A.n; ++I)
         coarse.A.dg[I] = coarse.A.val[coarse.dpos[I]];
 }
@@ -612,22 +718,16 @@ static Amg buildAmg(const Mesh &m) {
         if (nc == 0 || nc >= fine.A.n)
             break;
         AmgLevel coarse;
-        coarse.A = galerkinPattern(fine.A, map, nc);
-        coarse.dpos.resize(nc);
-        for (int I = 0; I < nc; ++I)
-            coarse.dpos[I] = csrFind(coarse.A, I, I);
-        fine.agg = std::move(map);
         fine.nc = nc;
-        fine.gIdx.resize(fine.A.val.size());
-        for (int i = 0; i < fine.A.n; ++i)
-            for (int k = fine.A.ptr[i]; k < fine.A.ptr[i + 1]; ++k)
-                fine.gIdx[k] = csrFind(coarse.A, fine.agg[i], fine.agg[fine.A.col[k]]);
+        prolongation(fine.A, map, attempt == 0 ? AMG_PROLONG_WEIGHT : 0.0, fine);
+        galerkinLevel(fine, coarse);
         sumCoarse(fine, coarse);
         h.lev.push_back(std::move(coarse));
     }
     if (attempt == 1) { // the fallback hierarchy over-corrects (as the linear solves)
         h.w = 0.75;
         h.alpha = 1.7;
+        h.sweeps = 2;
     }
     if (h.lev.back().A.n <= AMG_MIN_COARSE)
         break;
@@ -662,8 +762,8 @@ static void csrResidual(const Csr &A, const Vec &x, const Vec &b, Vec &r) {
     }
 }
 
-// One V-cycle z = M^-1 r: pre-smoothing from zero, restriction by aggregate sums,
-// prolongation by aggregate broadcast, the same post-smoothing (symmetric).
+// One V-cycle z = M^-1 r: pre-smoothing from zero (h.sweeps damped-Jacobi sweeps),
+// restriction by P^T, prolongation x + alpha P x_c, the same post-smoothing (symmetric).
 static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
     const Csr &A = h.lev[l].A;
     const int n = A.n;
@@ -679,7 +779,7 @@ static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
     Vec r(n);
     for (int i = 0; i < n; ++i)
         x[i] = h.w * b[i] / A.dg[i];
-    for (int s = 1; s < AMG_SWEEPS; ++s) {
+    for (int s = 1; s < h.sweeps; ++s) {
         csrResidual(A, x, b, r);
         for (int i = 0; i < n; ++i)
             x[i] += h.w * r[i] / A.dg[i];
@@ -688,11 +788,16 @@ static void vcycle(const Amg &h, int l, const Vec &b, Vec &x) {
     const AmgLevel &fl = h.lev[l];
     Vec bc(fl.nc, 0.0), xc(fl.nc, 0.0);
     for (int i = 0; i < n; ++i)
-        bc[fl.agg[i]] += r[i];
+        for (int a = fl.pPtr[i]; a < fl.pPtr[i + 1]; ++a)
+            bc[fl.pCol[a]] += fl.pVal[a] * r[i];
     vcycle(h, l + 1, bc, xc);
-    for (int i = 0; i < n; ++i)
-        x[i] += h.alpha * xc[fl.agg[i]];
-    for (int s = 0; s < AMG_SWEEPS; ++s) {
+    for (int i = 0; i < n; ++i) {
+        double pc = 0.0;
+        for (int a = fl.pPtr[i]; a < fl.pPtr[i + 1]; ++a)
+            pc += fl.pVal[a] * xc[fl.pCol[a]];
+        x[i] += h.alpha * pc;
+    }
+    for (int s = 0; s < h.sweeps; ++s) {
         csrResidual(A, x, b, r);
         for (int i = 0; i < n; ++i)
             x[i] += h.w * r[i] / A.dg[i];
@@ -722,7 +827,8 @@ static LinResult pcg(const Ldu &A, Vec &x, int maxIter, double tol, Amg *amg) {
     if (amg) {
         if (refreshed || amg->itersAfterRefresh <= 0)
             amg->itersAfterRefresh = res.iterations;
-        else if (!res.converged || res.iterations > 1.5 * amg->itersAfterRefresh + 2)
+        else if ((!res.converged && !res.breakdown) ||
+                 res.iterations > 1.5 * amg->itersAfterRefresh + 2)
             amg->needRefresh = true;
     }
     return res;
@@ -751,8 +857,10 @@ static LinResult pcgBody(const Ldu &A, Vec &x, int maxIter, double tol, Amg *amg
     for (int it = 0; it < maxIter; ++it) {
         A.matvec(p, Ap);
         const double pAp = dot(p, Ap);
-        if (std::abs(pAp) < 1e-30)
+        if (std::abs(pAp) < 1e-30) {
+            res.breakdown = true;
             break;
+        }
         const double alpha = rz / pAp;
         for (int i = 0; i < n; ++i) {
             x[i] += alpha * p[i];
@@ -1952,6 +2060,7 @@ int orc_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,
             Amg h;
             h.w = 0.75;
             h.alpha = 1.7;
+            h.sweeps = 2;
             AmgLevel l0;
             l0.A = lduCsr(n, ow, nb, nif, A.d, A.up, A.lo, &h.upPos, &h.loPos);
             l0.dpos.resize(n);
@@ -1968,16 +2077,9 @@ int orc_linear_solve(int32_t kind, int32_t n, int32_t nif, const double *diag,
                 if (nc == 0 || nc >= fine.A.n)
                     break;
                 AmgLevel coarse;
-                coarse.A = galerkinPattern(fine.A, map, nc);
-                coarse.dpos.resize(nc);
-                for (int I = 0; I < nc; ++I)
-                    coarse.dpos[I] = csrFind(coarse.A, I, I);
-                fine.agg = std::move(map);
                 fine.nc = nc;
-                fine.gIdx.resize(fine.A.val.size());
-                for (int i = 0; i < fine.A.n; ++i)
-                    for (int k = fine.A.ptr[i]; k < fine.A.ptr[i + 1]; ++k)
-                        fine.gIdx[k] = csrFind(coarse.A, fine.agg[i], fine.agg[fine.A.col[k]]);
+                prolongation(fine.A, map, 0.0, fine);
+                galerkinLevel(fine, coarse);
                 sumCoarse(fine, coarse);
                 h.lev.push_back(std::move(coarse));
             }
@@ -2009,7 +2111,7 @@ int orc_amg_hierarchy(const orc_case *c, int32_t *sizes, int32_t cap, int32_t *m
             sizes[l] = h.lev[l].A.n;
             if (maps && l + 1 < h.levels())
                 for (int i = 0; i < h.lev[l].A.n; ++i)
-                    maps[off++] = h.lev[l].agg[i];
+                    maps[off++] = h.lev[l].pCol[h.lev[l].pPtr[i]]; // first coarse row of P
         }
         return h.levels();
     } catch (const std::exception &e) {
