@@ -175,7 +175,7 @@ def test_1536_cell_class_fields_after_n_iterations(rq, checker, n_iter):
 def test_ensemble_classes_match_reference(rq):
     """The benchmark's three classes at (0.31, 0.09), one multi-class launch: each
     converges to the reference's own converged profile (the ensemble's synthetic
-    truth, written by data/make_channel_truth.py from oracle/_ref) to 1e-10, in an
+    truth, written by tests/golden/make_channel_truth.py from oracle/_ref) to 1e-10, in an
     iteration count within 2 % of the reference's (12460, 58690, 258900)."""
     import json
 

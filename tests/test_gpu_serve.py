@@ -103,3 +103,30 @@ def test_close_drains_and_rejects_new_requests(rq):
     assert srv.info()["slots"] == 2
     assert all(srv.poll(t) is not None for t in ts)
     srv.destroy()
+
+
+def test_served_far_off_draws_get_the_reference_verdicts(rq):
+    """In-bounds draws far from the calibration box (a1 or beta* at the edge of its
+    admissible range) do not converge within the cap; served among in-box draws that
+    do, every request must come back with the compiled reference's own verdict and
+    iteration count for the same draw (tests/golden/serve_failures_ref.json, made by
+    tests/golden/make_serve_failures.py from oracle/_ref), the failed ones flagged with
+    no predictions returned."""
+    import json
+
+    g = json.loads(open(cases.__file__.replace("cases.py", "golden/serve_failures_ref.json")).read())
+    batch = cases.product_batch(rq, cases.small_channel(max_iter=g["cap"]))
+    srv = rq.ForwardServer([batch], capacity=32, idle_timeout=5.0)
+    tickets = [srv.submit(0, r["theta"]) for r in g["rows"]]
+    assert srv.wait(600.0) == len(tickets)
+    served = [srv.poll(t) for t in tickets]
+    srv.destroy()
+    assert sum(r["status"] != "Converged" for r in g["rows"]) >= 3
+    for s, r in zip(served, g["rows"]):
+        assert s.status.name == r["status"], (r["theta"], s.status.name, r["status"])
+        if r["status"] == "Converged":
+            assert abs(s.iterations - r["iterations"]) <= 0.02 * r["iterations"]
+            assert not s.flagged and s.predictions is not None
+        else:
+            assert s.iterations == r["iterations"] == g["cap"]
+            assert s.flagged and s.predictions is None
