@@ -80,6 +80,7 @@ SIGNATURES = {
                            C.POINTER(C.c_void_p)], C.c_int),
     "rq_problem_destroy": ([C.c_void_p], C.c_int),
     "rq_problem_info": ([C.c_void_p, IP, IP, IP, IP], C.c_int),
+    "rq_problem_workspace_bytes": ([C.c_void_p, C.POINTER(C.c_uint64)], C.c_int),
     "rq_problem_tune": ([C.c_void_p, DP, C.c_int32, C.POINTER(LaunchShape), C.c_int32,
                          C.POINTER(LaunchShape), C.POINTER(LaunchShape)], C.c_int),
     "rq_problem_set_launch": ([C.c_void_p, C.POINTER(LaunchShape)], C.c_int),
@@ -115,6 +116,10 @@ SIGNATURES = {
                                      C.c_void_p], C.c_int),
     "rq_server_create": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double, C.c_int32,
                           C.POINTER(C.c_void_p)], C.c_int),
+    "rq_server_create_pooled": ([C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_double,
+                                 C.c_int32, C.c_uint64, C.POINTER(C.c_void_p)], C.c_int),
+    "rq_server_memory": ([C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                          C.POINTER(C.c_int64), IP], C.c_int),
     "rq_server_submit": ([C.c_void_p, C.c_int32, DP, C.POINTER(C.c_int64)], C.c_int),
     "rq_server_poll": ([C.c_void_p, C.c_int64, IP, C.POINTER(RowOut), DP,
                         C.POINTER(C.c_int64)], C.c_int),

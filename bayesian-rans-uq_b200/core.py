@@ -550,6 +550,11 @@ class _Problem:
         self.n_cells = mesh.n_cells()
         self.nx = mesh.nx
 
+    def workspace_bytes(self) -> int:
+        b = C.c_uint64()
+        N.call("rq_problem_workspace_bytes", self.handle, C.byref(b))
+        return b.value
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h is not None and h.value:
@@ -732,13 +737,14 @@ class ForwardServer:
     result of a request does not depend on what else is in flight."""
 
     def __init__(self, batches, capacity: int = 4096, idle_timeout: float = 2.0,
-                 max_slots: int = 0):
+                 max_slots: int = 0, pool_bytes: int = 0):
         self._batches = list(batches)  # the mesh classes must outlive the server
         nb = len(self._batches)
         handles = (C.c_void_p * nb)(*[b._problem.handle.value for b in self._batches])
         h = C.c_void_p()
-        N.call("rq_server_create", handles, C.c_int32(nb), C.c_int32(capacity),
-               C.c_double(idle_timeout), C.c_int32(max_slots), C.byref(h))
+        N.call("rq_server_create_pooled", handles, C.c_int32(nb), C.c_int32(capacity),
+               C.c_double(idle_timeout), C.c_int32(max_slots), C.c_uint64(pool_bytes),
+               C.byref(h))
         self.handle = h
         self._no = max(max(b.n_observations() for b in self._batches), 1)
         self._cls: list[int] = []
@@ -781,6 +787,19 @@ class ForwardServer:
                C.byref(lau))
         return {"slots": slots.value, "submitted": sub.value, "completed": comp.value,
                 "launches": lau.value}
+
+    def memory(self) -> dict:
+        """The workspace pool (rq_server_memory): bytes, bytes held by admitted requests,
+        requests waiting for admission, CTAs running now."""
+        pool, used, waiting, running = C.c_uint64(), C.c_uint64(), C.c_int64(), C.c_int32()
+        N.call("rq_server_memory", self.handle, C.byref(pool), C.byref(used),
+               C.byref(waiting), C.byref(running))
+        return {"pool_bytes": pool.value, "in_use_bytes": used.value, "waiting": waiting.value,
+                "running_ctas": running.value}
+
+    def workspace_bytes(self, cls: int) -> int:
+        """Device workspace one solve of mesh class `cls` takes from the pool."""
+        return int(self._batches[cls]._problem.workspace_bytes())
 
     def destroy(self) -> None:
         h = getattr(self, "handle", None)

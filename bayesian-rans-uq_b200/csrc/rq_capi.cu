@@ -595,6 +595,14 @@ int rq_problem_destroy(rq_problem *p) {
     });
 }
 
+int rq_problem_workspace_bytes(const rq_problem *p, uint64_t *bytes) {
+    return guarded([&] {
+        if (!p || !bytes)
+            throw std::invalid_argument("null argument");
+        *bytes = sizeof(double) * static_cast<uint64_t>(p->cls.wsDoubles);
+    });
+}
+
 int rq_problem_set_launch(rq_problem *p, const rq_launch_shape *shape) {
     return guarded([&] {
         if (!p || !shape)

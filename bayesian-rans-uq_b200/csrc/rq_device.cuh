@@ -103,6 +103,9 @@ struct DevJob {
     // device face layout (x faces, then y faces), the beta1 of the final wall-face omega,
     // and the turbulence-established marker (0 or 1).
     double *snap;
+    // Solve workspace of this job (the serving loop's pool region of the job's class),
+    // or null: the CTA's own per-slot workspace.
+    double *ws;
 };
 
 // Request queue of the serving loop. The host appends requests (jobs[i], with
@@ -115,7 +118,7 @@ struct ServeQueue {
     const int *closed;       // host-mapped: 1 = no more requests (drain), 2 = cancel the rest
     int *done;               // host-mapped: one flag per request
     int *head;               // device: next request to claim
-    int *idleExits;          // device: CTAs that left after idleNs without work
+    int *exits;              // device: CTAs that have left (idle, drained or cancelled)
     int capacity, pad;
     long long idleNs;
 };

@@ -53,6 +53,25 @@ template <typename T> struct KW {
     T *amgVal, *amgVec;                   // coarse levels: values; b, xa, xb, r, 1/diag
 };
 
+struct LinRes {
+    int iterations;
+    double finalRes, initialRes;
+    bool converged;
+    bool breakdown = false; // stopped on the |p.Ap| < 1e-30 guard (a round-off right-hand side)
+};
+
+// The outer loop's scalars. Every thread derives them identically from the same
+// block reductions and writes the same value, so they can live here rather than in
+// registers: a phase call then has no live loop state to save and restore around it
+// (those saves were local-memory traffic that missed L1 at large meshes).
+struct LoopState {
+    double lastK, lastW, worst, fluxRef, n0x, n0y, n0p, rateU;
+    double momRes, momScale, contScaled, fluxScale, uChange;
+    LinRes resU[2], resP, resK, resW;
+    int amgNeed, amgAfter, status, finalIter;
+    bool established, converged, diverged;
+};
+
 struct Shared {
     DevClass C;
     Work W;
@@ -73,6 +92,7 @@ struct Shared {
     double wallBeta;  // beta1 the wall-face omega was last set with (applyAllBCs' default
                       // on a cold start, the cached solve's on a warm one, then b1)
     double coarse[32 * 32];               // in-place inverse of a coarsest level of <= 32 rows
+    LoopState L;                          // the outer loop's scalars (runSolve)
 };
 
 // stage timers, as the reference's momentum / pressure / turbulence timers
@@ -256,13 +276,6 @@ __device__ __forceinline__ double rowDot(const Cell &q, const double *d, const d
 __device__ __forceinline__ double jac(double r, double d) {
     return (fabs(d) > 1e-30) ? r / d : r; // jacobiPrecond, LinearSolver.hpp:173-177
 }
-
-struct LinRes {
-    int iterations;
-    double finalRes, initialRes;
-    bool converged;
-    bool breakdown = false; // stopped on the |p.Ap| < 1e-30 guard (a round-off right-hand side)
-};
 
 #define FOR_CELLS(c) for (int c = threadIdx.x; c < n; c += blockDim.x)
 
@@ -537,24 +550,24 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
     }
 }
 
-// Sum over the slots of one ELL row, k ascending, of coef(k) * vec(col(k)) for columns
-// >= 0. The loads of four slots are issued before their products are added (padding
-// slots load entry 0 and add nothing), so a wide row costs a few load latencies, not
-// one per slot; the order of the additions is the slots' order.
+// Sum over the slots k = first, first + step, ... (< width) of one ELL row of
+// coef(k) * vec(col(k)) for columns >= 0, k ascending. The loads of four slots are
+// issued before their products are added (padding slots load entry 0 and add
+// nothing), so a wide row costs a few load latencies, not one per slot.
 template <typename T, typename C, typename V>
 __device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V *vec, int width,
-                                    int stride, int row) {
+                                    int stride, int row, int first = 0, int step = 1) {
     T s = T(0);
-    int k = 0;
-    for (; k + 4 <= width; k += 4) {
+    int k = first;
+    for (; k + 3 * step < width; k += 4 * step) {
         int c[4];
         T v[4], x[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            c[u] = __ldg(cols + (k + u) * stride + row);
+            c[u] = __ldg(cols + (k + u * step) * stride + row);
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            v[u] = T(coef[(k + u) * stride + row]);
+            v[u] = T(coef[(k + u * step) * stride + row]);
             x[u] = T(vec[c[u] < 0 ? 0 : c[u]]);
         }
 #pragma unroll
@@ -562,15 +575,15 @@ __device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V 
             if (c[u] >= 0)
                 s += v[u] * x[u];
     }
-    if (k + 2 <= width) {
-        const int c0 = __ldg(cols + k * stride + row), c1 = __ldg(cols + (k + 1) * stride + row);
-        const T v0 = T(coef[k * stride + row]), v1 = T(coef[(k + 1) * stride + row]);
+    if (k + step < width) {
+        const int c0 = __ldg(cols + k * stride + row), c1 = __ldg(cols + (k + step) * stride + row);
+        const T v0 = T(coef[k * stride + row]), v1 = T(coef[(k + step) * stride + row]);
         const T x0 = T(vec[c0 < 0 ? 0 : c0]), x1 = T(vec[c1 < 0 ? 0 : c1]);
         if (c0 >= 0)
             s += v0 * x0;
         if (c1 >= 0)
             s += v1 * x1;
-        k += 2;
+        k += 2 * step;
     }
     if (k < width) {
         const int c = __ldg(cols + k * stride + row);
@@ -578,6 +591,36 @@ __device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V 
             s += T(coef[k * stride + row]) * T(vec[c]);
     }
     return s;
+}
+
+// Threads per row of a pass over n rows: the largest power of two up to 32 for which
+// one pass of the CTA still covers every row (1 when there are more rows than half
+// the CTA's threads).
+__device__ __forceinline__ int segOf(int n) {
+    int seg = 1;
+    while (seg < 32 && 2 * seg * n <= static_cast<int>(blockDim.x))
+        seg *= 2;
+    return seg;
+}
+
+// A pass over the rows of a small level with several threads per row: lane j of a
+// row's segment computes part(i, j, seg), the partial sum of the row's terms j,
+// j + seg, ...; the partials are added by shuffles within the segment (a tree) and
+// the segment's first lane calls use(i, total). Every thread of the CTA takes part
+// (the shuffles need whole warps), so calls must be uniform across the CTA. With one
+// thread per row this is the plain row loop.
+template <typename T, typename Part, typename Use>
+__device__ __forceinline__ void segPass(int n, Part part, Use use) {
+    const int seg = segOf(n), per = static_cast<int>(blockDim.x) / seg;
+    const int r = threadIdx.x / seg, j = threadIdx.x - r * seg;
+    for (int base = 0; base < n; base += per) {
+        const int i = base + r;
+        T s = i < n ? part(i, j, seg) : T(0);
+        for (int o = seg >> 1; o > 0; o >>= 1)
+            s += __shfl_xor_sync(FULL, s, o);
+        if (j == 0 && i < n)
+            use(i, s);
+    }
 }
 
 // row i of an ELL level times x, entries in column order
@@ -607,11 +650,12 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     auto vb = [&](int l) { return amgVec + C.lev[l].vecOff; }; // b, xa, xb, r, 1/diag
     auto sync = [] { __syncthreads(); };
     const int t0 = threadIdx.x, ts = blockDim.x;
-    // residual of level l-1 restricted to row I of level l: sum_k R_Ik r_k
-    auto restrictRow = [&](int l, int I) {
+    // residual of level l-1 restricted to row I of level l: sum_k R_Ik r_k (lane j of
+    // the row's segment: the terms j, j + seg, ...)
+    auto restrictPart = [&](int l, int I, int j, int seg) {
         const DevAmgLevel &F = C.lev[l - 1];
         const T *fr = (l == 1) ? Krr : vb(l - 1) + 3 * F.n;
-        return ellDot<T>(F.rcol, F.rval, fr, F.rw, C.lev[l].n, I);
+        return ellDot<T>(F.rcol, F.rval, fr, F.rw, C.lev[l].n, I, j, seg);
     };
     // the prolongated coarse correction at row i of level l: sum_k P_ik x_c
     auto prolong = [&](int l, int i) {
@@ -620,55 +664,52 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         return ellDot<T>(Lv.pcol, Lv.pval, xc, Lv.pw, Lv.n, i);
     };
     // one level of the down sweep; the pre-smoothed iterate ends in xa (one sweep) or
-    // xb (two sweeps), the residual in rr
+    // xb (two sweeps), the residual in rr. Coarse levels run several threads per row.
     auto down = [&](int l) {
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
-        T *b, *xa, *xb, *rr;
         if (l == 0) {
-            b = Kr;
-            xa = Kxa;
-            xb = Kxb;
-            rr = Krr;
-        } else {
-            b = vb(l);
-            xa = b + n;
-            xb = b + 2 * n;
-            rr = b + 3 * n;
-        }
-        const T *val = amgVal + Lv.valOff;
-        for (int i = t0; i < n; i += ts) {
-            T bi;
-            if (l == 0) {
-                bi = b[i];
-            } else {
-                bi = restrictRow(l, i);
-                b[i] = bi;
+            for (int i = t0; i < n; i += ts)
+                Kxa[i] = om * Kr[i] * Krd[i];
+            sync();
+            const T *xs = Kxa;
+            if (two) {
+                for (int i = t0; i < n; i += ts) {
+                    const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
+                    Kxb[i] = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
+                }
+                sync();
+                xs = Kxb;
             }
-            const T ri = (l == 0) ? Krd[i] : b[4 * n + i];
-            xa[i] = om * bi * ri;
+            for (int i = t0; i < n; i += ts)
+                Krr[i] = Kr[i] - rowDotT(cellOf(C, i), M, xs, nx);
+            sync();
+            return;
         }
+        T *b = vb(l), *xa = b + n, *xb = b + 2 * n, *rr = b + 3 * n;
+        const T *rd = b + 4 * n;
+        const T *val = amgVal + Lv.valOff;
+        segPass<T>(n, [&](int i, int j, int seg) { return restrictPart(l, i, j, seg); },
+                   [&](int i, T bi) {
+                       b[i] = bi;
+                       xa[i] = om * bi * rd[i];
+                   });
         sync();
         const T *xs = xa;
         if (two) {
-            for (int i = t0; i < n; i += ts) {
-                T ax, ri;
-                if (l == 0) {
-                    ax = rowDotT(cellOf(C, i), M, xa, nx);
-                    ri = Krd[i];
-                } else {
-                    ax = csrRowT(Lv, val, xa, i);
-                    ri = b[4 * n + i];
-                }
-                xb[i] = xa[i] + om * (b[i] - ax) * ri;
-            }
+            segPass<T>(n,
+                       [&](int i, int j, int seg) {
+                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                       },
+                       [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
             xs = xb;
         }
-        for (int i = t0; i < n; i += ts) {
-            const T ax = (l == 0) ? rowDotT(cellOf(C, i), M, xs, nx) : csrRowT(Lv, val, xs, i);
-            rr[i] = b[i] - ax;
-        }
+        segPass<T>(n,
+                   [&](int i, int j, int seg) {
+                       return ellDot<T>(Lv.ecol, val, xs, Lv.width, n, i, j, seg);
+                   },
+                   [&](int i, T ax) { rr[i] = b[i] - ax; });
         sync();
     };
     // the coarsest level: restriction of the level above, then the dense inverse
@@ -680,20 +721,24 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             for (int i = t0; i < m; i += ts)
                 b[i] = Kr[i];
         } else {
-            for (int i = t0; i < m; i += ts)
-                b[i] = restrictRow(l, i);
+            segPass<T>(m, [&](int i, int j, int seg) { return restrictPart(l, i, j, seg); },
+                       [&](int i, T bi) { b[i] = bi; });
         }
         sync();
         // the coarsest solve stays FP64 in both forms: the coarsest level of the
         // pinned all-Neumann pressure system is nearly singular, and an FP32
         // copy of its inverse loses the coarse correction
-        for (int i = t0; i < m; i += ts) {
-            double s = 0.0;
-            const double *row = (m <= 32) ? S.coarse + i * m : W.dense0 + i * m2 + m;
-            for (int j = 0; j < m; ++j)
-                s += row[j] * double(b[j]);
-            xb[i] = T(s);
-        }
+        const double *inv = (m <= 32) ? S.coarse : W.dense0 + m;
+        const int ld = (m <= 32) ? m : m2;
+        segPass<double>(m,
+                        [&](int i, int j, int seg) {
+                            const double *row = inv + i * ld;
+                            double s = 0.0;
+                            for (int k = j; k < m; k += seg)
+                                s += row[k] * double(b[k]);
+                            return s;
+                        },
+                        [&](int i, double s) { xb[i] = T(s); });
         sync();
     };
     // one level of the up sweep (levels >= 1; level 0 ends in the reduction below):
@@ -706,6 +751,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         T *b = vb(l), *xa = b + n, *xb = b + 2 * n, *xi = b + 3 * n;
+        const T *rd = b + 4 * n;
         const T *xpre = two ? xb : xa;
         T *out = two ? xa : xb;
         const T *val = amgVal + Lv.valOff;
@@ -713,8 +759,11 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             for (int i = t0; i < n; i += ts)
                 xi[i] = xpre[i] + al * prolong(l, i);
             sync();
-            for (int i = t0; i < n; i += ts)
-                out[i] = xi[i] + om * (b[i] - csrRowT(Lv, val, xi, i)) * b[4 * n + i];
+            segPass<T>(n,
+                       [&](int i, int j, int seg) {
+                           return ellDot<T>(Lv.ecol, val, xi, Lv.width, n, i, j, seg);
+                       },
+                       [&](int i, T ax) { out[i] = xi[i] + om * (b[i] - ax) * rd[i]; });
         } else {
             for (int i = t0; i < n; i += ts) {
                 const T x0 = xpre[i] + al * prolong(l, i);
@@ -724,13 +773,16 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
                     if (jj >= 0)
                         ax += val[k * n + i] * (xpre[jj] + al * prolong(l, jj));
                 }
-                out[i] = x0 + om * (b[i] - ax) * b[4 * n + i];
+                out[i] = x0 + om * (b[i] - ax) * rd[i];
             }
         }
         sync();
         if (two) {
-            for (int i = t0; i < n; i += ts)
-                xb[i] = xa[i] + om * (b[i] - csrRowT(Lv, val, xa, i)) * b[4 * n + i];
+            segPass<T>(n,
+                       [&](int i, int j, int seg) {
+                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                       },
+                       [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
         }
     };
@@ -788,6 +840,87 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     return rz;
 }
 
+// The sweeps of one PCG iteration as functions of their own, so that the PCG loop
+// itself keeps only a few scalars live across the V-cycle call (every value live
+// across a call is saved to and reloaded from local memory around it).
+// Ap = A p; returns (p, Ap).
+template <typename T> __device__ __noinline__ double pcgMatvec(Shared &S, int &rp, const KW<T> &K) {
+    const DevClass &C = S.C;
+    const int n = C.n, nx = C.nx;
+    const Mat<T> M = matOf(K);
+    const T *p = K.pv;
+    T *Ap = K.v;
+    double a[1] = {0.0};
+    FOR_CELLS(c) {
+        const T v = rowDotT(cellOf(C, c), M, p, nx);
+        Ap[c] = v;
+        a[0] += double(p[c]) * double(v);
+    }
+    blockSum<1>(a, S, rp);
+    return a[0];
+}
+// x += alpha p, r -= alpha Ap; returns (r, r)
+template <typename T>
+__device__ __noinline__ double pcgUpdate(Shared &S, int &rp, const KW<T> &K, T *x, double alpha) {
+    const int n = S.C.n;
+    const T *p = K.pv, *Ap = K.v;
+    T *r = K.r;
+    double a[1] = {0.0};
+    FOR_CELLS(c) {
+        x[c] += T(alpha) * p[c];
+        const T rc = r[c] - T(alpha) * Ap[c];
+        r[c] = rc;
+        a[0] += double(rc) * double(rc);
+    }
+    blockSum<1>(a, S, rp);
+    return a[0];
+}
+// z = r / diag; returns (r, z)
+template <typename T> __device__ __noinline__ double pcgJacobi(Shared &S, int &rp, const KW<T> &K) {
+    const int n = S.C.n;
+    const T *r = K.r, *rdv = K.rd;
+    T *z = K.z;
+    double a[1] = {0.0};
+    FOR_CELLS(c) {
+        z[c] = r[c] * rdv[c];
+        a[0] += double(r[c]) * double(z[c]);
+    }
+    blockSum<1>(a, S, rp);
+    return a[0];
+}
+// p = z + beta p (beta 0: p = z), then a barrier
+template <typename T> __device__ __noinline__ void pcgDirection(Shared &S, const KW<T> &K, double beta) {
+    const int n = S.C.n;
+    const T *z = K.z;
+    T *p = K.pv;
+    if (beta == 0.0) {
+        FOR_CELLS(c) p[c] = z[c];
+    } else {
+        FOR_CELLS(c) p[c] = z[c] + T(beta) * p[c];
+    }
+    __syncthreads();
+}
+// z = M^-1 r through the FP32 V-cycle of S.K32; returns (r, z) in FP64
+template <typename T> __device__ __noinline__ double pcgPrecondF32(Shared &S, int &rp, const KW<T> &K) {
+    const int n = S.C.n;
+    {
+        const KW<float> &F = S.K32;
+        const T *r = K.r;
+        FOR_CELLS(c) F.r[c] = float(r[c]);
+    }
+    vcycleT<float>(S, rp, S.K32);
+    const KW<float> &F = S.K32;
+    const T *r = K.r;
+    T *z = K.z;
+    double a[1] = {0.0};
+    FOR_CELLS(c) {
+        z[c] = T(F.z[c]);
+        a[0] += double(r[c]) * double(z[c]);
+    }
+    blockSum<1>(a, S, rp);
+    return a[0];
+}
+
 // PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0 with the Jacobi or the AMG
 // preconditioner; K.r holds b and r0n its norm, x receives the solution.
 // With F32Precond the AMG V-cycle runs on the FP32 copies (S.K32) while PCG itself
@@ -795,32 +928,34 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
 template <typename T, bool F32Precond>
 __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, double r0n,
                                     int maxIter, double tol, bool amg, bool refresh) {
-    const DevClass &C = S.C;
-    const int n = C.n, nx = C.nx;
     LinRes res{0, 0.0, r0n, false};
     if (r0n < 1e-30) {
         res.converged = true;
         return res;
     }
-    const Mat<T> M = matOf(K);
-    T *const rdv = K.rd;
-    FOR_CELLS(c) {
-        const T dc = M.d[c];
-        rdv[c] = (fabs(double(dc)) > 1e-30) ? T(1) / dc : T(1);
-        x[c] = T(0);
-    }
-    if constexpr (F32Precond) {
-        if (amg) { // FP32 copy of the finest level for the FP32 V-cycle
-            const KW<float> &F = S.K32;
-            FOR_CELLS(c) {
-                F.d[c] = float(M.d[c]);
-                F.aW[c] = float(M.aW[c]);
-                F.aE[c] = float(M.aE[c]);
-                F.aS[c] = float(M.aS[c]);
-                F.aN[c] = float(M.aN[c]);
-                F.rd[c] = (fabs(double(F.d[c])) > 1e-30) ? 1.0f / F.d[c] : 1.0f;
+    {
+        const int n = S.C.n;
+        const T *d = K.d;
+        T *rdv = K.rd;
+        FOR_CELLS(c) {
+            const T dc = d[c];
+            rdv[c] = (fabs(double(dc)) > 1e-30) ? T(1) / dc : T(1);
+            x[c] = T(0);
+        }
+        if constexpr (F32Precond) {
+            if (amg) { // FP32 copy of the finest level for the FP32 V-cycle
+                const KW<float> &F = S.K32;
+                const Mat<T> M = matOf(K);
+                FOR_CELLS(c) {
+                    F.d[c] = float(M.d[c]);
+                    F.aW[c] = float(M.aW[c]);
+                    F.aE[c] = float(M.aE[c]);
+                    F.aS[c] = float(M.aS[c]);
+                    F.aN[c] = float(M.aN[c]);
+                    F.rd[c] = (fabs(double(F.d[c])) > 1e-30) ? 1.0f / F.d[c] : 1.0f;
+                }
+                __syncthreads();
             }
-            __syncthreads();
         }
     }
     if (amg && refresh) {
@@ -833,84 +968,31 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
     } else {
         __syncthreads();
     }
-    T *r = K.r, *z = K.z, *p = K.pv, *Ap = K.v;
-    // z = M^-1 r through the FP32 V-cycle, (r, z) in FP64
-    auto precondF32 = [&]() {
-        const KW<float> &F = S.K32;
-        FOR_CELLS(c) F.r[c] = float(r[c]);
-        vcycleT<float>(S, rp, F);
-        double a[1] = {0.0};
-        FOR_CELLS(c) {
-            z[c] = T(F.z[c]);
-            a[0] += double(r[c]) * double(z[c]);
-        }
-        blockSum<1>(a, S, rp);
-        return a[0];
-    };
-    double rz;
-    if (amg) {
+    auto precond = [&]() {
+        if (!amg)
+            return pcgJacobi(S, rp, K);
         if constexpr (F32Precond)
-            rz = precondF32();
+            return pcgPrecondF32(S, rp, K);
         else
-            rz = vcycleT(S, rp, K);
-    } else {
-        double a[1] = {0.0};
-        FOR_CELLS(c) {
-            z[c] = r[c] * rdv[c];
-            a[0] += double(r[c]) * double(z[c]);
-        }
-        blockSum<1>(a, S, rp);
-        rz = a[0];
-    }
-    FOR_CELLS(c) p[c] = z[c];
-    __syncthreads();
+            return vcycleT(S, rp, K);
+    };
+    double rz = precond();
+    pcgDirection(S, K, 0.0);
     for (int it = 0; it < maxIter; ++it) {
-        double a1[1] = {0.0};
-        FOR_CELLS(c) {
-            const T v = rowDotT(cellOf(C, c), M, p, nx);
-            Ap[c] = v;
-            a1[0] += double(p[c]) * double(v);
-        }
-        blockSum<1>(a1, S, rp);
-        const double pAp = a1[0];
+        const double pAp = pcgMatvec(S, rp, K);
         if (fabs(pAp) < 1e-30) {
             res.breakdown = true;
             break;
         }
-        const double alpha = rz / pAp;
-        double a2[1] = {0.0};
-        FOR_CELLS(c) {
-            x[c] += T(alpha) * p[c];
-            const T rc = r[c] - T(alpha) * Ap[c];
-            r[c] = rc;
-            a2[0] += double(rc) * double(rc);
-        }
-        blockSum<1>(a2, S, rp);
-        const double rn = sqrt(a2[0]);
+        const double rn = sqrt(pcgUpdate(S, rp, K, x, rz / pAp));
         res.iterations = it + 1;
         res.finalRes = rn / r0n;
         if (res.finalRes < tol) {
             res.converged = true;
             return res;
         }
-        double rzNew;
-        if (amg) {
-            if constexpr (F32Precond)
-                rzNew = precondF32();
-            else
-                rzNew = vcycleT(S, rp, K);
-        } else {
-            double a3[1] = {0.0};
-            FOR_CELLS(c) {
-                z[c] = r[c] * rdv[c];
-                a3[0] += double(r[c]) * double(z[c]);
-            }
-            blockSum<1>(a3, S, rp);
-            rzNew = a3[0];
-        }
-        const double beta = rzNew / (rz + 1e-30);
-        FOR_CELLS(c) p[c] = z[c] + T(beta) * p[c];
-        __syncthreads();
+        const double rzNew = precond();
+        pcgDirection(S, K, rzNew / (rz + 1e-30));
         rz = rzNew;
     }
     return res;
@@ -1031,7 +1113,7 @@ __device__ __forceinline__ LinRes solvePressure(Shared &S, int &rp, double *x, d
 struct Est {
     double rate, remaining;
 };
-__device__ Est estimate(const Shared &S, int e, int window, double negligible) {
+__device__ __forceinline__ Est estimate(const Shared &S, int e, int window, double negligible) {
     const int m = window < 2 ? 2 : window;
     const int cnt = S.cnt[e];
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
@@ -2002,14 +2084,27 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
     phInitFlux(S);
     __syncthreads();
 
-    bool established = job.warm != nullptr;
-    int amgNeed = 1, amgAfter = -1; // AMG coarse-value refresh state
-    double lastK = 1.0, lastW = 1.0;
-    const double tol = st.tol, negligible = 0.01 * tol;
-    double worst = inf, fluxRef = 0.0, n0x = 1, n0y = 1, n0p = 1;
-    int status = 1, finalIter = st.maxIter;
-    bool converged = false, diverged = false;
-    double rateU = __longlong_as_double(0x7ff8000000000000LL);
+    // the loop state lives in shared memory (LoopState); every thread writes the same
+    // values, and reads after its own writes
+    LoopState &Ls = S.L;
+    bool &established = Ls.established, &converged = Ls.converged, &diverged = Ls.diverged;
+    int &amgNeed = Ls.amgNeed, &amgAfter = Ls.amgAfter; // AMG coarse-value refresh state
+    double &lastK = Ls.lastK, &lastW = Ls.lastW;
+    double &worst = Ls.worst, &fluxRef = Ls.fluxRef, &n0x = Ls.n0x, &n0y = Ls.n0y, &n0p = Ls.n0p;
+    int &status = Ls.status, &finalIter = Ls.finalIter;
+    double &rateU = Ls.rateU;
+    established = job.warm != nullptr;
+    amgNeed = 1;
+    amgAfter = -1;
+    lastK = 1.0;
+    lastW = 1.0;
+    worst = inf;
+    fluxRef = 0.0;
+    n0x = n0y = n0p = 1.0;
+    status = 1;
+    finalIter = st.maxIter;
+    converged = diverged = false;
+    rateU = __longlong_as_double(0x7ff8000000000000LL);
 
 
     for (int iter = 0; iter < st.maxIter; ++iter) {
@@ -2031,8 +2126,8 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
 
         mark(S, 1);
         // ---- momentum x then y (assembleMomentum :303-482)
-        LinRes resU[2];
-        double momRes = 0.0, momScale = 0.0;
+        LinRes *resU = Ls.resU;
+        double &momRes = Ls.momRes, &momScale = Ls.momScale;
         for (int comp = 0; comp < 2; ++comp) {
             if (comp == 1) { // gradients of the updated Ux for the y assembly
                 phGradU(S);
@@ -2059,11 +2154,12 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         double pacc[3] = {0.0, 0.0, fs[0]};
         phPressureCells(S, pacc);
         blockSum<3>(pacc, S, rp);
-        const double contScaled = pacc[0] / dmax(pacc[2], 1e-300);
-        const double fluxScale = pacc[2];
+        Ls.contScaled = pacc[0] / dmax(pacc[2], 1e-300);
+        Ls.fluxScale = pacc[2];
         mark(S, 3);
-        LinRes resP = solvePressure(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol,
-                                    st.pSolver, amgNeed, amgAfter);
+        LinRes &resP = Ls.resP;
+        resP = solvePressure(S, rp, W.pp, sqrt(pacc[1]), st.innerIter, st.innerTol, st.pSolver,
+                             amgNeed, amgAfter);
         if (threadIdx.x == 0)
             S.innerPressure += resP.iterations;
         __syncthreads();
@@ -2076,7 +2172,9 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         __syncthreads();
 
         // ---- turbulence (:1476-1538)
-        LinRes resK{0, 0, 0, true}, resW{0, 0, 0, true};
+        LinRes &resK = Ls.resK, &resW = Ls.resW;
+        resK = LinRes{0, 0, 0, true};
+        resW = LinRes{0, 0, 0, true};
         if (turbUpdate) {
             phTurbGradK(S);
             __syncthreads();
@@ -2117,22 +2215,11 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             lastK = mx[2] / mx[0];
             lastW = mx[3] / mx[1];
         }
-        double e[11];
-        e[0] = iter;
-        e[1] = resU[0].initialRes;
-        e[2] = resU[1].initialRes;
-        e[3] = 0.0;
-        e[4] = resP.initialRes;
-        e[5] = turbActive ? lastK : 0.0;
-        e[6] = turbActive ? lastW : 0.0;
-        e[7] = momRes / dmax(momScale, 1e-300);
-        e[8] = contScaled;
-        e[9] = mx[5] / mx[4];
-        e[10] = inf;
+        Ls.uChange = mx[5] / mx[4];
         // one barrier pair for every sample of this iteration (U, k, omega, monitor)
         __syncthreads();
         if (threadIdx.x == 0) {
-            S.ring[0][S.cnt[0] % kWindowCap] = e[9];
+            S.ring[0][S.cnt[0] % kWindowCap] = Ls.uChange;
             S.cnt[0] += 1;
             if (turbUpdate) {
                 S.ring[1][S.cnt[1] % kWindowCap] = lastK;
@@ -2171,14 +2258,28 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 S.haveQPrev = 1;
             __syncthreads();
         }
+        // the history entry of this iteration (ResidualEntry order); no phase call follows
+        const double tol = st.tol, negligible = 0.01 * tol;
+        double e[11];
+        e[0] = iter;
+        e[1] = resU[0].initialRes;
+        e[2] = resU[1].initialRes;
+        e[3] = 0.0;
+        e[4] = resP.initialRes;
+        e[5] = turbActive ? lastK : 0.0;
+        e[6] = turbActive ? lastW : 0.0;
+        e[7] = momRes / dmax(momScale, 1e-300);
+        e[8] = Ls.contScaled;
+        e[9] = Ls.uChange;
+        e[10] = inf;
         if (iter == 0) {
             n0x = dmax(e[1], 1e-30);
             n0y = dmax(e[2], 1e-30);
             n0p = dmax(e[4], 1e-30);
-            fluxRef = fluxScale;
+            fluxRef = Ls.fluxScale;
         } else if (iter < 50) {
             n0p = dmax(n0p, e[4]);
-            fluxRef = dmax(fluxRef, fluxScale);
+            fluxRef = dmax(fluxRef, Ls.fluxScale);
         }
         auto safe = [](double v, double ref) { return ref < 1e-20 ? 0.0 : v / ref; };
         const double nm = dmax(n0x, n0y);
@@ -2204,6 +2305,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         const bool divergingNow = isnan(maxRes) || isinf(maxRes) || maxRes > st.divLimit;
         const bool needEst = cheap < tol || iter == st.maxIter - 1 || divergingNow ||
                              (job.hist && iter < job.histCap);
+        double w;
         if (needEst) {
             const Est eU = estimate(S, 0, st.window, negligible);
             e[10] = eU.remaining;
@@ -2212,7 +2314,6 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             wv = dmax(wv, e[8]);
             wv = dmax(wv, e[9]);
             wv = dmax(wv, e[10]);
-            worst = wv;
             if (turbActive) {
                 const Est eK = estimate(S, 1, st.window, negligible);
                 const Est eW = estimate(S, 2, st.window, negligible);
@@ -2220,26 +2321,24 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                 wv = dmax(wv, eK.remaining);
                 wv = dmax(wv, lastW);
                 wv = dmax(wv, eW.remaining);
-                worst = wv;
             }
             if (haveMonitor) {
                 const Est eQ = estimate(S, 3, st.window, negligible);
                 wv = dmax(wv, qLast);
                 wv = dmax(wv, eQ.remaining);
-                worst = wv;
             }
-            if (!isfinite(worst))
-                worst = inf;
+            w = isfinite(wv) ? wv : inf;
         } else {
-            worst = cheap; // >= tol: not a verdict iteration
+            w = cheap; // >= tol: not a verdict iteration
         }
         if (job.hist && iter < job.histCap && threadIdx.x == 0)
             for (int t = 0; t < 11; ++t)
                 job.hist[11L * iter + t] = e[t];
         if (bad)
-            worst = inf;
+            w = inf;
+        worst = w;
         const bool turbScheduled = st.turbStart < st.maxIter;
-        if (worst < tol && iter > 0 && (!turbScheduled || (turbActive && established))) {
+        if (w < tol && iter > 0 && (!turbScheduled || (turbActive && established))) {
             converged = true;
             finalIter = iter;
             status = 0;
@@ -2400,9 +2499,11 @@ __global__ void __launch_bounds__(NT) solveKernel(const DevJob *jobs, int njobs,
 // once h < published, by a compare-and-swap on the device-side head, so no
 // ticket is ever held for an unpublished request. A CTA leaves when the host
 // closes the queue and nothing is left, or after idleNs without work (the host
-// relaunches if requests arrive later); closed = 2 cancels the requests not yet
-// claimed (solves in flight still finish). Results go straight to host-mapped
-// rows; the request's done flag is raised after a system-scope fence.
+// launches more CTAs when requests wait and fewer than the slots run); closed = 2
+// cancels the requests not yet claimed (solves in flight still finish). A request
+// solves in its own pool region when it carries one (DevJob::ws), else in the CTA's
+// slot workspace. Results go straight to host-mapped rows; the request's done flag
+// is raised after a system-scope fence; every CTA counts its exit.
 template <int NT>
 __global__ void __launch_bounds__(NT) serveKernel(ServeQueue q, double *wsBase, long wsStride,
                                                   int arenaDoubles) {
@@ -2431,10 +2532,8 @@ __global__ void __launch_bounds__(NT) serveKernel(ServeQueue q, double *wsBase, 
                 }
                 if (closed) // closed and drained
                     break;
-                if (globalNs() - idleFrom > q.idleNs) {
-                    atomicAdd(q.idleExits, 1);
+                if (globalNs() - idleFrom > q.idleNs) // idle: leave (the host tops up)
                     break;
-                }
                 __nanosleep(4000);
             }
             S.job = got;
@@ -2445,13 +2544,15 @@ __global__ void __launch_bounds__(NT) serveKernel(ServeQueue q, double *wsBase, 
         const int j = S.job;
         if (j < 0)
             break;
-        runJob(S, S.jd, ws, arena, arenaDoubles);
+        runJob(S, S.jd, S.jd.ws ? S.jd.ws : ws, arena, arenaDoubles);
         __threadfence_system();
         __syncthreads();
         if (threadIdx.x == 0)
             asm volatile("st.release.sys.global.s32 [%0], %1;" ::"l"(q.done + j), "r"(1) : "memory");
         __syncthreads();
     }
+    if (threadIdx.x == 0) // counted so the host can tell how many CTAs still run
+        atomicAdd(q.exits, 1);
 }
 
 // ---------------------------------------------------------------- allocation-free single solve

@@ -33,10 +33,17 @@ UNIT = "solves/s"
 # (CPU pilot of the compiled reference); used only by the CPU arm's extrapolation
 REF_ITERS = (12460, 58690, 258900)
 BYTES_OUTER, BYTES_KRYLOV, BYTES_PRESSURE = 1600, 360, 400  # algorithmic B/cell (FP64)
-# DRAM bytes (read + write) of one 1536-cell draw as ncu counted them over a
-# 600-iteration solve with 768-thread CTAs: the first touch of the mesh class and the
-# workspace; later iterations hit L2, so the figure does not grow with iterations
-DRAM_BYTES_PER_DRAW_1536 = 1_236_992 + 2_048
+# From one ncu capture of solveKernel<768> solving one 1536-cell draw for 600 outer
+# iterations (profiles/solveKernel768_1536cells_full_ncu.md):
+# * DRAM bytes (read + write): the first touch of the mesh class and the workspace;
+#   later iterations hit L2, so the figure does not grow with the iteration count;
+# * L2 bytes (lts__t_sectors x 32 B) per outer iteration: what the solve moves
+#   between its SM and L2 (L1 misses, spills, stores);
+# * the L2's peak: 3 sectors per cycle on each of the 184 slices (ncu's
+#   lts__t_sectors peak_sustained) x 32 B at the 1965 MHz clock.
+DRAM_BYTES_PER_DRAW_1536 = 2_215_168 + 1_280
+L2_BYTES_PER_ITER_1536 = 303_402_369 * 32 / 600
+L2_PEAK_GBS = 3 * 32 * 184 * 1.965
 
 
 def parse():
@@ -57,7 +64,8 @@ def parse():
                     help="ensemble: the 256-draw channel ensemble (headline); linear: 512 "
                          "variable-coefficient Poisson systems by AMG-PCG; serve: open-loop "
                          "Poisson arrivals of channel requests to the serving loop")
-    ap.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
+    ap.add_argument("--rate", default="200,500,1000,2000",
+                    help="serve: arrivals per second (a comma list runs one stream per rate)")
     ap.add_argument("--requests", type=int, default=96, help="serve: requests in the stream")
     ap.add_argument("--systems", type=int, default=512)
     ap.add_argument("--cpu-sample-systems", type=int, default=12)
@@ -435,6 +443,10 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
         dur = (clock[sel, 1].max() - clock[sel, 0].min()) / 1e9
         per_class.append((dur, float(np.sum(work[sel])), c))
     dom_s, dom_bytes, dom_c = max(per_class)
+    dom_sel = cls == dom_c
+    is1536 = int(np.max(cells[dom_sel])) == 1536
+    dram = DRAM_BYTES_PER_DRAW_1536 * int(np.sum(dom_sel)) if is1536 else None
+    l2 = L2_BYTES_PER_ITER_1536 * float(np.sum(iters[dom_sel])) if is1536 else None
     names = ["setup", "closure", "momentum", "p_assembly", "p_solve", "amg_refresh", "turbulence",
              "bookkeeping"]
     stages = {}
@@ -482,17 +494,23 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": len(per_class) * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm,
-                     "traffic": (DRAM_BYTES_PER_DRAW_1536 * int(np.sum(cls == dom_c))
-                                 if int(np.max(cells[cls == dom_c])) == 1536 else None),
-                     "traffic_note": "ncu DRAM read+write of one 1536-cell draw (first touch; "
-                                     "constant in the iteration count) x draws in the launch",
+                     "frac": achieved / hbm, "algorithmic_frac": achieved / hbm,
+                     "traffic": dram, "dram_frac": (dram / dom_s / 1e9 / hbm) if dram else None,
+                     "l2_bytes": l2, "l2_gbs": (l2 / dom_s / 1e9) if l2 else None,
+                     "l2_peak_gbs": L2_PEAK_GBS,
+                     "l2_frac": (l2 / dom_s / 1e9 / L2_PEAK_GBS) if l2 else None,
+                     "traffic_note": "DRAM: ncu read+write of one 1536-cell draw (first touch; "
+                                     "constant in the iteration count) x draws in the launch; "
+                                     "L2: ncu L2 bytes per outer iteration of a 1536-cell draw x "
+                                     "the launch's outer iterations",
                      "peak_source": "measured" if "gpu_name" in peaks else "fallback",
                      "kernel": f"solveKernel, Re_tau class {dom_c} ({int(np.sum(cls == dom_c))} rows)",
                      "kernel_ms": dom_s * 1e3, "step_bytes_per_s": alg_bytes / (ms / 1e3),
-                     "note": "algorithmic FP64 bytes (1600 B/cell/outer + 360 B/cell/Krylov it + "
-                             "400 B/cell/pressure it); the state is SMEM/L2 resident, so the "
-                             "bound in practice is per-phase latency, not HBM"},
+                     "note": "frac = algorithmic_frac: algorithmic FP64 bytes (1600 B/cell/outer "
+                             "+ 360 B/cell/Krylov it + 400 B/cell/pressure it) / time / HBM peak, "
+                             "a rate of on-chip work, not HBM use: the state lives in shared "
+                             "memory, L1 and L2 (dram_frac), and the bound in practice is the "
+                             "latency of the dependent phases of each outer iteration"},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -667,23 +685,33 @@ def student_t_theta(ids, seed=20261012, center=(0.324, 0.0968), std=(0.004, 0.00
     return np.array(out)
 
 
-def serve_arm(args):
-    import torch
-    import rans_uq_b200 as rq
-    import rans_uq_b200.workloads as wl
+SERVE_BUMP_SIZES = ((100, 50), (200, 100), (400, 200))
+SERVE_BUMP_CAP = 200
 
-    if int(os.environ.get("RANK", "0")) != 0:
-        return
-    torch.cuda.set_device(0)
-    ens = wl.channel_ensemble(3)
-    R = args.requests
-    rng = np.random.default_rng(20261013)
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, R))
-    cls = rng.integers(0, 3, R)
-    theta = student_t_theta(range(R))
-    poisoned = rng.random(R) < 0.05
-    theta[poisoned, 0] = 0.95  # a1 above its bound: must come back flagged, not returned
-    srv = rq.ForwardServer(ens.batches, capacity=R, idle_timeout=10.0)
+
+def serve_stream(n, seed=20261013):
+    """The request mix of one stream: 70 % channel (Re_tau 182 / 550 / 1000 equally) and
+    30 % bump-wall (100 x 50, 200 x 100, 400 x 200 equally; capped at 200 outer
+    iterations, so they come back flagged Unconverged); theta from the Student-t
+    proposal; 5 % poisoned, half out of bounds (a1 = 0.95: InvalidParameters) and half
+    in bounds but far from the box ((a1, beta*) = (0.1, 0.2), which does not converge).
+    Returns (class index per request: 0-2 channel, 3-5 bump; theta; poisoned mask)."""
+    rng = np.random.default_rng(seed)
+    bump = rng.random(n) < 0.30
+    cls = np.where(bump, 3 + rng.integers(0, 3, n), rng.integers(0, 3, n))
+    theta = student_t_theta(range(n))
+    poisoned = rng.random(n) < 0.05
+    far = poisoned & (rng.random(n) < 0.5)
+    theta[poisoned & ~far, 0] = 0.95
+    theta[far] = (0.1, 0.2)
+    return cls, theta, poisoned
+
+
+def serve_one_rate(rq, batches, rate, R, seed):
+    cls, theta, poisoned = serve_stream(R, seed)
+    rng = np.random.default_rng(seed + 1)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, R))
+    srv = rq.ForwardServer(batches, capacity=R, idle_timeout=10.0)
     done_at = np.full(R, np.nan)
     results = [None] * R
     tickets = []
@@ -697,43 +725,74 @@ def serve_arm(args):
                     results[k] = r
                     done_at[k] = time.perf_counter() - t0
 
-    with Clocks(0) as clk:
-        for i in range(R):
-            while time.perf_counter() - t0 < arrivals[i]:
-                poll_all()
-                time.sleep(2e-4)
-            tickets.append(srv.submit(int(cls[i]), theta[i]))
-        while any(r is None for r in results):
+    for i in range(R):
+        while time.perf_counter() - t0 < arrivals[i]:
             poll_all()
-            time.sleep(1e-3)
-            if time.perf_counter() - t0 > 3600:
-                break
+            time.sleep(2e-4)
+        tickets.append(srv.submit(int(cls[i]), theta[i]))
+    while any(r is None for r in results):
+        poll_all()
+        time.sleep(1e-3)
+        if time.perf_counter() - t0 > 3600:
+            break
     span = float(np.nanmax(done_at))
-    info = srv.info()
+    info, mem = srv.info(), srv.memory()
     srv.destroy()
     lat = done_at - arrivals
     status = np.array([int(r.status) for r in results])
-    conv = int(np.sum(status == 0))
-    flagged_poison = int(sum(1 for k in range(R) if poisoned[k] and results[k].flagged))
+    conv = status == 0
     service = np.array([(r.end_ns - r.start_ns) / 1e9 for r in results])
-    print(json.dumps({
-        "metric": SERVE_METRIC, "value": conv / span, "unit": "solves/s", "n_gpus": 1,
-        "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{R} channel requests (Re_tau 182/550/1000 equally), Student-t "
-                               "theta (nu 4, centre 0.324/0.0968), 5% out of bounds",
-                   "rate_per_s": args.rate, "slots": info["slots"]},
-        "requests": R, "converged": conv, "poisoned": int(poisoned.sum()),
-        "poisoned_flagged": flagged_poison,
+    return {
+        "rate_per_s": rate, "requests": R, "converged": int(conv.sum()),
+        "converged_per_s": float(conv.sum() / span), "span_s": span,
+        "poisoned": int(poisoned.sum()),
+        "poisoned_flagged": int(sum(1 for k in range(R) if poisoned[k] and results[k].flagged)),
+        "returned_poisoned": int(sum(1 for k in range(R) if poisoned[k] and
+                                     results[k].predictions is not None)),
         "statuses": {s: int(np.sum(status == k)) for k, s in
                      enumerate(["converged", "unconverged", "diverged", "invalid", "unknown"])},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                      "max": float(lat.max()),
-                      "note": "host clock: scheduled arrival to result seen by poll"},
+                      "max": float(lat.max())},
+        "latency_converged_s": ({"p50": float(np.percentile(lat[conv], 50)),
+                                 "p99": float(np.percentile(lat[conv], 99))} if conv.any() else None),
         "service_s": {"p50": float(np.percentile(service, 50)),
                       "p99": float(np.percentile(service, 99))},
-        "span_s": span, "kernel_launches": info["launches"], "clocks": clk.summary(),
-    }))
+        "slots": info["slots"], "kernel_launches": info["launches"],
+        "pool_bytes": mem["pool_bytes"]}
+
+
+def serve_arm(args):
+    """Open-loop Poisson arrivals of the mixed stream (serve_stream) to the serving
+    loop, one stream per rate, each on a fresh server over the same six mesh classes."""
+    import torch
+    import rans_uq_b200 as rq
+    import rans_uq_b200.workloads as wl
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    torch.cuda.set_device(0)
+    ens = wl.channel_ensemble(3)
+    bumps = [wl.bump_batch(nx, ny, max_iter=SERVE_BUMP_CAP) for nx, ny in SERVE_BUMP_SIZES]
+    batches = ens.batches + bumps
+    rates = [float(r) for r in str(args.rate).split(",")]
+    per_rate = []
+    with Clocks(0) as clk:
+        for k, rate in enumerate(rates):
+            per_rate.append(serve_one_rate(rq, batches, rate, args.requests, 20261013 + k))
+            print(f"serve: rate {rate}: {json.dumps(per_rate[-1])}", file=sys.stderr, flush=True)
+    top = per_rate[-1]
+    print(json.dumps({
+        "metric": SERVE_METRIC, "value": top["converged_per_s"], "unit": "solves/s", "n_gpus": 1,
+        "steps": len(rates), "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.requests} requests per rate: 70 % channel (Re_tau "
+                               "182/550/1000), 30 % bump-wall (100x50, 200x100, 400x200, capped at "
+                               f"{SERVE_BUMP_CAP} outer iterations); Student-t theta (nu 4, centre "
+                               "0.324/0.0968); 5 % poisoned (half out of bounds, half far off)",
+                   "rates_per_s": rates},
+        "per_rate": per_rate, "clocks": clk.summary(),
+        "note": "value = converged solves/s over the stream's span at the highest rate; "
+                "latency = scheduled arrival to result seen by poll (host clock)"}))
 
 
 # ---------------------------------------------------------------- bump-wall workload

@@ -159,6 +159,10 @@ int rq_problem_destroy(rq_problem *p);
 int rq_problem_info(const rq_problem *p, int32_t *n_cells, int32_t *n_obs, int32_t *n_active,
                     int32_t *amg_levels);
 
+/* Device workspace one solve of this mesh class uses (a batch CTA's slot, a serving
+   request's pool region), in bytes. */
+int rq_problem_workspace_bytes(const rq_problem *p, uint64_t *bytes);
+
 /* Launch shape of a mesh class: the CTA size of its solves and the shared-memory
    arena each CTA places the solve's hottest arrays in. */
 typedef struct rq_launch_shape {
@@ -292,17 +296,28 @@ int rq_posterior_weights_device(const double *loglik_dev, const double *log_q_de
 
 /* ---- serving loop (no reference counterpart: the reference evaluates fixed
    batches only, ForwardBatch.hpp:52-124). A server owns a persistent kernel whose
-   CTAs claim requests as they are submitted, in submission order, each on its own
-   solve slot (per-CTA workspace); a slot is reused as soon as its solve retires.
-   Slots = min(SMs x resident CTAs, max_slots if > 0, what 80% of free device memory
-   holds). Requests and results live in pinned host memory mapped into the device,
-   so a request needs no copy and a result is visible to rq_server_poll as soon as
-   its done flag is raised. The problems must outlive the server. CTAs leave after
-   idle_timeout_s without requests; submit / poll / wait relaunch them when needed.
-   capacity bounds the requests over the server's lifetime. */
+   CTAs (slots = min(SMs x resident CTAs, max_slots if > 0)) claim requests in
+   submission order as they are admitted; a CTA takes the next request as soon as
+   its solve retires. Each admitted request solves in its own region of a device
+   workspace pool sized for its mesh class; a request is admitted once its region
+   fits in the pool (in submission order) and its region returns to the pool when
+   its solve retires, so admission follows free memory as solves come and go.
+   Requests and results live in pinned host memory mapped into the device, so a
+   request needs no copy and a result is visible to rq_server_poll as soon as its
+   done flag is raised. The problems must outlive the server. CTAs leave after
+   idle_timeout_s without requests; submit / poll / wait launch more CTAs beside
+   the ones still running whenever admitted requests wait and fewer CTAs than slots
+   run. capacity bounds the requests over the server's lifetime. rq_server_create
+   sizes the pool at 80 % of the free device memory (at most what the slots can use
+   at once). */
 typedef struct rq_server rq_server;
 int rq_server_create(rq_problem *const *problems, int32_t n_problems, int32_t capacity,
                      double idle_timeout_s, int32_t max_slots, rq_server **out);
+/* The same with the workspace pool's size given (pool_bytes 0 = the default above);
+   RQ_E_OOM when it cannot hold one solve of the largest class. */
+int rq_server_create_pooled(rq_problem *const *problems, int32_t n_problems, int32_t capacity,
+                            double idle_timeout_s, int32_t max_slots, uint64_t pool_bytes,
+                            rq_server **out);
 /* theta: the problem's n_active values (host, copied). ticket: request index. */
 int rq_server_submit(rq_server *s, int32_t problem, const double *theta, int64_t *ticket);
 /* done = 1 once the request's row, predictions and clock record (12 int64, as
@@ -315,6 +330,10 @@ int rq_server_wait(rq_server *s, double timeout_s, int64_t *completed);
 int rq_server_close(rq_server *s);
 int rq_server_info(rq_server *s, int32_t *slots, int64_t *submitted, int64_t *completed,
                    int32_t *launches);
+/* The pool: its bytes, the bytes held by admitted requests whose solves have not
+   retired, requests submitted but not yet admitted, and CTAs running now. */
+int rq_server_memory(rq_server *s, uint64_t *pool_bytes, uint64_t *in_use_bytes,
+                     int64_t *waiting, int32_t *running_ctas);
 /* Cancels requests not yet claimed, waits for the solves in flight, frees. */
 int rq_server_destroy(rq_server *s);
 

@@ -53,6 +53,12 @@ def test_summary_has_contract_keys():
     want = 4 * 1536 * (1600 * 400 + 360 * 4000 + 400 * 2000) / 4e-3 / 1e9
     assert abs(out["roofline"]["achieved"] - want) < 1e-9 * want
     assert out["roofline"]["peak"] == 6552.3
+    r = out["roofline"]
+    assert r["algorithmic_frac"] == r["frac"]
+    # DRAM: first touch per 1536-cell draw x 4 draws; L2: bytes per iteration x 4 x 400
+    assert r["traffic"] == bench.DRAM_BYTES_PER_DRAW_1536 * 4
+    assert abs(r["l2_bytes"] - bench.L2_BYTES_PER_ITER_1536 * 1600) < 1e-6 * r["l2_bytes"]
+    assert abs(r["l2_frac"] - r["l2_bytes"] / 4e-3 / 1e9 / bench.L2_PEAK_GBS) < 1e-12
     assert abs(out["latency_ms"]["max"] - 4.0) < 1e-12
     assert out["plain_fp64"]["solves_per_s"] > 0 and out["batched_vs_plain"] > 0
 

@@ -83,9 +83,10 @@ def test_converged_bump_100x50_matches_reference(rq, solver, key):
     oracle/_ref), with the AMG and with the BiCGSTAB pressure solver. The converged
     state is the fixed point of the discrete equations, independent of how the inner
     solves got there, so both are held to the converged-parity tolerance: identical
-    verdict, predictions and the Ux, Uy, p, omega fields within 1e-10 of the field's
-    max-norm (k within 1e-8); outer iterations within 2 %. (After a few iterations the
-    BiCGSTAB trajectories of two implementations differ at 1e-3; the converged states
+    verdict, predictions and the Ux, Uy, omega fields within 1e-10 of the field's
+    max-norm, the pressure's deviation from its mean likewise (its level is arbitrary
+    on the periodic domain), k within 1e-8; outer iterations within 2 %. (After a few
+    iterations the BiCGSTAB trajectories of two implementations differ at 1e-3; the converged states
     do not.) About a GPU minute each."""
     g = np.load(cases.__file__.replace("cases.py", "golden/bump_100x50_ref.npz"))
     case = cases.bump_case(100, 50, tol=1e-8, max_iter=30000)
@@ -100,6 +101,10 @@ def test_converged_bump_100x50_matches_reference(rq, solver, key):
     for name, tol in (("Ux", 1e-10), ("Uy", 1e-10), ("p", 1e-10), ("omega", 1e-10),
                       ("k", 1e-8)):
         i = ck.FIELD_NAMES.index(name)
-        want = g[f"{key}_{name}"]
-        err = np.max(np.abs(fields[0, i] - want)) / max(np.max(np.abs(want)), 1e-300)
+        got, want = fields[0, i], g[f"{key}_{name}"]
+        if name == "p":
+            # the periodic pressure is defined up to a constant (the p' pin only anchors
+            # corrections): compare the deviation from the mean, against its own size
+            got, want = got - got.mean(), want - want.mean()
+        err = np.max(np.abs(got - want)) / max(np.max(np.abs(want)), 1e-300)
         assert err < tol, (name, err)

@@ -130,3 +130,53 @@ def test_served_far_off_draws_get_the_reference_verdicts(rq):
         else:
             assert s.iterations == r["iterations"] == g["cap"]
             assert s.flagged and s.predictions is None
+
+
+def test_admission_by_pool_space(rq):
+    """A workspace pool that holds two solves of the class: six requests submitted at
+    once are admitted two at a time, in submission order, as earlier solves retire and
+    return their regions; at no moment do more than two solves run, every result
+    equals the same request evaluated alone, and the pool is empty at the end."""
+    batch = cases.product_batch(rq, cases.small_channel(max_iter=3000))
+    ws = batch._problem.workspace_bytes()
+    pool = 2 * ((ws + 255) // 256 * 256)
+    srv = rq.ForwardServer([batch], capacity=16, idle_timeout=5.0, pool_bytes=pool)
+    theta = np.column_stack([np.linspace(0.29, 0.33, 6), np.linspace(0.086, 0.094, 6)])
+    tickets = [srv.submit(0, t) for t in theta]
+    mem = srv.memory()
+    assert mem["pool_bytes"] == pool
+    assert mem["waiting"] >= 3 and mem["in_use_bytes"] <= pool
+    assert srv.wait(600.0) == len(tickets)
+    served = [srv.poll(t) for t in tickets]
+    mem = srv.memory()
+    srv.destroy()
+    assert mem["waiting"] == 0 and mem["in_use_bytes"] == 0
+    ref = alone([batch], [0] * 6, theta)
+    for s, r in zip(served, ref):
+        check_same(s, r)
+    # never more than two solves at once, and starts follow submission order
+    ev = sorted([(s.start_ns, 1) for s in served] + [(s.end_ns, -1) for s in served])
+    live, peak = 0, 0
+    for _, d in ev:
+        live += d
+        peak = max(peak, live)
+    assert peak <= 2
+
+
+def test_top_up_while_a_long_solve_runs(rq):
+    """CTAs that leave after the idle timeout while another CTA is still in a long
+    solve are replaced beside it: a request submitted then starts before the long
+    solve ends, instead of waiting for the whole kernel to finish."""
+    long_batch = cases.product_batch(rq, cases.small_channel(max_iter=60000, tol=1e-14))
+    short_batch = cases.product_batch(rq, cases.small_channel(max_iter=200))
+    srv = rq.ForwardServer([long_batch, short_batch], capacity=8, idle_timeout=0.2)
+    t_long = srv.submit(0, (0.31, 0.09))
+    time.sleep(1.5)  # every other CTA leaves after 0.2 s without requests
+    t_short = srv.submit(1, (0.30, 0.088))
+    assert srv.wait(600.0) == 2
+    r_long, r_short = srv.poll(t_long), srv.poll(t_short)
+    info = srv.info()
+    srv.destroy()
+    assert info["launches"] >= 2
+    assert r_short.start_ns < r_long.end_ns
+    assert r_short.end_ns < r_long.end_ns
