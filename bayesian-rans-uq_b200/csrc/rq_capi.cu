@@ -259,7 +259,7 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     if (L > rq::kMaxLevels)
         throw RqError(RQ_E_UNSUPPORTED, "AMG hierarchy deeper than 12 levels");
     if (h.coarseN() > rq::kMaxCoarse)
-        throw RqError(RQ_E_UNSUPPORTED, "coarsest AMG level above 64 rows");
+        throw RqError(RQ_E_UNSUPPORTED, "coarsest AMG level above 128 rows");
     C.nlev = L;
     // ELL slots of levels >= 1: CSR entry k of row i -> (k - ptr[i]) * n + i
     std::vector<std::vector<int>> slotOf(L), entryOf(L);

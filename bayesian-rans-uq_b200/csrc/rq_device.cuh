@@ -9,7 +9,7 @@
 namespace rq {
 
 constexpr int kMaxLevels = 12;    // AMG levels (the reference allows 20; meshes here need <= 8)
-constexpr int kMaxCoarse = 64;    // rows of the dense coarsest AMG level
+constexpr int kMaxCoarse = 128;   // rows of the dense coarsest AMG level
 constexpr int kMaxProbes = 64;    // observations per problem
 constexpr int kWindowCap = 64;    // 2 * convergenceWindow samples kept per estimator
 

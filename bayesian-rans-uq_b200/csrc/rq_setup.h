@@ -80,10 +80,11 @@ struct AmgHost {
     int coarseN() const { return lev.back().n; }
     size_t coarseNnz() const { return lev.size() > 1 ? lev.back().col.size() : 0; }
 };
-// Coarsening stops at <= 64 rows (the reference stops at 50): a dense inverse of
-// up to 64 rows costs less per V-cycle than the two levels below it (measured 7 %
-// per outer iteration at 768 and 1536 cells).
-AmgHost buildAmg(const StructMesh &m, int minCoarse = 64, int maxLevels = 20);
+// Coarsening stops at <= 96 rows (the reference stops at 50): a dense inverse of up
+// to 96 rows, applied with several threads per row, costs less per V-cycle than the
+// level below it (each coarse level is two barrier-separated phases down and two up,
+// about 14k cycles per V-cycle at 1536 cells).
+AmgHost buildAmg(const StructMesh &m, int minCoarse = 96, int maxLevels = 20);
 // Smoothing weight of the prolongation, as a fraction of 1 / rho(D_F^-1 F): 0.85
 // (PCG on pressure systems taken from Re_tau 182-1000 channel solves needs 2-4
 // iterations with it; 1.15 and above lose the coarse correction).

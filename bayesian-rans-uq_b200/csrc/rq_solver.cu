@@ -277,7 +277,13 @@ __device__ __forceinline__ double jac(double r, double d) {
     return (fabs(d) > 1e-30) ? r / d : r; // jacobiPrecond, LinearSolver.hpp:173-177
 }
 
-#define FOR_CELLS(c) for (int c = threadIdx.x; c < n; c += blockDim.x)
+// The cells a thread owns in every per-cell sweep: c = thread, thread + threads, ...
+// (a warp's loads of one sweep cover whole cache lines; contiguous blocks of cells per
+// thread measured 12 % slower per outer iteration at 1536 cells). Every per-cell
+// loop of a solve uses this one assignment, so a thread may read its own writes of
+// an earlier loop without a barrier.
+#define FOR_OWN(c, count) for (int c = threadIdx.x; c < (count); c += blockDim.x)
+#define FOR_CELLS(c) FOR_OWN(c, n)
 
 // ---------------------------------------------------------------- inner linear solvers
 // The Krylov and AMG routines are templated on the value type T of their
@@ -418,7 +424,7 @@ template <typename T> __device__ __forceinline__ T level0EntryT(const KW<T> &K, 
 // Galerkin values of every coarse level from the current pressure system, the
 // reciprocal diagonals of the smoothed levels, then the inverse of the coarsest
 // level (Gauss-Jordan, SPD: no pivoting): in place by one warp, one row per lane,
-// when it has at most 32 rows; above that (up to 64) by the whole CTA, one
+// when it has at most 32 rows; above that (up to 128) by the whole CTA, one
 // barrier per pivot, ping-ponging [A | I] between two workspace buffers. (One warp
 // with two rows per lane was measured 17 % slower per outer iteration at 1536
 // cells: 128 dependent updates per lane and pivot against 16 per thread.) The
@@ -453,7 +459,7 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
             rdl[i] = T(1) / val[__ldg(Lv.diagPos + i)];
     }
     const DevAmgLevel &Q = C.lev[L - 1];
-    const int m = Q.n; // at most kMaxCoarse = 64 rows (the set-up rejects more)
+    const int m = Q.n; // at most kMaxCoarse = 128 rows (the set-up rejects more)
     const T *qv = K.amgVal + Q.valOff;
     if (m <= 32) {
         double *a = S.coarse;
@@ -669,19 +675,19 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const DevAmgLevel &Lv = C.lev[l];
         const int n = Lv.n;
         if (l == 0) {
-            for (int i = t0; i < n; i += ts)
+            FOR_OWN(i, n)
                 Kxa[i] = om * Kr[i] * Krd[i];
             sync();
             const T *xs = Kxa;
             if (two) {
-                for (int i = t0; i < n; i += ts) {
+                FOR_OWN(i, n) {
                     const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
                     Kxb[i] = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
                 }
                 sync();
                 xs = Kxb;
             }
-            for (int i = t0; i < n; i += ts)
+            FOR_OWN(i, n)
                 Krr[i] = Kr[i] - rowDotT(cellOf(C, i), M, xs, nx);
             sync();
             return;
@@ -718,7 +724,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const int m = C.lev[l].n, m2 = 2 * m;
         T *b = vb(l), *xb = b + 2 * m;
         if (L == 1) {
-            for (int i = t0; i < m; i += ts)
+            FOR_OWN(i, m)
                 b[i] = Kr[i];
         } else {
             segPass<T>(m, [&](int i, int j, int seg) { return restrictPart(l, i, j, seg); },
@@ -798,7 +804,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         const T *xprev = two ? Kxb : Kxa;
         T *out = two ? Kxa : Kz;
         double part = 0.0;
-        for (int i = tid; i < n; i += nt) {
+        FOR_OWN(i, n) {
             const T xi = xprev[i] + al * prolong(0, i);
             const Cell q = cellOf(C, i);
             const int c = i;
@@ -816,7 +822,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         }
         if (two) {
             __syncthreads();
-            for (int i = tid; i < n; i += nt) {
+            FOR_OWN(i, n) {
                 const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
                 const T zi = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
                 Kz[i] = zi;
@@ -829,7 +835,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
     } else {
         const T *xb = vb(0) + 2 * C.lev[0].n;
         double part = 0.0;
-        for (int i = tid; i < n0; i += nt) {
+        FOR_OWN(i, n0) {
             Kz[i] = xb[i];
             part += double(Kr[i]) * double(xb[i]);
         }
@@ -900,22 +906,64 @@ template <typename T> __device__ __noinline__ void pcgDirection(Shared &S, const
     }
     __syncthreads();
 }
-// z = M^-1 r through the FP32 V-cycle of S.K32; returns (r, z) in FP64
-template <typename T> __device__ __noinline__ double pcgPrecondF32(Shared &S, int &rp, const KW<T> &K) {
+// x += alpha p, r -= alpha Ap; returns (r, r) and the sum of r (the mixed form's
+// deflation of the constant vector needs it)
+struct Two {
+    double a, b;
+};
+template <typename T>
+__device__ __noinline__ Two pcgUpdateSum(Shared &S, int &rp, const KW<T> &K, T *x, double alpha) {
+    const int n = S.C.n;
+    const T *p = K.pv, *Ap = K.v;
+    T *r = K.r;
+    double a[2] = {0.0, 0.0};
+    FOR_CELLS(c) {
+        x[c] += T(alpha) * p[c];
+        const T rc = r[c] - T(alpha) * Ap[c];
+        r[c] = rc;
+        a[0] += double(rc) * double(rc);
+        a[1] += double(rc);
+    }
+    blockSum<2>(a, S, rp);
+    return Two{a[0], a[1]};
+}
+// the sum of r (the first residual of a solve)
+template <typename T> __device__ __noinline__ double sumOf(Shared &S, int &rp, const T *r) {
+    const int n = S.C.n;
+    double a[1] = {0.0};
+    FOR_CELLS(c) a[0] += double(r[c]);
+    blockSum<1>(a, S, rp);
+    return a[0];
+}
+
+// z = M^-1 r of the mixed form: the FP32 V-cycle of S.K32 with the constant vector 1
+// deflated in FP64. The pressure system is all-Neumann but for the pin of cell 0, so
+// A 1 = rowsum0 e_0 and 1 spans its near-null space; FP32 coarse values round each
+// coarse row sum (zero in exact arithmetic) by about 1e-7 of its diagonal, which is
+// comparable to that mode's eigenvalue and spoils its coarse correction. So the
+// constant mode is solved exactly in FP64 and the V-cycle sees only the rest
+// (balancing: M^-1 = Q + (I - Q A) V (I - A Q), Q = 1 (1' A 1)^-1 1', SPD when V is):
+//   r~ = r - (1'r) e_0,  y = V r~,  z = y + ((1'r) / rowsum0 - y_0) 1.
+// sumR = 1'r; returns (r, z) in FP64.
+template <typename T>
+__device__ __noinline__ double pcgPrecondF32(Shared &S, int &rp, const KW<T> &K, double sumR,
+                                             double rowsum0) {
     const int n = S.C.n;
     {
         const KW<float> &F = S.K32;
         const T *r = K.r;
-        FOR_CELLS(c) F.r[c] = float(r[c]);
+        FOR_CELLS(c) F.r[c] = float(c == 0 ? double(r[c]) - sumR : double(r[c]));
     }
-    vcycleT<float>(S, rp, S.K32);
+    vcycleT<float>(S, rp, S.K32); // ends with a block reduction: F.z is complete
     const KW<float> &F = S.K32;
+    const double shift = sumR / rowsum0 - double(F.z[0]);
     const T *r = K.r;
     T *z = K.z;
     double a[1] = {0.0};
     FOR_CELLS(c) {
-        z[c] = T(F.z[c]);
-        a[0] += double(r[c]) * double(z[c]);
+        const T zc = T(double(F.z[c]) + shift);
+        z[c] = zc;
+        a[0] += double(r[c]) * double(zc);
     }
     blockSum<1>(a, S, rp);
     return a[0];
@@ -968,11 +1016,21 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
     } else {
         __syncthreads();
     }
+    // the mixed form deflates the constant vector (pcgPrecondF32): the row sum of the
+    // pinned row and the running sum of r
+    double rowsum0 = 0.0, sumR = 0.0;
+    if constexpr (F32Precond) {
+        if (amg) {
+            rowsum0 = double(K.d[0]) + double(K.aW[0]) + double(K.aE[0]) + double(K.aS[0]) +
+                      double(K.aN[0]);
+            sumR = sumOf(S, rp, K.r);
+        }
+    }
     auto precond = [&]() {
         if (!amg)
             return pcgJacobi(S, rp, K);
         if constexpr (F32Precond)
-            return pcgPrecondF32(S, rp, K);
+            return pcgPrecondF32(S, rp, K, sumR, rowsum0);
         else
             return vcycleT(S, rp, K);
     };
@@ -984,7 +1042,15 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
             res.breakdown = true;
             break;
         }
-        const double rn = sqrt(pcgUpdate(S, rp, K, x, rz / pAp));
+        double rr2;
+        if constexpr (F32Precond) {
+            const Two u = pcgUpdateSum(S, rp, K, x, rz / pAp);
+            rr2 = u.a;
+            sumR = u.b;
+        } else {
+            rr2 = pcgUpdate(S, rp, K, x, rz / pAp);
+        }
+        const double rn = sqrt(rr2);
         res.iterations = it + 1;
         res.finalRes = rn / r0n;
         if (res.finalRes < tol) {

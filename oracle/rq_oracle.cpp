@@ -384,9 +384,9 @@ struct Amg {
 };
 
 // coarsening stops at this many rows: the reference stops at 50 (LinearSolver.hpp:664);
-// the pressure hierarchy at 64 (a dense inverse of up to 64 rows is cheaper than two
-// more levels), the standalone linear solves at 32
-static const int AMG_MIN_COARSE = 64;
+// the pressure hierarchy at 96 (a dense inverse of up to 96 rows is cheaper than the
+// level below it), the standalone linear solves at 32
+static const int AMG_MIN_COARSE = 96;
 static const int AMG_MIN_COARSE_LINEAR = 32;
 static const int AMG_MAX_LEVELS = 20;  // :663
 static const double AMG_PROLONG_WEIGHT = 0.85;
