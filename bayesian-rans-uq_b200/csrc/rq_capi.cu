@@ -358,7 +358,7 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
     // FP64 arrays, FP32 inner-solver copies (mixed form), faces, AMG, dense coarse
     C.wsDoubles = 43 * pad32(n) + 15 * pad32((n + 1) / 2) + pad32((valOff + 1) / 2) +
                   pad32((vecOff + 1) / 2) +
-                  4 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
+                  5 * pad32(nf) + pad32(valOff) + pad32(vecOff) + 2 * pad32(2 * mc * mc);
     // upload and patch pointers
     P.dDoubles.ensure(std::max<size_t>(D.size(), 1) * sizeof(double));
     P.dInts.ensure(std::max<size_t>(I.size(), 1) * sizeof(int32_t));

@@ -36,6 +36,7 @@ struct Work {
     double *Ux, *Uy, *p, *k, *w, *nuT, *F1, *F2, *Pk, *CD, *S;
     double *gUxx, *gUxy, *gUyx, *gUyy, *gKx, *gKy, *gWx, *gWy, *gPx, *gPy;
     double *phi, *phiOld, *phiPred, *pCoeff; // x faces [0,n) then y faces [n, n+nfy)
+    double *fScr;                            // face scratch of the transport assemblies
     double *d, *aW, *aE, *aS, *aN, *b, *aP, *aPraw;
     double *Uxp, *Uyp, *kOld, *wOld, *pp;
     double *r, *rh, *pv, *v, *s, *t, *ph, *sh;
@@ -557,44 +558,30 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
 }
 
 // Sum over the slots k = first, first + step, ... (< width) of one ELL row of
-// coef(k) * vec(col(k)) for columns >= 0, k ascending. The loads of four slots are
-// issued before their products are added (padding slots load entry 0 and add
-// nothing), so a wide row costs a few load latencies, not one per slot.
-template <typename T, typename C, typename V>
+// coef(k) * vec(col(k)) for columns >= 0, k ascending. The loads of up to eight slots
+// B slots are issued before their products are added (padding slots and slots past
+// the row add nothing), so a row of up to B slots per lane costs one column load and
+// one value load in sequence, not one pair per slot. The coarse operators (up to 15
+// slots a row) take B = 8, the transfers (2-4) B = 4.
+template <typename T, int B = 4, typename C, typename V>
 __device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V *vec, int width,
                                     int stride, int row, int first = 0, int step = 1) {
     T s = T(0);
-    int k = first;
-    for (; k + 3 * step < width; k += 4 * step) {
-        int c[4];
-        T v[4], x[4];
+    for (int k = first; k < width; k += B * step) {
+        int c[B];
+        T v[B], x[B];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            c[u] = __ldg(cols + (k + u * step) * stride + row);
+        for (int u = 0; u < B; ++u)
+            c[u] = (k + u * step < width) ? __ldg(cols + (k + u * step) * stride + row) : -1;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            v[u] = T(coef[(k + u * step) * stride + row]);
-            x[u] = T(vec[c[u] < 0 ? 0 : c[u]]);
+        for (int u = 0; u < B; ++u) {
+            v[u] = c[u] >= 0 ? T(coef[(k + u * step) * stride + row]) : T(0);
+            x[u] = c[u] >= 0 ? T(vec[c[u]]) : T(0);
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < B; ++u)
             if (c[u] >= 0)
                 s += v[u] * x[u];
-    }
-    if (k + step < width) {
-        const int c0 = __ldg(cols + k * stride + row), c1 = __ldg(cols + (k + step) * stride + row);
-        const T v0 = T(coef[k * stride + row]), v1 = T(coef[(k + step) * stride + row]);
-        const T x0 = T(vec[c0 < 0 ? 0 : c0]), x1 = T(vec[c1 < 0 ? 0 : c1]);
-        if (c0 >= 0)
-            s += v0 * x0;
-        if (c1 >= 0)
-            s += v1 * x1;
-        k += 2 * step;
-    }
-    if (k < width) {
-        const int c = __ldg(cols + k * stride + row);
-        if (c >= 0)
-            s += T(coef[k * stride + row]) * T(vec[c]);
     }
     return s;
 }
@@ -705,7 +692,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         if (two) {
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                           return ellDot<T, 8>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
@@ -713,7 +700,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         }
         segPass<T>(n,
                    [&](int i, int j, int seg) {
-                       return ellDot<T>(Lv.ecol, val, xs, Lv.width, n, i, j, seg);
+                       return ellDot<T, 8>(Lv.ecol, val, xs, Lv.width, n, i, j, seg);
                    },
                    [&](int i, T ax) { rr[i] = b[i] - ax; });
         sync();
@@ -767,7 +754,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             sync();
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T>(Lv.ecol, val, xi, Lv.width, n, i, j, seg);
+                           return ellDot<T, 8>(Lv.ecol, val, xi, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { out[i] = xi[i] + om * (b[i] - ax) * rd[i]; });
         } else {
@@ -786,7 +773,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         if (two) {
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                           return ellDot<T, 8>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
@@ -799,7 +786,37 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         up(l);
     const int tid = t0, nt = ts;
     double rz = 0.0;
-    if (L > 1) { // level 0: prolongation fused into the first post sweep (then the second)
+    if (L > 1 && C.lev[0].pw > 1) { // level 0, smoothed P: x = x_pre + alpha P x_c in a
+        // sweep of its own (into rr, free since the restriction to level 1), then the
+        // post sweep(s) read it (each x once, not re-formed at every neighbour)
+        const int n = C.lev[0].n;
+        const T *xprev = two ? Kxb : Kxa;
+        T *out = two ? Kxa : Kz;
+        FOR_OWN(i, n)
+            Krr[i] = xprev[i] + al * prolong(0, i);
+        __syncthreads();
+        double part = 0.0;
+        FOR_OWN(i, n) {
+            const T ax = rowDotT(cellOf(C, i), M, Krr, nx);
+            const T zi = Krr[i] + om * (Kr[i] - ax) * Krd[i];
+            out[i] = zi;
+            if (!two)
+                part += double(Kr[i]) * double(zi);
+        }
+        if (two) {
+            __syncthreads();
+            FOR_OWN(i, n) {
+                const T ax = rowDotT(cellOf(C, i), M, Kxa, nx);
+                const T zi = Kxa[i] + om * (Kr[i] - ax) * Krd[i];
+                Kz[i] = zi;
+                part += double(Kr[i]) * double(zi);
+            }
+        }
+        double a[1] = {part};
+        blockSum<1>(a, S, rp);
+        rz = a[0];
+    } else if (L > 1) { // level 0, piecewise-constant P: prolongation fused into the
+        // first post sweep (then the second)
         const int n = C.lev[0].n;
         const T *xprev = two ? Kxb : Kxa;
         T *out = two ? Kxa : Kz;
@@ -944,10 +961,11 @@ template <typename T> __device__ __noinline__ double sumOf(Shared &S, int &rp, c
 // constant mode is solved exactly in FP64 and the V-cycle sees only the rest
 // (balancing: M^-1 = Q + (I - Q A) V (I - A Q), Q = 1 (1' A 1)^-1 1', SPD when V is):
 //   r~ = r - (1'r) e_0,  y = V r~,  z = y + ((1'r) / rowsum0 - y_0) 1.
-// sumR = 1'r; returns (r, z) in FP64.
+// sumR = 1'r; returns (r, z) and (r, z_previous) in FP64 (the latter for the flexible
+// direction update: an FP32 V-cycle is symmetric only to its rounding).
 template <typename T>
-__device__ __noinline__ double pcgPrecondF32(Shared &S, int &rp, const KW<T> &K, double sumR,
-                                             double rowsum0) {
+__device__ __noinline__ Two pcgPrecondF32(Shared &S, int &rp, const KW<T> &K, double sumR,
+                                          double rowsum0) {
     const int n = S.C.n;
     {
         const KW<float> &F = S.K32;
@@ -959,14 +977,15 @@ __device__ __noinline__ double pcgPrecondF32(Shared &S, int &rp, const KW<T> &K,
     const double shift = sumR / rowsum0 - double(F.z[0]);
     const T *r = K.r;
     T *z = K.z;
-    double a[1] = {0.0};
+    double a[2] = {0.0, 0.0};
     FOR_CELLS(c) {
         const T zc = T(double(F.z[c]) + shift);
+        a[1] += double(r[c]) * double(z[c]);
         z[c] = zc;
         a[0] += double(r[c]) * double(zc);
     }
-    blockSum<1>(a, S, rp);
-    return a[0];
+    blockSum<2>(a, S, rp);
+    return Two{a[0], a[1]};
 }
 
 // PCG (LinearSolver.hpp:184-246 / :908-982) from x = 0 with the Jacobi or the AMG
@@ -1026,14 +1045,24 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
             sumR = sumOf(S, rp, K.r);
         }
     }
+    // (r, z) of the new preconditioned residual; rzPrev receives (r, z_previous) where
+    // the flexible update applies (the FP32 V-cycle), else 0
+    double rzPrev = 0.0;
     auto precond = [&]() {
         if (!amg)
             return pcgJacobi(S, rp, K);
-        if constexpr (F32Precond)
-            return pcgPrecondF32(S, rp, K, sumR, rowsum0);
-        else
+        if constexpr (F32Precond) {
+            const Two u = pcgPrecondF32(S, rp, K, sumR, rowsum0);
+            rzPrev = u.b;
+            return u.a;
+        } else {
             return vcycleT(S, rp, K);
+        }
     };
+    if constexpr (F32Precond) { // z_previous of the first direction: zero
+        const int n = S.C.n;
+        FOR_CELLS(c) K.z[c] = T(0);
+    }
     double rz = precond();
     pcgDirection(S, K, 0.0);
     for (int it = 0; it < maxIter; ++it) {
@@ -1058,7 +1087,9 @@ __device__ __noinline__ LinRes pcgT(Shared &S, int &rp, const KW<T> &K, T *x, do
             return res;
         }
         const double rzNew = precond();
-        pcgDirection(S, K, rzNew / (rz + 1e-30));
+        // Fletcher-Reeves as the reference; Polak-Ribiere (flexible CG) around the
+        // FP32 V-cycle
+        pcgDirection(S, K, (rzNew - rzPrev) / (rz + 1e-30));
         rz = rzNew;
     }
     return res;
@@ -1310,6 +1341,7 @@ __device__ void carve(Shared &S, double *ws, double *arena, long arenaDoubles) {
     W.phi = take(nf);
     W.phiPred = take(nf);
     W.pCoeff = take(nf);
+    W.fScr = take(nf);
     W.gPx = take(n);
     W.gPy = take(n);
     W.gUxx = take(n);
@@ -1525,6 +1557,8 @@ __device__ __noinline__ void phClosure(Shared &S, double floorV) {
             }
 }
 
+// gradient of the solved Ux for the y assembly (Uy, and so its gradient from
+// phStart, is unchanged until the y solve)
 __device__ __noinline__ void phGradU(Shared &S) {
     RQ_PRELUDE
                 FOR_CELLS(c) {
@@ -1533,27 +1567,87 @@ __device__ __noinline__ void phGradU(Shared &S) {
                     ggCell(C, q, W.Ux, 0.0, 0.0, gx, gy);
                     W.gUxx[c] = gx;
                     W.gUxy[c] = gy;
-                    ggCell(C, q, W.Uy, 0.0, 0.0, gx, gy);
-                    W.gUyx[c] = gx;
-                    W.gUyy[c] = gy;
                 }
 }
 
+// The internal faces of the momentum assembly, each once (assembleMomentum
+// :303-482): the diffusion coefficient D = nu_f A / delta (both components: stored
+// by the x pass in pCoeff, free until the p' assembly), the transpose-stress flux of
+// this component (phiPred, free likewise) and its limitedLinearUpwind deferred
+// correction F (phi_f - phi_up) (fScr, :495-532). Wall faces belong to one cell and
+// are formed by the cell sweep.
+__device__ __noinline__ void phMomentumFaces(Shared &S, int comp) {
+    RQ_PRELUDE
+            const double *U = comp == 0 ? W.Ux : W.Uy;
+            const double *gUc_x = comp == 0 ? W.gUxx : W.gUyx; // grad of this component
+            const double *gUc_y = comp == 0 ? W.gUxy : W.gUyy;
+            const double *colX = comp == 0 ? W.gUxx : W.gUxy;  // dUx/dx_comp
+            const double *colY = comp == 0 ? W.gUyx : W.gUyy;  // dUy/dx_comp
+            for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+                int fi, o, qn;
+                const double *A, *NX, *NY, *WT, *DL;
+                double sh = 0.0;
+                if (f < n) {
+                    fi = f;
+                    o = f;
+                    qn = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                    A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl;
+                    sh = C.xsh[fi];
+                } else {
+                    fi = f - n;
+                    const int jf = fi / nx;
+                    if (jf == 0 || jf == ny)
+                        continue;
+                    o = fi - nx;
+                    qn = fi;
+                    A = C.ya; NX = C.ynx; NY = C.yny; WT = C.yw; DL = C.ydl;
+                }
+                const double delta = dmax(DL[fi], 1e-20);
+                const double F = W.phi[f];
+                const double w = WT[fi];
+                if (comp == 0) {
+                    const double nuO = nu + W.nuT[o], nuN = nu + W.nuT[qn];
+                    const double nuF = w * nuO + (1.0 - w) * nuN;
+                    W.pCoeff[f] = nuF * A[fi] / delta;
+                }
+                const double cf = w * W.nuT[o] + (1.0 - w) * W.nuT[qn];
+                const double gxf = colX[o] * w + colX[qn] * (1.0 - w);
+                const double gyf = colY[o] * w + colY[qn] * (1.0 - w);
+                W.phiPred[f] = cf * (gxf * NX[fi] + gyf * NY[fi]) * A[fi];
+                double corr = 0.0;
+                if (F != 0.0) {
+                    const bool ownerUp = F > 0.0;
+                    const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
+                    const double xUx = C.cx[up], xUy = C.cy[up];
+                    const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
+                    const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
+                    const double dphi = U[dn] - U[up];
+                    double psi = 0.0;
+                    if (fabs(dphi) > 1e-300) {
+                        const double rr = 2.0 * (gUc_x[up] * (xDx - xUx) + gUc_y[up] * (xDy - xUy)) / dphi - 1.0;
+                        psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
+                    }
+                    const double pf = U[up] + 0.5 * psi * dphi;
+                    corr = F * (pf - U[up]);
+                }
+                W.fScr[f] = corr;
+            }
+}
+
+// The momentum rows of one component from the face values of phMomentumFaces
+// (the wall faces here), summed in the reference's face order; the row's residual.
 __device__ __noinline__ void phMomentum(Shared &S, int comp, double (&acc)[3]) {
     RQ_PRELUDE
             double *U = comp == 0 ? W.Ux : W.Uy;
-            const double *gUc_x = comp == 0 ? W.gUxx : W.gUyx; // grad of this component
-            const double *gUc_y = comp == 0 ? W.gUxy : W.gUyy;
             const double *colX = comp == 0 ? W.gUxx : W.gUxy;  // dUx/dx_comp
             const double *colY = comp == 0 ? W.gUyx : W.gUyy;  // dUy/dx_comp
             const double fb = comp == 0 ? st.fx : st.fy;
             FOR_CELLS(c) {
                 const Cell q = cellOf(C, c);
                 const int i = q.i, j = q.j;
-                // faces: 0 W 1 E 2 S 3 N. owner flags, neighbour cells, face arrays
+                // faces: 0 W 1 E 2 S 3 N
                 double dT[4], aT[4], tsT[4], ccT[4];
                 const bool isWall[4] = {false, false, !q.south, !q.north};
-                const int nb[4] = {q.W, q.E, c - nx, c + nx};
                 for (int k = 0; k < 4; ++k) {
                     dT[k] = 0.0;
                     aT[k] = 0.0;
@@ -1562,29 +1656,22 @@ __device__ __noinline__ void phMomentum(Shared &S, int comp, double (&acc)[3]) {
                 }
                 for (int k = 0; k < 4; ++k) {
                     bool own;
-                    int f, o, qn;
-                    const double *A, *NX, *NY, *WT, *DL;
-                    double sh = 0.0;
-                    int fi;
+                    int f, fi;
+                    const double *A, *DL;
                     if (k < 2) {
                         fi = (k == 0) ? q.W : c;
                         own = (k == 1);
-                        o = fi;
-                        qn = (k == 0) ? c : q.E;
-                        A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl;
-                        sh = C.xsh[fi];
+                        A = C.xa; DL = C.xdl;
                         f = fi;
                     } else {
                         fi = (k == 2) ? c : c + nx;
                         own = (k == 3) || isWall[k];
-                        o = (k == 2) ? c - nx : c;
-                        qn = (k == 2) ? c : c + nx;
-                        A = C.ya; NX = C.ynx; NY = C.yny; WT = C.yw; DL = C.ydl;
+                        A = C.ya; DL = C.ydl;
                         f = n + fi;
                     }
-                    const double delta = dmax(DL[fi], 1e-20);
                     const double F = W.phi[f];
                     if (isWall[k]) { // resolved wall: molecular viscosity, U_b = 0
+                        const double delta = dmax(DL[fi], 1e-20);
                         const double Db = nu * A[fi] / delta;
                         const double Ub = 0.0;
                         if (F >= 0) {
@@ -1596,34 +1683,15 @@ __device__ __noinline__ void phMomentum(Shared &S, int comp, double (&acc)[3]) {
                         }
                         continue;
                     }
-                    const double w = WT[fi];
-                    const double nuO = nu + W.nuT[o], nuN = nu + W.nuT[qn];
-                    const double nuF = w * nuO + (1.0 - w) * nuN;
-                    const double D = nuF * A[fi] / delta;
+                    const double D = W.pCoeff[f];
                     const double cp = dmax(F, 0.0), cn = dmax(-F, 0.0);
                     dT[k] = own ? D + cp : D + cn;
                     aT[k] = own ? -(D + cn) : -(D + cp);
                     // transpose stress flux through this face (StressOperators.hpp:31-81)
-                    const double cf = w * W.nuT[o] + (1.0 - w) * W.nuT[qn];
-                    const double gxf = colX[o] * w + colX[qn] * (1.0 - w);
-                    const double gyf = colY[o] * w + colY[qn] * (1.0 - w);
-                    const double fl = cf * (gxf * NX[fi] + gyf * NY[fi]) * A[fi];
+                    const double fl = W.phiPred[f];
                     tsT[k] = own ? fl : -fl;
-                    // limitedLinearUpwind deferred correction (:495-532)
                     if (F != 0.0) {
-                        const bool ownerUp = F > 0.0;
-                        const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
-                        const double xUx = C.cx[up], xUy = C.cy[up];
-                        const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
-                        const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
-                        const double dphi = U[dn] - U[up];
-                        double psi = 0.0;
-                        if (fabs(dphi) > 1e-300) {
-                            const double rr = 2.0 * (gUc_x[up] * (xDx - xUx) + gUc_y[up] * (xDy - xUy)) / dphi - 1.0;
-                            psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
-                        }
-                        const double pf = U[up] + 0.5 * psi * dphi;
-                        const double corr = F * (pf - U[up]);
+                        const double corr = W.fScr[f];
                         ccT[k] = own ? -corr : corr;
                     }
                 }
@@ -1810,24 +1878,25 @@ __device__ __noinline__ void phPressureCells(Shared &S, double (&pacc)[3]) {
         }
 }
 
-__device__ __noinline__ void phCorrGrad(Shared &S) {
+// Pressure-velocity corrections (:916-940, :1443-1467): U -= grad p' V / aP with
+// owner-valued wall faces for grad p', p += alpha_p p', the face fluxes from p'; on a
+// turbulence update also the k and omega values the change norms compare against.
+// The k and omega gradients of the transport equations are the ones phStart formed:
+// k and omega do not change between the start of the iteration and their solves.
+__device__ __noinline__ void phCorrect(Shared &S, bool turbUpdate) {
     RQ_PRELUDE
         FOR_CELLS(c) {
             const Cell q = cellOf(C, c);
             double gx, gy;
             ggCell(C, q, W.pp, W.pp[c], W.pp[c], gx, gy);
-            W.gKx[c] = gx; // scratch for grad p' (k gradients are recomputed below)
-            W.gKy[c] = gy;
-        }
-}
-
-__device__ __noinline__ void phCorrApply(Shared &S) {
-    RQ_PRELUDE
-        FOR_CELLS(c) {
             const double rA = (fabs(W.aP[c]) > 1e-30) ? 1.0 / W.aP[c] : 0.0;
-            W.Ux[c] -= rA * W.gKx[c] * C.vol[c];
-            W.Uy[c] -= rA * W.gKy[c] * C.vol[c];
+            W.Ux[c] -= rA * gx * C.vol[c];
+            W.Uy[c] -= rA * gy * C.vol[c];
             W.p[c] += st.aP * W.pp[c];
+            if (turbUpdate) {
+                W.kOld[c] = W.k[c];
+                W.wOld[c] = W.w[c];
+            }
         }
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
             double v;
@@ -1845,64 +1914,113 @@ __device__ __noinline__ void phCorrApply(Shared &S) {
         }
 }
 
-__device__ __noinline__ void phTurbGradK(Shared &S) {
+// bounds of the solved k and omega (:1500-1518); a wall cell of omega takes its wall
+// value
+__device__ __forceinline__ void clampK(const Shared &S, int c) {
+    const DevSettings &st = S.C.st;
+    S.W.k[c] = dmax(st.kMin, dmin(st.kMax, S.W.k[c]));
+}
+__device__ __forceinline__ void clampW(const Shared &S, int c) {
+    const DevClass &C = S.C;
+    const Cell q = cellOf(C, c);
+    double v = dmax(C.st.wMin, dmin(1e15, S.W.w[c]));
+    if (!q.south || !q.north)
+        v = wallOmega(C, S.coeff[2], dmax(C.ydl[wallFaceOf(C, c)], 1e-20));
+    S.W.w[c] = v;
+}
+
+// The internal faces of the k or omega assembly, each once (assembleTurbulence
+// :1000-1100): the diffusion coefficient (nu + sigma(F1_f) nuT)_f A / delta (pCoeff),
+// the deferred correction of the limitedLinearUpwind face value (fScr) and, for omega
+// with the near-wall balance, its face term (phiPred). Wall faces are formed by the
+// cell sweep.
+__device__ __noinline__ void phTurbFaces(Shared &S, int eq) {
     RQ_PRELUDE
-            FOR_CELLS(c) {
-                const Cell q = cellOf(C, c);
-                W.kOld[c] = W.k[c];
-                W.wOld[c] = W.w[c];
-                double gx, gy;
-                ggCell(C, q, W.k, 0.0, 0.0, gx, gy);
-                W.gKx[c] = gx;
-                W.gKy[c] = gy;
+    const double *X = eq == 0 ? W.k : W.w;
+    const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
+            for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
+                int fi, o, qn;
+                const double *A, *WT, *DL;
+                double sh = 0.0;
+                const bool xFace = f < n;
+                if (xFace) {
+                    fi = f;
+                    o = f;
+                    qn = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                    A = C.xa; WT = C.xw; DL = C.xdl;
+                    sh = C.xsh[fi];
+                } else {
+                    fi = f - n;
+                    const int jf = fi / nx;
+                    if (jf == 0 || jf == ny)
+                        continue;
+                    o = fi - nx;
+                    qn = fi;
+                    A = C.ya; WT = C.yw; DL = C.ydl;
+                }
+                const double delta = dmax(DL[fi], 1e-20);
+                const double F = W.phi[f];
+                const double w = WT[fi];
+                const double F1f = w * W.F1[o] + (1.0 - w) * W.F1[qn];
+                const double sg = eq == 0 ? blend(sk1, sk2, F1f) : blend(sw1, sw2, F1f);
+                const double eO = nu + sg * W.nuT[o], eN = nu + sg * W.nuT[qn];
+                const double ef = w * eO + (1.0 - w) * eN;
+                W.pCoeff[f] = ef * A[fi] / delta;
+                if (eq == 1 && C.balance) { // singular near-wall balance (:1073-1087)
+                    const double amp = 6 * nu / b1;
+                    const double diff = (C.sing[qn] - C.sing[o]) / delta;
+                    const double sgd = xFace ? C.sgx[fi] : C.sgy[fi];
+                    W.phiPred[f] = amp * A[fi] * ((ef - nu) * sgd - ef * diff);
+                }
+                double corr = 0.0;
+                if (F != 0.0) {
+                    const bool ownerUp = F > 0.0;
+                    const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
+                    const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
+                    const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
+                    const double dphi = X[dn] - X[up];
+                    double psi = 0.0;
+                    if (fabs(dphi) > 1e-300) {
+                        const double rr = 2.0 * (gX[up] * (xDx - C.cx[up]) + gY[up] * (xDy - C.cy[up])) / dphi - 1.0;
+                        psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
+                    }
+                    const double pf = X[up] + 0.5 * psi * dphi;
+                    corr = F * (pf - X[up]);
+                }
+                W.fScr[f] = corr;
             }
 }
 
-__device__ __noinline__ void phTurbGradW(Shared &S) {
-    RQ_PRELUDE
-                    FOR_CELLS(c) {
-                        const Cell q = cellOf(C, c);
-                        double gx, gy;
-                        ggCell(C, q, W.w, bwOf(q.i), bwOf(ny * nx + q.i), gx, gy);
-                        W.gWx[c] = gx;
-                        W.gWy[c] = gy;
-                    }
-}
-
+// The k or omega rows from the face values of phTurbFaces (the wall faces here),
+// sources, relaxation and the omega wall constraint, summed in face order.
 __device__ __noinline__ void phTurbAssemble(Shared &S, int eq) {
     RQ_PRELUDE
     double *X = eq == 0 ? W.k : W.w;
-    const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
-    (void)gX; (void)gY;
                 FOR_CELLS(c) {
+                    if (eq == 1) // the bounds of the k just solved (read below at this cell only)
+                        clampK(S, c);
                     const Cell q = cellOf(C, c);
                     const bool isWall[4] = {false, false, !q.south, !q.north};
                     double dT[4] = {0, 0, 0, 0}, aT[4] = {0, 0, 0, 0}, ccT[4] = {0, 0, 0, 0};
                     double bT[4] = {0, 0, 0, 0}, balT[4] = {0, 0, 0, 0};
                     for (int k = 0; k < 4; ++k) {
                         bool own;
-                        int o, qn, fi, f;
-                        const double *A, *WT, *DL;
-                        double sh = 0.0;
+                        int fi, f;
+                        const double *A, *DL;
                         if (k < 2) {
                             fi = (k == 0) ? q.W : c;
                             own = (k == 1);
-                            o = fi;
-                            qn = (k == 0) ? c : q.E;
-                            A = C.xa; WT = C.xw; DL = C.xdl;
-                            sh = C.xsh[fi];
+                            A = C.xa; DL = C.xdl;
                             f = fi;
                         } else {
                             fi = (k == 2) ? c : c + nx;
                             own = (k == 3) || isWall[k];
-                            o = (k == 2) ? c - nx : c;
-                            qn = (k == 2) ? c : c + nx;
-                            A = C.ya; WT = C.yw; DL = C.ydl;
+                            A = C.ya; DL = C.ydl;
                             f = n + fi;
                         }
-                        const double delta = dmax(DL[fi], 1e-20);
                         const double F = W.phi[f];
                         if (isWall[k]) {
+                            const double delta = dmax(DL[fi], 1e-20);
                             const double sg = eq == 0 ? blend(sk1, sk2, W.F1[c]) : blend(sw1, sw2, W.F1[c]);
                             const double Db = (nu + sg * W.nuT[c]) * A[fi] / delta;
                             const double xb = eq == 0 ? 0.0 : bwOf(fi);
@@ -1915,35 +2033,16 @@ __device__ __noinline__ void phTurbAssemble(Shared &S, int eq) {
                             }
                             continue;
                         }
-                        const double w = WT[fi];
-                        const double F1f = w * W.F1[o] + (1.0 - w) * W.F1[qn];
-                        const double sg = eq == 0 ? blend(sk1, sk2, F1f) : blend(sw1, sw2, F1f);
-                        const double eO = nu + sg * W.nuT[o], eN = nu + sg * W.nuT[qn];
-                        const double ef = w * eO + (1.0 - w) * eN;
-                        const double D = ef * A[fi] / delta;
+                        const double D = W.pCoeff[f];
                         const double cp = dmax(F, 0.0), cn = dmax(-F, 0.0);
                         dT[k] = own ? D + cp : D + cn;
                         aT[k] = own ? -(D + cn) : -(D + cp);
-                        if (eq == 1 && C.balance) { // singular near-wall balance (:1073-1087)
-                            const double amp = 6 * nu / b1;
-                            const double diff = (C.sing[qn] - C.sing[o]) / delta;
-                            const double sgd = (k < 2) ? C.sgx[fi] : C.sgy[fi];
-                            const double corr = amp * A[fi] * ((ef - nu) * sgd - ef * diff);
+                        if (eq == 1 && C.balance) {
+                            const double corr = W.phiPred[f];
                             balT[k] = own ? corr : -corr;
                         }
                         if (F != 0.0) {
-                            const bool ownerUp = F > 0.0;
-                            const int up = ownerUp ? o : qn, dn = ownerUp ? qn : o;
-                            const double xDx = ownerUp ? C.cx[qn] + sh : C.cx[o] - sh;
-                            const double xDy = ownerUp ? C.cy[qn] + 0.0 : C.cy[o] - 0.0;
-                            const double dphi = X[dn] - X[up];
-                            double psi = 0.0;
-                            if (fabs(dphi) > 1e-300) {
-                                const double rr = 2.0 * (gX[up] * (xDx - C.cx[up]) + gY[up] * (xDy - C.cy[up])) / dphi - 1.0;
-                                psi = rr > 0.0 ? (rr * rr + rr) / (rr * rr + 1.0) : 0.0;
-                            }
-                            const double pf = X[up] + 0.5 * psi * dphi;
-                            const double corr = F * (pf - X[up]);
+                            const double corr = W.fScr[f];
                             ccT[k] = own ? -corr : corr;
                         }
                     }
@@ -2058,27 +2157,13 @@ __device__ __noinline__ void phTurbResidual(Shared &S, int eq, double (&acc)[1])
                 }
 }
 
-__device__ __noinline__ void phTurbClamp(Shared &S, int eq) {
-    RQ_PRELUDE
-                if (eq == 0) {
-                    FOR_CELLS(c) W.k[c] = dmax(st.kMin, dmin(st.kMax, W.k[c]));
-                } else {
-                    FOR_CELLS(c) {
-                        const Cell q = cellOf(C, c);
-                        double v = dmax(st.wMin, dmin(1e15, W.w[c]));
-                        if (!q.south || !q.north)
-                            v = wallOmega(C, b1, dmax(C.ydl[wallFaceOf(C, c)], 1e-20));
-                        W.w[c] = v;
-                    }
-                    if (threadIdx.x == 0)
-                        S.wallBeta = b1;
-                }
-}
-
 __device__ __noinline__ void phNorms(Shared &S, bool turbUpdate, double (&mx)[6]) {
     RQ_PRELUDE
+        if (turbUpdate && threadIdx.x == 0)
+            S.wallBeta = b1;
         FOR_CELLS(c) {
             if (turbUpdate) {
+                clampW(S, c);
                 mx[0] = dmax(mx[0], fabs(W.k[c]));
                 mx[1] = dmax(mx[1], fabs(W.w[c]));
                 mx[2] = dmax(mx[2], fabs(W.k[c] - W.kOld[c]));
@@ -2201,6 +2286,8 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             }
             double *U = comp == 0 ? W.Ux : W.Uy;
             double acc[3] = {0.0, 0.0, 0.0};
+            phMomentumFaces(S, comp);
+            __syncthreads();
             phMomentum(S, comp, acc);
             blockSum<3>(acc, S, rp);
             momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
@@ -2231,10 +2318,8 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         __syncthreads();
 
         mark(S, 4);
-        // ---- corrections (:916-940, :1443-1467): grad p' with owner-valued wall faces
-        phCorrGrad(S);
-        __syncthreads();
-        phCorrApply(S);
+        // ---- corrections (:916-940, :1443-1467)
+        phCorrect(S, turbUpdate);
         __syncthreads();
 
         // ---- turbulence (:1476-1538)
@@ -2242,16 +2327,13 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
         resK = LinRes{0, 0, 0, true};
         resW = LinRes{0, 0, 0, true};
         if (turbUpdate) {
-            phTurbGradK(S);
-            __syncthreads();
+            // the clamp of k runs inside the omega assembly and the clamp of omega
+            // inside the change norms (each reads only its own cell's value)
             for (int eq = 0; eq < 2; ++eq) { // 0: k, 1: omega
                 double *X = eq == 0 ? W.k : W.w;
-                const double *gX = eq == 0 ? W.gKx : W.gWx, *gY = eq == 0 ? W.gKy : W.gWy;
-                if (eq == 1) {
-                    phTurbGradW(S);
-                    __syncthreads();
-                }
                 double acc[1] = {0.0};
+                phTurbFaces(S, eq);
+                __syncthreads();
                 phTurbAssemble(S, eq);
                 __syncthreads();
                 // initial residual with the (constrained) initial guess: wall cells of
@@ -2266,8 +2348,6 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     resW = rr;
                 if (threadIdx.x == 0)
                     S.innerKrylov += rr.iterations;
-                __syncthreads();
-                phTurbClamp(S, eq);
                 __syncthreads();
             }
         }
