@@ -254,6 +254,9 @@ void upload(rq_problem &P, const rq_obs_desc *obs, double nu, const rq_settings 
         addD(&C.obsVar, var);
         addD(&C.obsFloor, fl);
     }
+    // cell and face rows are found without integer division (exact below 2^21)
+    if (static_cast<long>(m.n) + m.nfy() >= (1L << 21))
+        throw RqError(RQ_E_UNSUPPORTED, "meshes of 2^21 cells and faces or more are not supported on the GPU path");
     // AMG hierarchy
     const int L = static_cast<int>(h.lev.size());
     if (L > rq::kMaxLevels)

@@ -171,10 +171,21 @@ struct Cell {
     bool yNfirst;      // north before south (bottom row of a multi-row mesh)
 };
 
+// row of a cell or y face index (idx / nx), without an integer division: exact while
+// (idx + 0.5) / nx stays clear of an integer by more than the FP32 rounding, i.e. for
+// any index below 2^21
+__device__ __forceinline__ int rowOf(const DevClass &C, int idx) {
+    return __float2int_rd((static_cast<float>(idx) + 0.5f) * __frcp_rn(static_cast<float>(C.nx)));
+}
+// the east neighbour of the cell owning x face f (periodic in x)
+__device__ __forceinline__ int eastOf(const DevClass &C, int f) {
+    return (f - rowOf(C, f) * C.nx == C.nx - 1) ? f - C.nx + 1 : f + 1;
+}
+
 __device__ __forceinline__ Cell cellOf(const DevClass &C, int c) {
     Cell q;
     q.c = c;
-    q.j = __float2int_rd((static_cast<float>(c) + 0.5f) * __frcp_rn(static_cast<float>(C.nx)));
+    q.j = rowOf(C, c);
     q.i = c - q.j * C.nx;
     q.W = q.i == 0 ? c + C.nx - 1 : c - 1;
     q.E = q.i == C.nx - 1 ? c - C.nx + 1 : c + 1;
@@ -201,12 +212,11 @@ __device__ __forceinline__ double accum4(const Cell &q, double acc, double tW, d
 
 // the wall face of a wall cell; a cell touching both walls keeps the last (top) one
 __device__ __forceinline__ int wallFaceOf(const DevClass &C, int c) {
-    const int j = c / C.nx;
-    return (j == C.ny - 1 ? C.ny : 0) * C.nx + c % C.nx;
+    const int j = rowOf(C, c);
+    return (j == C.ny - 1 ? C.ny : 0) * C.nx + (c - j * C.nx);
 }
 __device__ __forceinline__ bool isWallCell(const DevClass &C, int c) {
-    const int j = c / C.nx;
-    return j == 0 || j == C.ny - 1;
+    return c < C.nx || c >= C.n - C.nx;
 }
 
 __device__ __forceinline__ double wallOmega(const DevClass &C, double b1, double y) {
@@ -558,30 +568,44 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
 }
 
 // Sum over the slots k = first, first + step, ... (< width) of one ELL row of
-// coef(k) * vec(col(k)) for columns >= 0, k ascending. The loads of up to eight slots
-// B slots are issued before their products are added (padding slots and slots past
-// the row add nothing), so a row of up to B slots per lane costs one column load and
-// one value load in sequence, not one pair per slot. The coarse operators (up to 15
-// slots a row) take B = 8, the transfers (2-4) B = 4.
-template <typename T, int B = 4, typename C, typename V>
+// coef(k) * vec(col(k)) for columns >= 0, k ascending. The loads of four slots are
+// issued before their products are added (padding slots load entry 0 and add
+// nothing), so a wide row costs a few load latencies, not one per slot.
+template <typename T, typename C, typename V>
 __device__ __forceinline__ T ellDot(const int32_t *cols, const C *coef, const V *vec, int width,
                                     int stride, int row, int first = 0, int step = 1) {
     T s = T(0);
-    for (int k = first; k < width; k += B * step) {
-        int c[B];
-        T v[B], x[B];
+    int k = first;
+    for (; k + 3 * step < width; k += 4 * step) {
+        int c[4];
+        T v[4], x[4];
 #pragma unroll
-        for (int u = 0; u < B; ++u)
-            c[u] = (k + u * step < width) ? __ldg(cols + (k + u * step) * stride + row) : -1;
+        for (int u = 0; u < 4; ++u)
+            c[u] = __ldg(cols + (k + u * step) * stride + row);
 #pragma unroll
-        for (int u = 0; u < B; ++u) {
-            v[u] = c[u] >= 0 ? T(coef[(k + u * step) * stride + row]) : T(0);
-            x[u] = c[u] >= 0 ? T(vec[c[u]]) : T(0);
+        for (int u = 0; u < 4; ++u) {
+            v[u] = T(coef[(k + u * step) * stride + row]);
+            x[u] = T(vec[c[u] < 0 ? 0 : c[u]]);
         }
 #pragma unroll
-        for (int u = 0; u < B; ++u)
+        for (int u = 0; u < 4; ++u)
             if (c[u] >= 0)
                 s += v[u] * x[u];
+    }
+    if (k + step < width) {
+        const int c0 = __ldg(cols + k * stride + row), c1 = __ldg(cols + (k + step) * stride + row);
+        const T v0 = T(coef[k * stride + row]), v1 = T(coef[(k + step) * stride + row]);
+        const T x0 = T(vec[c0 < 0 ? 0 : c0]), x1 = T(vec[c1 < 0 ? 0 : c1]);
+        if (c0 >= 0)
+            s += v0 * x0;
+        if (c1 >= 0)
+            s += v1 * x1;
+        k += 2 * step;
+    }
+    if (k < width) {
+        const int c = __ldg(cols + k * stride + row);
+        if (c >= 0)
+            s += T(coef[k * stride + row]) * T(vec[c]);
     }
     return s;
 }
@@ -692,7 +716,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         if (two) {
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T, 8>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
@@ -700,7 +724,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         }
         segPass<T>(n,
                    [&](int i, int j, int seg) {
-                       return ellDot<T, 8>(Lv.ecol, val, xs, Lv.width, n, i, j, seg);
+                       return ellDot<T>(Lv.ecol, val, xs, Lv.width, n, i, j, seg);
                    },
                    [&](int i, T ax) { rr[i] = b[i] - ax; });
         sync();
@@ -754,7 +778,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
             sync();
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T, 8>(Lv.ecol, val, xi, Lv.width, n, i, j, seg);
+                           return ellDot<T>(Lv.ecol, val, xi, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { out[i] = xi[i] + om * (b[i] - ax) * rd[i]; });
         } else {
@@ -773,7 +797,7 @@ template <typename T> __device__ __noinline__ double vcycleT(Shared &S, int &rp,
         if (two) {
             segPass<T>(n,
                        [&](int i, int j, int seg) {
-                           return ellDot<T, 8>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
+                           return ellDot<T>(Lv.ecol, val, xa, Lv.width, n, i, j, seg);
                        },
                        [&](int i, T ax) { xb[i] = xa[i] + om * (b[i] - ax) * rd[i]; });
             sync();
@@ -1457,12 +1481,12 @@ __device__ __noinline__ void phInitFlux(Shared &S) {
     for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
         double v = 0.0;
         if (f < n) {
-            const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+            const int q = eastOf(C, f);
             const double w = C.xw[f];
             const double ux = W.Ux[f] * w + W.Ux[q] * (1.0 - w), uy = W.Uy[f] * w + W.Uy[q] * (1.0 - w);
             v = (ux * C.xnx[f] + uy * C.xny[f]) * C.xa[f];
         } else {
-            const int g = f - n, jf = g / nx;
+            const int g = f - n, jf = rowOf(C, g);
             if (jf > 0 && jf < ny) {
                 const int o = g - nx;
                 const double w = C.yw[g];
@@ -1481,12 +1505,12 @@ __device__ __noinline__ void phStart(Shared &S, bool turbUpdate) {
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
             double v = 0.0;
             if (f < n) {
-                const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                const int q = eastOf(C, f);
                 const double w = C.xw[f];
                 const double ux = W.Ux[f] * w + W.Ux[q] * (1.0 - w), uy = W.Uy[f] * w + W.Uy[q] * (1.0 - w);
                 v = (ux * C.xnx[f] + uy * C.xny[f]) * C.xa[f];
             } else {
-                const int g = f - n, jf = g / nx;
+                const int g = f - n, jf = rowOf(C, g);
                 if (jf > 0 && jf < ny) {
                     const int o = g - nx;
                     const double w = C.yw[g];
@@ -1590,12 +1614,12 @@ __device__ __noinline__ void phMomentumFaces(Shared &S, int comp) {
                 if (f < n) {
                     fi = f;
                     o = f;
-                    qn = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                    qn = eastOf(C, f);
                     A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl;
                     sh = C.xsh[fi];
                 } else {
                     fi = f - n;
-                    const int jf = fi / nx;
+                    const int jf = rowOf(C, fi);
                     if (jf == 0 || jf == ny)
                         continue;
                     o = fi - nx;
@@ -1790,11 +1814,11 @@ __device__ __noinline__ void phPressureFaces(Shared &S, double (&fs)[1]) {
             if (f < n) {
                 fi = f;
                 o = f;
-                q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                q = eastOf(C, f);
                 A = C.xa; NX = C.xnx; NY = C.xny; WT = C.xw; DL = C.xdl; DX = C.xdx; DY = C.xdy;
             } else {
                 fi = f - n;
-                const int jf = fi / nx;
+                const int jf = rowOf(C, fi);
                 wall = (jf == 0 || jf == ny);
                 o = fi - nx;
                 q = fi;
@@ -1901,10 +1925,10 @@ __device__ __noinline__ void phCorrect(Shared &S, bool turbUpdate) {
         for (int f = threadIdx.x; f < n + nfy; f += blockDim.x) {
             double v;
             if (f < n) {
-                const int q = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                const int q = eastOf(C, f);
                 v = W.phiPred[f] - W.pCoeff[f] * (W.pp[q] - W.pp[f]);
             } else {
-                const int g = f - n, jf = g / nx;
+                const int g = f - n, jf = rowOf(C, g);
                 if (jf > 0 && jf < ny)
                     v = W.phiPred[f] - W.pCoeff[f] * (W.pp[g] - W.pp[g - nx]);
                 else
@@ -1946,12 +1970,12 @@ __device__ __noinline__ void phTurbFaces(Shared &S, int eq) {
                 if (xFace) {
                     fi = f;
                     o = f;
-                    qn = (f % nx == nx - 1) ? f - nx + 1 : f + 1;
+                    qn = eastOf(C, f);
                     A = C.xa; WT = C.xw; DL = C.xdl;
                     sh = C.xsh[fi];
                 } else {
                     fi = f - n;
-                    const int jf = fi / nx;
+                    const int jf = rowOf(C, fi);
                     if (jf == 0 || jf == ny)
                         continue;
                     o = fi - nx;
@@ -2098,8 +2122,7 @@ __device__ __noinline__ void phTurbAssemble(Shared &S, int eq) {
                             if (isWall[k])
                                 continue;
                             const int qq = nbc[k];
-                            const int jq = qq / nx;
-                            const bool nbW = (jq == 0 || jq == ny - 1);
+                            const bool nbW = qq < nx || qq >= n - nx; // first or last row
                             const bool own = (k == 1 || k == 3);
                             if (own) {
                                 if (selfW) {
