@@ -231,54 +231,46 @@ __device__ __forceinline__ double wallFaceOmega(const DevClass &C, double b1, in
 
 // Green-Gauss gradient of one cell (Field.hpp:178-212); bS / bN are the wall
 // face values used where the cell touches the bottom / top wall.
-// The face geometry of one cell's Green-Gauss gradient: interpolation weights and
-// area vectors of its four faces and its volume (shared by the gradients of several
-// fields of the same cell).
-struct GGeo {
-    double wE, sxE, syE, wW, sxW, syW, wN, sxN, syN, wS, sxS, syS, V;
-};
-__device__ __forceinline__ GGeo ggGeo(const DevClass &C, const Cell &q) {
-    const int c = q.c, fn = c + C.nx, fs = c;
-    GGeo g;
-    g.wE = __ldg(C.xw + (c));
-    g.sxE = __ldg(C.xnx + (c)) * __ldg(C.xa + (c));
-    g.syE = __ldg(C.xny + (c)) * __ldg(C.xa + (c));
-    g.wW = __ldg(C.xw + (q.W));
-    g.sxW = __ldg(C.xnx + (q.W)) * __ldg(C.xa + (q.W));
-    g.syW = __ldg(C.xny + (q.W)) * __ldg(C.xa + (q.W));
-    g.wN = q.north ? __ldg(C.yw + (fn)) : 0.0;
-    g.sxN = __ldg(C.ynx + (fn)) * __ldg(C.ya + (fn));
-    g.syN = __ldg(C.yny + (fn)) * __ldg(C.ya + (fn));
-    g.wS = q.south ? __ldg(C.yw + (fs)) : 0.0;
-    g.sxS = __ldg(C.ynx + (fs)) * __ldg(C.ya + (fs));
-    g.syS = __ldg(C.yny + (fs)) * __ldg(C.ya + (fs));
-    g.V = __ldg(C.vol + (c));
-    return g;
-}
-// Green-Gauss gradient of one cell (Field.hpp:178-212) from its face geometry; bS / bN
-// are the wall face values used where the cell touches the bottom / top wall.
-__device__ __forceinline__ void ggApply(const DevClass &C, const Cell &q, const GGeo &g,
-                                        const double *phi, double bS, double bN, double &gx,
-                                        double &gy) {
-    const int c = q.c;
-    const double pc = phi[c];
-    const double fE = pc * g.wE + phi[q.E] * (1.0 - g.wE);   // east (owner c)
-    const double fW = phi[q.W] * g.wW + pc * (1.0 - g.wW);   // west (owner W, neighbour c)
-    // north: internal (owner c) or top wall (owner c)
-    const double fN = q.north ? pc * g.wN + phi[c + C.nx] * (1.0 - g.wN) : bN;
-    // south: internal (owner c - nx, neighbour c) or bottom wall (owner c)
-    const double fS = q.south ? phi[c - C.nx] * g.wS + pc * (1.0 - g.wS) : bS;
-    const double sgnS = q.south ? -1.0 : 1.0;
-    gx = order4(q, -(g.sxW * fW), g.sxE * fE, sgnS * (g.sxS * fS), g.sxN * fN);
-    gy = order4(q, -(g.syW * fW), g.syE * fE, sgnS * (g.syS * fS), g.syN * fN);
-    if (g.V > 1e-30) {
-        gx = gx / g.V;
-        gy = gy / g.V;
-    }
-}
 __device__ __forceinline__ void ggCell(const DevClass &C, const Cell &q, const double *phi,
                                        double bS, double bN, double &gx, double &gy) {
-    ggApply(C, q, ggGeo(C, q), phi, bS, bN, gx, gy);
+    const int c = q.c;
+    const double pc = phi[c];
+    // east (owner c)
+    const double wE = __ldg(C.xw + (c));
+    const double fE = pc * wE + phi[q.E] * (1.0 - wE);
+    const double sxE = __ldg(C.xnx + (c)) * __ldg(C.xa + (c)), syE = __ldg(C.xny + (c)) * __ldg(C.xa + (c));
+    // west (owner W, neighbour c)
+    const double wWf = __ldg(C.xw + (q.W));
+    const double fW = phi[q.W] * wWf + pc * (1.0 - wWf);
+    const double sxW = __ldg(C.xnx + (q.W)) * __ldg(C.xa + (q.W)), syW = __ldg(C.xny + (q.W)) * __ldg(C.xa + (q.W));
+    // north: internal (owner c) or top wall (owner c)
+    const int fn = c + C.nx;
+    double fN;
+    if (q.north) {
+        const double w = __ldg(C.yw + (fn));
+        fN = pc * w + phi[c + C.nx] * (1.0 - w);
+    } else {
+        fN = bN;
+    }
+    const double sxN = __ldg(C.ynx + (fn)) * __ldg(C.ya + (fn)), syN = __ldg(C.yny + (fn)) * __ldg(C.ya + (fn));
+    // south: internal (owner c - nx, neighbour c) or bottom wall (owner c)
+    const int fs = c;
+    double fS;
+    if (q.south) {
+        const double w = __ldg(C.yw + (fs));
+        fS = phi[c - C.nx] * w + pc * (1.0 - w);
+    } else {
+        fS = bS;
+    }
+    const double sxS = __ldg(C.ynx + (fs)) * __ldg(C.ya + (fs)), syS = __ldg(C.yny + (fs)) * __ldg(C.ya + (fs));
+    const double sgnS = q.south ? -1.0 : 1.0;
+    gx = order4(q, -(sxW * fW), sxE * fE, sgnS * (sxS * fS), sxN * fN);
+    gy = order4(q, -(syW * fW), syE * fE, sgnS * (syS * fS), syN * fN);
+    const double V = __ldg(C.vol + (c));
+    if (V > 1e-30) {
+        gx = gx / V;
+        gy = gy / V;
+    }
 }
 
 // matrix row times x in the reference's matvec order (diagonal first, then faces)
@@ -1535,22 +1527,21 @@ __device__ __noinline__ void phStart(Shared &S, bool turbUpdate) {
             W.Uxp[c] = W.Ux[c];
             W.Uyp[c] = W.Uy[c];
             double gx, gy;
-            const GGeo g = ggGeo(C, q); // one geometry load for the five gradients
-            ggApply(C, q, g, W.Ux, 0.0, 0.0, gx, gy);
+            ggCell(C, q, W.Ux, 0.0, 0.0, gx, gy);
             W.gUxx[c] = gx;
             W.gUxy[c] = gy;
-            ggApply(C, q, g, W.Uy, 0.0, 0.0, gx, gy);
+            ggCell(C, q, W.Uy, 0.0, 0.0, gx, gy);
             W.gUyx[c] = gx;
             W.gUyy[c] = gy;
             // pressure faces carry the owner value (Neumann walls)
-            ggApply(C, q, g, W.p, W.p[c], W.p[c], gx, gy);
+            ggCell(C, q, W.p, W.p[c], W.p[c], gx, gy);
             W.gPx[c] = gx;
             W.gPy[c] = gy;
             if (turbUpdate) {
-                ggApply(C, q, g, W.k, 0.0, 0.0, gx, gy);
+                ggCell(C, q, W.k, 0.0, 0.0, gx, gy);
                 W.gKx[c] = gx;
                 W.gKy[c] = gy;
-                ggApply(C, q, g, W.w, bwOf(q.i), bwOf(C.ny * nx + q.i), gx, gy);
+                ggCell(C, q, W.w, bwOf(q.i), bwOf(C.ny * nx + q.i), gx, gy);
                 W.gWx[c] = gx;
                 W.gWy[c] = gy;
             }
@@ -2325,11 +2316,10 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
             momRes = comp == 0 ? acc[0] : dmax(momRes, acc[0]);
             if (comp == 0)
                 momScale = acc[2];
-            // every inner solver's last write of its x precedes a barrier of its own
-            // (a reduction's or the exit's), so the next sweep may read neighbours
             resU[comp] = solveBicg(S, rp, U, sqrt(acc[1]), st.innerIter, st.innerTol);
             if (threadIdx.x == 0)
                 S.innerKrylov += resU[comp].iterations;
+            __syncthreads();
         }
 
         mark(S, 2);
@@ -2348,6 +2338,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                              amgNeed, amgAfter);
         if (threadIdx.x == 0)
             S.innerPressure += resP.iterations;
+        __syncthreads();
 
         mark(S, 4);
         // ---- corrections (:916-940, :1443-1467)
@@ -2380,6 +2371,7 @@ __device__ void runSolve(Shared &S, const DevJob &job) {
                     resW = rr;
                 if (threadIdx.x == 0)
                     S.innerKrylov += rr.iterations;
+                __syncthreads();
             }
         }
 
