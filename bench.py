@@ -41,8 +41,8 @@ BYTES_OUTER, BYTES_KRYLOV, BYTES_PRESSURE = 1600, 360, 400  # algorithmic B/cell
 #   between its SM and L2 (L1 misses, spills, stores);
 # * the L2's peak: 3 sectors per cycle on each of the 184 slices (ncu's
 #   lts__t_sectors peak_sustained) x 32 B at the 1965 MHz clock.
-DRAM_BYTES_PER_DRAW_1536 = 2_215_168 + 1_280
-L2_BYTES_PER_ITER_1536 = 303_402_369 * 32 / 600
+DRAM_BYTES_PER_DRAW_1536 = 2_609_408 + 2_304
+L2_BYTES_PER_ITER_1536 = 280_240_249 * 32 / 600
 L2_PEAK_GBS = 3 * 32 * 184 * 1.965
 
 
