@@ -548,12 +548,21 @@ template <typename T> __device__ __noinline__ void amgRefreshT(Shared &S, const 
             }
     }
     __syncthreads();
+    // the (row, column) of a thread's entries advance by the CTA width without a division
+    const int dq = static_cast<int>(blockDim.x) / m2, dr = static_cast<int>(blockDim.x) - dq * m2;
+    const int r0 = static_cast<int>(threadIdx.x) / m2, c0 = static_cast<int>(threadIdx.x) - r0 * m2;
     for (int piv = 0; piv < m; ++piv) {
         const double inv = 1.0 / A0[piv * m2 + piv];
+        int r = r0, col = c0;
         for (int e = threadIdx.x; e < m * m2; e += blockDim.x) {
-            const int r = e / m2, col = e - r * m2;
             const double pr = A0[piv * m2 + col] * inv;
             A1[e] = (r == piv) ? pr : A0[e] - A0[r * m2 + piv] * pr;
+            r += dq;
+            col += dr;
+            if (col >= m2) {
+                col -= m2;
+                ++r;
+            }
         }
         __syncthreads();
         double *tmp = A0;
