@@ -911,7 +911,7 @@ def plain_cpu_seconds_per_iteration(cap: int = 20000) -> float:
 
 
 def plain_arm(args):
-    """The survey's configuration 1: one cold FP64 solve at (a1, beta*) = (0.31, 0.09) on
+    """Configuration 1 (one plain solve): one cold FP64 solve at (a1, beta*) = (0.31, 0.09) on
     the 3 x 128 channel (y+ 0.5, alpha_U 0.5, tol 1e-10, cap 150000), timed on the device
     with theta resident, and once more through the host API (e2e)."""
     import torch

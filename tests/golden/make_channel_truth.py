@@ -1,8 +1,7 @@
 """Writes bayesian-rans-uq_b200/data/channel_truth.json: the noise-free synthetic observed profile of each
 Re_tau class of the channel ensemble -- the reference's own FP64 ForwardModel
 solve at (a1, beta*) = (0.31, 0.09) on that class's mesh, sampled at the 30
-stations (the survey's stand-in for the Lee-Moser DNS profile, which is not
-shipped). Run where oracle/_ref is built:  python tests/golden/make_channel_truth.py
+stations (the stand-in for the Lee-Moser DNS profile, which is not shipped). Run where oracle/_ref is built:  python tests/golden/make_channel_truth.py
 """
 import json
 import multiprocessing
