@@ -510,7 +510,8 @@ def summarize(recs, clock, cls, cells, ms, total_conv, world, args, max_iter, e2
                              "+ 360 B/cell/Krylov it + 400 B/cell/pressure it) / time / HBM peak, "
                              "a rate of on-chip work, not HBM use: the state lives in shared "
                              "memory, L1 and L2 (dram_frac), and the bound in practice is the "
-                             "latency of the dependent phases of each outer iteration"},
+                             "dependent work of each outer iteration on one SM (instruction "
+                             "issue and the latency of L1 misses served by L2: l2_frac)"},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
