@@ -1947,7 +1947,7 @@ __device__ __noinline__ void phCorrect(Shared &S, bool turbUpdate) {
         }
 }
 
-// bounds of the solved k and omega (:1500-1518); a wall cell of omega takes its wall
+// bounds of the solved k and omega (:1489, :1505-1513); a wall cell of omega takes its wall
 // value
 __device__ __forceinline__ void clampK(const Shared &S, int c) {
     const DevSettings &st = S.C.st;
@@ -1962,11 +1962,12 @@ __device__ __forceinline__ void clampW(const Shared &S, int c) {
     S.W.w[c] = v;
 }
 
-// The internal faces of the k or omega assembly, each once (assembleTurbulence
-// :1000-1100): the diffusion coefficient (nu + sigma(F1_f) nuT)_f A / delta (pCoeff),
-// the deferred correction of the limitedLinearUpwind face value (fScr) and, for omega
-// with the near-wall balance, its face term (phiPred). Wall faces are formed by the
-// cell sweep.
+// The internal faces of the k or omega assembly, each once (assembleKEquation
+// :947-1028, assembleOmegaEquation :1030-1171): the diffusion coefficient
+// (nu + sigma(F1_f) nuT)_f A / delta (pCoeff), the deferred correction of the
+// limitedLinearUpwind face value (fScr, addConvectionCorrection :495-552) and, for
+// omega with the near-wall balance, its face term (phiPred, :1073-1087). Wall faces
+// are formed by the cell sweep.
 __device__ __noinline__ void phTurbFaces(Shared &S, int eq) {
     RQ_PRELUDE
     const double *X = eq == 0 ? W.k : W.w;
